@@ -1,0 +1,384 @@
+#!/usr/bin/env python
+"""TV-L1 frame pairs/s at 1024x436 on B200 (5 scales x 5 warps x <= 50 inner
+iterations, lambda 0.15, tau 0.25, theta 0.3, epsilon 0.01).
+
+One step = one batch of --batch synthetic pairs (seeded generator of the
+1024x436 workload: textured noise, affine background, moving disc, N(0,2)
+noise, uint8 frames) solved through the library.  Prints one JSON line on
+rank 0.
+
+  python bench.py [--gpus N --steps K --warmup W --batch P]
+  python bench.py --impl reference ...   # the reference's sequential C++ TV-L1
+                                         # (compiled in place) on the host cores
+
+Under torchrun (N > 1) every rank solves its own batch (pairs are independent,
+no data-path collective: weak scaling); the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "sycl-optic-flow_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+W, H = 1024, 436
+METRIC = "TV-L1 pairs/s @1024x436: learned warm-start vs plain at equal EPE; HBM GB/s"
+PARAMS = dict(nscales=5, max_iterations=50)  # other parameters: reference defaults
+BYTES_PER_PX_ITER = 60  # read u1,u2,p11,p12,p21,p22,I1wx,I1wy,rho_c; write u1,u2,p x4
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def make_pairs(n, seed0):
+    from oflow import synth
+    out = []
+    for i in range(n):
+        p = synth.tvl1_pair(seed=seed0 + i, w=W, h=H)
+        out.append((synth.quantize(p.I0), synth.quantize(p.I1), p))
+    return out
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            v = json.load(f)["hbm_gbs"]
+        return float(v), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per inner-iteration launch from the committed ncu summary
+    (a line 'traffic_bytes_per_launch: N' in profiles/), or None."""
+    path = os.path.join(ROOT, "profiles", "tvl1_iter_1024x436.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampled every 200 ms while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines()]
+        except OSError:
+            rows = []
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.strip() == "Active":
+                    reasons.add(n)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_bytes(stats_list, nx, ny):
+    """Sum over pairs, scales, warps of n_{s,w} * px_s * 60 B (inner iterations)."""
+    tot = 0
+    for st in stats_list:
+        its = st["iterations"]
+        for s in range(its.shape[0]):
+            tot += int(its[s].sum()) * nx[s] * ny[s] * BYTES_PER_PX_ITER
+    return tot
+
+
+def level_sizes(ns):
+    nx, ny = [W], [H]
+    for _ in range(1, ns):
+        nx.append(int(float(nx[-1]) * 0.5 + 0.5))
+        ny.append(int(float(ny[-1]) * 0.5 + 0.5))
+    return nx, ny
+
+
+# ------------------------------------------------------------- CPU baseline
+def cpu_worker(args):
+    """Runs in a subprocess: the reference's sequential TV-L1 (oracle/_ref,
+    OpenMP over all host threads) or, without it, the oracle port (one
+    thread), on up to --cpu-pairs pairs or --cpu-seconds of work."""
+    import numpy as np
+    import oracle
+    pairs = make_pairs(1, 1000)
+    a, b, _ = pairs[0]
+    prm = oracle.TVL1Params(**PARAMS)
+    if oracle.ref_available():
+        kind, cores = "reference", int(os.environ.get("OMP_NUM_THREADS", "1"))
+        run = lambda: oracle.ref_tvl1(a, b, prm)
+    else:
+        kind, cores = "port", 1
+        run = lambda: oracle.tvl1(a.astype(np.float32), b.astype(np.float32), prm)
+    run()  # warm-up
+    n, t0 = 0, time.perf_counter()
+    times = []
+    while n < args.cpu_pairs and (time.perf_counter() - t0) < args.cpu_seconds:
+        t = time.perf_counter()
+        run()
+        times.append(time.perf_counter() - t)
+        n += 1
+    el = time.perf_counter() - t0
+    print(json.dumps({"value": n / el, "unit": "pairs/s", "cores": cores, "kind": kind,
+                      "sample": f"{n} pairs of the 1024x436 workload, {el:.1f} s, "
+                                f"median {1e3 * sorted(times)[len(times) // 2]:.0f} ms/pair"}))
+
+
+def cpu_baseline(pairs=30, seconds=20.0, threads=None):
+    threads = threads or os.cpu_count() or 1
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    cmd = [sys.executable, os.path.abspath(__file__), "--cpu-worker", "--cpu-pairs", str(pairs),
+           "--cpu-seconds", str(seconds)]
+    out = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=600)
+    if out.returncode != 0:
+        log(out.stderr[-2000:])
+        return None
+    return json.loads(out.stdout.strip().splitlines()[-1])
+
+
+# ------------------------------------------------------------- reference arm
+def reference_arm(args, rank):
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    import numpy as np
+    import oracle
+    a, b, _ = make_pairs(1, 1000)[0]
+    prm = oracle.TVL1Params(**PARAMS)
+    if oracle.ref_available():
+        kind = "reference"
+        run = lambda: oracle.ref_tvl1(a, b, prm)
+    else:
+        kind, threads = "port", 1
+        run = lambda: oracle.tvl1(a.astype(np.float32), b.astype(np.float32), prm)
+    for _ in range(args.warmup):
+        run()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        run()
+    el = time.perf_counter() - t0
+    v = args.steps / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "pairs/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "tvl1 1024x436, 5 scales x 5 warps x <=50 inner iterations, "
+                               "1 uint8 pair per step", "solver": "reference sequential C++ "
+                               "(src/tvl1/sequential, OpenMP)"},
+        "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": threads, "kind": kind,
+                         "sample": f"{args.steps} pairs, one per step"},
+        "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------- our arm
+def our_arm(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import oflow
+    from oflow import synth
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180),
+                                device_id=torch.device("cuda", local_rank))
+    dev = torch.device("cuda", local_rank)
+    P = args.batch
+    log(f"[rank {rank}] generating {P} pairs ...")
+    pairs = make_pairs(P, 10_000 * rank)
+    prm = oflow.TVL1Params(**PARAMS)
+    ctx = oflow.Context(local_rank)
+    stream = torch.cuda.current_stream(dev)
+    ctx.set_stream(stream.cuda_stream)
+
+    d_in = [(torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)) for a, b, _ in pairs]
+    d_out = [(torch.empty((H, W), dtype=torch.float32, device=dev),
+              torch.empty((H, W), dtype=torch.float32, device=dev)) for _ in range(P)]
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # --- device-resident inputs (value)
+    for _ in range(args.warmup):
+        oflow.tvl1_batch(d_in, prm, ctx, out=d_out)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local_rank) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            oflow.tvl1_batch(d_in, prm, ctx, out=d_out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    t_dev = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    clocks = clk.summary()
+
+    # --- quality of the timed results, and the per-kernel profile
+    (res, stats, prof) = oflow.tvl1_batch_profile(d_in, prm, ctx, out=d_out)
+    torch.cuda.synchronize()
+    u0 = d_out[0][0].cpu().numpy()
+    v0 = d_out[0][1].cpu().numpy()
+    g = pairs[0][2]
+    epe = synth.epe(u0, v0, g.u, g.v, g.valid, 8)
+    nx, ny = level_sizes(stats[0]["nscales"])
+    alg_iter = algorithmic_bytes(stats, nx, ny)
+    iters_total = int(sum(int(s["iterations"].sum()) for s in stats))
+    peak, peak_kind = measured_peak()
+    achieved = alg_iter / (prof["iter_ms"] / 1e3) / 1e9 if prof["iter_ms"] > 0 else None
+    traffic = ncu_traffic()
+    launches_per_step = prof["launches"]
+
+    # --- end to end through the public API: pinned host frames in, flow out
+    h_in = []
+    for a, b, _ in pairs:
+        ta = torch.from_numpy(a).pin_memory()
+        tb = torch.from_numpy(b).pin_memory()
+        h_in.append((ta.numpy(), tb.numpy()))
+    h_out = [(torch.empty((H, W), dtype=torch.float32).pin_memory().numpy(),
+              torch.empty((H, W), dtype=torch.float32).pin_memory().numpy()) for _ in range(P)]
+    for _ in range(max(1, args.warmup // 2)):
+        oflow.tvl1_batch(h_in, prm, ctx, out=h_out)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    e2e_steps = max(3, args.steps // 2)
+    for _ in range(e2e_steps):
+        oflow.tvl1_batch(h_in, prm, ctx, out=h_out)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    assert np.array_equal(h_out[0][0], u0), "end-to-end result differs from the device run"
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.cpu_pairs, args.cpu_seconds)
+
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    value = world * P * args.steps / t_dev
+    line = {
+        "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_dev / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"tvl1 1024x436, 5 scales x 5 warps x <=50 inner iterations, "
+                               f"{P} uint8 pairs per GPU per step (plain TV-L1)",
+                   "batch_pairs_per_gpu": P, "parallelism": f"independent pairs x{world}",
+                   "l2": f"inputs larger than L2 (per-step state ~{P * 0.052:.1f} GB)",
+                   "inner_iterations_per_step": iters_total,
+                   "epe_vs_ground_truth": round(epe, 5)},
+        "e2e": {"value": world * P * e2e_steps / t_e2e, "unit": "pairs/s",
+                "h2d_bytes_per_step": P * 2 * W * H, "d2h_bytes_per_step": P * 2 * W * H * 4},
+        "gpu_launches": args.steps * launches_per_step,
+        "roofline": {"bound": "hbm", "kernel": "k_tvl1_iter",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None,
+                     "traffic": traffic, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": alg_iter / max(prof["iter_launches"], 1),
+                     "launch_ms_avg": prof["iter_ms"] / max(prof["iter_launches"], 1),
+                     "iter_share_of_step": prof["iter_ms"] / prof["total_ms"]
+                     if prof["total_ms"] else None},
+        "clocks": clocks,
+    }
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=32, help="pairs per GPU per step")
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-pairs", type=int, default=30)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--cpu-worker", action="store_true", help=argparse.SUPPRESS)
+    args = ap.parse_args()
+    if args.cpu_worker:
+        return cpu_worker(args)
+    if args.warmup < 3 and args.impl == "ours":
+        log("warm-up raised to 3 steps")
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        return reference_arm(args, rank)
+    return our_arm(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main() or 0)

@@ -1,0 +1,198 @@
+/*
+ * oflow -- dense optical flow (TV-L1, Horn-Schunck, Lucas-Kanade) on NVIDIA
+ * B200 (sm_100a).  Thin C ABI: plain pointers, sizes and status codes; no
+ * exceptions cross it and nothing in it exits the process.
+ *
+ * Each solver entry point takes two grayscale frames and the solver
+ * parameters and returns a dense flow field (u = horizontal, v = vertical
+ * displacement of a frame-0 pixel into frame 1).  It replaces these
+ * reference interfaces (paths relative to the reference project root):
+ *
+ *   oflow_tvl1      TV_L1::TV_L1 + TV_L1::runDualTVL1Multiscale + TV_L1::getU
+ *                   src/tvl1/sequential/tvl1.hpp:12-17 (uint8 frames) and
+ *                   src/tvl1/cuda/tvl1.cuh:12-20 (float frames, streaming)
+ *   oflow_hs        initFlow / ComputeFlow / deleteFlow_mem
+ *                   src/hs/cuda/flow.cuh:19-33
+ *   oflow_lk        LucasKanade::LucasKanade / copy_frames_circularbuffer_GPU_wrapper
+ *                   / lucas_kanade, src/lk/cuda/lucaskanade.cuh:6-12
+ *   oflow_pyrlk     pyramidal, iterated LK (no reference entry point; built from
+ *                   the steps of src/lk/cuda/kernels/kernels.cu)
+ *
+ * Threading: a context is used by one host thread at a time; contexts are
+ * independent.  Calls are synchronous (they return when the flow is in the
+ * caller's buffers) unless a stream was set with oflow_ctx_set_stream and the
+ * outputs are device buffers, in which case the call returns once the work is
+ * enqueued on that stream.
+ */
+#ifndef OFLOW_H
+#define OFLOW_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OFLOW_ABI_VERSION 1
+#define OFLOW_MAX_SCALES 16
+#define OFLOW_MAX_WARPS 32
+
+typedef enum {
+    OFLOW_OK = 0,
+    OFLOW_ERR_BAD_ARG = 1,     /* invalid sizes, pointers or parameters */
+    OFLOW_ERR_CUDA = 2,        /* CUDA runtime error (message via oflow_ctx_last_error) */
+    OFLOW_ERR_TIMEOUT = 3,     /* a bounded device-side wait gave up */
+    OFLOW_ERR_NO_DEVICE = 4,   /* no usable CUDA device */
+    OFLOW_ERR_OOM = 5,         /* device allocation failed */
+    OFLOW_ERR_UNSUPPORTED = 6  /* valid request outside what this build supports */
+} oflow_status;
+
+typedef enum { OFLOW_U8 = 0, OFLOW_F32 = 1 } oflow_dtype;
+typedef enum { OFLOW_HOST = 0, OFLOW_DEVICE = 1 } oflow_location;
+
+typedef struct oflow_ctx oflow_ctx;
+
+/* A grayscale frame.  pitch is in elements (0 means width). */
+typedef struct {
+    const void *data;
+    int width, height, pitch;
+    int dtype;    /* oflow_dtype */
+    int location; /* oflow_location */
+} oflow_image;
+
+/* Output flow planes, caller-owned.  pitch in elements (0 means width). */
+typedef struct {
+    float *u;
+    float *v;
+    int pitch;
+    int location; /* oflow_location */
+} oflow_flow;
+
+/* ------------------------------------------------------------------ context */
+oflow_status oflow_ctx_create(int device, oflow_ctx **out);
+oflow_status oflow_ctx_destroy(oflow_ctx *ctx);
+/* Run subsequent work on a caller-owned cudaStream_t (NULL: the context's own
+ * stream). */
+oflow_status oflow_ctx_set_stream(oflow_ctx *ctx, void *cuda_stream);
+/* Drop cached plans (device buffers and captured graphs). */
+oflow_status oflow_ctx_trim(oflow_ctx *ctx);
+const char *oflow_ctx_last_error(const oflow_ctx *ctx);
+const char *oflow_status_string(int status);
+int oflow_abi_version(void);
+
+/* ------------------------------------------------------------------- TV-L1 */
+/* Parameters of src/tvl1/sequential/tvl1.hpp:12-14 plus the inner-iteration
+ * cap (tvl1.hpp:6).  Defaults: tau 0.25, lambda 0.15, theta 0.3, nscales 100
+ * (then limited by the image size, tvl1.cpp:42-43), zfactor 0.5, warps 5,
+ * epsilon 0.01, max_iterations 300. */
+typedef struct {
+    float tau, lambda, theta;
+    int nscales;
+    float zfactor;
+    int warps;
+    float epsilon;
+    int max_iterations;
+} oflow_tvl1_params;
+
+/* Per-pair records of one solve.  iterations[s * warps + w] is the number of
+ * inner iterations run at scale s (0 = finest), warp w. */
+typedef struct {
+    int nscales;
+    int warps;
+    int iterations[OFLOW_MAX_SCALES * OFLOW_MAX_WARPS];
+    double energy; /* TV-L1 energy of the result (finest scale, last warp) */
+} oflow_tvl1_stats;
+
+void oflow_tvl1_default_params(oflow_tvl1_params *p);
+
+/* Number of pyramid scales the solver will use for a w x h frame. */
+int oflow_tvl1_nscales(int width, int height, const oflow_tvl1_params *p);
+
+/* One frame pair.  stats may be NULL. */
+oflow_status oflow_tvl1(oflow_ctx *ctx, const oflow_image *I0, const oflow_image *I1,
+                        const oflow_tvl1_params *p, const oflow_flow *out,
+                        oflow_tvl1_stats *stats);
+
+/* n independent pairs in one schedule (sizes may differ).  Arrays of n.
+ * stats may be NULL. */
+oflow_status oflow_tvl1_batch(oflow_ctx *ctx, int n, const oflow_image *I0,
+                              const oflow_image *I1, const oflow_tvl1_params *p,
+                              const oflow_flow *out, oflow_tvl1_stats *stats);
+
+/* Diagnostic form of oflow_tvl1: also records the TV-L1 energy (sum of |grad u|
+ * over both components plus lambda * sum |rho(u)|, rho linearised at the
+ * current warp) after the u update of every inner iteration, at
+ * energy[(s * warps + w) * max_iterations + n]; entries past a stage's early
+ * stop are left untouched.  energy holds nscales*warps*max_iterations doubles.
+ * Slow (one extra reduction per iteration, no graph); for validation. */
+oflow_status oflow_tvl1_energy_trace(oflow_ctx *ctx, const oflow_image *I0,
+                                     const oflow_image *I1, const oflow_tvl1_params *p,
+                                     const oflow_flow *out, oflow_tvl1_stats *stats,
+                                     double *energy);
+
+/* Timing of one solve, measured with CUDA events on the launching stream
+ * around every warp and inner-iteration kernel (eager launches, no graph). */
+typedef struct {
+    double total_ms;       /* whole solve */
+    double iter_ms;        /* sum over inner-iteration launches */
+    double warp_ms;        /* sum over warp (bicubic resampling) launches */
+    int iter_launches;
+    int warp_launches;
+    int launches;          /* all kernel launches of the schedule */
+} oflow_tvl1_profile;
+
+/* Like oflow_tvl1_batch (outputs and stats included) with the timings above. */
+oflow_status oflow_tvl1_batch_profile(oflow_ctx *ctx, int n, const oflow_image *I0,
+                                      const oflow_image *I1, const oflow_tvl1_params *p,
+                                      const oflow_flow *out, oflow_tvl1_stats *stats,
+                                      oflow_tvl1_profile *prof);
+
+/* ------------------------------------------------------------ Horn-Schunck */
+/* Parameters of ComputeFlow (src/hs/cuda/flow.cuh:21-31).  nlevels pyramid
+ * levels (2x2 box downscale), nwarp warps per level, nsolver Jacobi sweeps. */
+typedef struct {
+    float alpha;
+    int nlevels;
+    int nwarp;
+    int nsolver;
+} oflow_hs_params;
+
+void oflow_hs_default_params(oflow_hs_params *p);
+oflow_status oflow_hs(oflow_ctx *ctx, const oflow_image *I0, const oflow_image *I1,
+                      const oflow_hs_params *p, const oflow_flow *out);
+oflow_status oflow_hs_batch(oflow_ctx *ctx, int n, const oflow_image *I0,
+                            const oflow_image *I1, const oflow_hs_params *p,
+                            const oflow_flow *out);
+
+/* ------------------------------------------------------------ Lucas-Kanade */
+/* spac: spatial derivative taps (1,3,5,7,9); temp: temporal taps
+ * (1,2,3,5,7,9); window: odd window side (src/lk/cuda/lucaskanade.cuh:8).
+ * levels/iters are used by oflow_pyrlk only. */
+typedef struct {
+    int spac;
+    int temp;
+    int window;
+    int levels;
+    int iters;
+} oflow_lk_params;
+
+void oflow_lk_default_params(oflow_lk_params *p);
+
+/* Single-step LK over a ring of `temp` uint8 frames: frames[k] is ring slot k,
+ * and the newest frame sits in slot iframe % temp (the reference keeps the
+ * ring on the device and fills slot fr % temp, kernels.cu:6-10).  The spatial
+ * derivatives are taken on the oldest frame of the ring. */
+oflow_status oflow_lk(oflow_ctx *ctx, const oflow_image *frames, int iframe,
+                      const oflow_lk_params *p, const oflow_flow *out);
+
+/* Pyramidal, iterated LK on two frames (levels at scale 0.5, `iters`
+ * warp-and-solve refinements per level, temporal taps (-1, 1)). */
+oflow_status oflow_pyrlk(oflow_ctx *ctx, const oflow_image *I0, const oflow_image *I1,
+                         const oflow_lk_params *p, const oflow_flow *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OFLOW_H */

@@ -76,6 +76,8 @@ def orc_lib():
         lib = C.CDLL(ORACLE_SO)
         lib.orc_gaussian.argtypes = [_f32p, C.c_int, C.c_int, C.c_double]
         lib.orc_gaussian.restype = C.c_int
+        lib.orc_gaussian_window.argtypes = [C.c_double]
+        lib.orc_gaussian_window.restype = C.c_int
         lib.orc_bicubic_at.argtypes = [_f32p, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int]
         lib.orc_bicubic_at.restype = C.c_float
         lib.orc_bicubic_warp.argtypes = [_f32p, _f32p, _f32p, _f32p, C.c_int, C.c_int, C.c_int]

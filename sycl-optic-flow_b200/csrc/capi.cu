@@ -1,0 +1,440 @@
+// The C ABI (include/oflow.h): contexts, plan caches, staging of frames and
+// flows, and the status-code boundary.  Nothing here throws across the ABI or
+// exits the process; CUDA errors come back as OFLOW_ERR_CUDA with the message
+// kept in the context.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <new>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "hs.hpp"
+#include "internal.hpp"
+#include "lk.hpp"
+#include "tvl1.hpp"
+
+using namespace oflow;
+
+namespace oflow {
+
+size_t dtype_size(int dtype) { return dtype == OFLOW_U8 ? 1 : 4; }
+
+void check_image(const oflow_image *img, const char *name) {
+    OF_CHECK(img != nullptr, std::string(name) + ": null image");
+    OF_CHECK(img->data != nullptr, std::string(name) + ": null data pointer");
+    OF_CHECK(img->width > 0 && img->height > 0, std::string(name) + ": empty image");
+    OF_CHECK(img->dtype == OFLOW_U8 || img->dtype == OFLOW_F32, std::string(name) + ": bad dtype");
+    OF_CHECK(img->location == OFLOW_HOST || img->location == OFLOW_DEVICE,
+             std::string(name) + ": bad location");
+    OF_CHECK(img->pitch == 0 || img->pitch >= img->width, std::string(name) + ": pitch < width");
+}
+
+static void check_flow(const oflow_flow *f, int w) {
+    OF_CHECK(f != nullptr && f->u != nullptr && f->v != nullptr, "output: null flow pointer");
+    OF_CHECK(f->location == OFLOW_HOST || f->location == OFLOW_DEVICE, "output: bad location");
+    OF_CHECK(f->pitch == 0 || f->pitch >= w, "output: pitch < width");
+}
+
+void stage_image(const oflow_image &img, void *dst, size_t elem, cudaStream_t s) {
+    const size_t spitch = (size_t)(img.pitch ? img.pitch : img.width) * elem;
+    const size_t row = (size_t)img.width * elem;
+    OF_CUDA(cudaMemcpy2DAsync(dst, row, img.data, spitch, row, img.height,
+                              img.location == OFLOW_HOST ? cudaMemcpyHostToDevice
+                                                         : cudaMemcpyDeviceToDevice,
+                              s));
+}
+
+void unstage_plane(const float *src, int w, int h, float *dst, int pitch, int loc,
+                   cudaStream_t s) {
+    const size_t row = (size_t)w * 4, dpitch = (size_t)(pitch ? pitch : w) * 4;
+    OF_CUDA(cudaMemcpy2DAsync(dst, dpitch, src, row, row, h,
+                              loc == OFLOW_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                              s));
+}
+
+}  // namespace oflow
+
+struct oflow_ctx {
+    int device = 0;
+    cudaStream_t own = nullptr;
+    cudaStream_t user = nullptr;
+    std::string err;
+    std::vector<std::unique_ptr<TvPlan>> tv;
+    std::vector<std::unique_ptr<HsPlan>> hs;
+    std::vector<std::unique_ptr<PyrLkPlan>> pyrlk;
+    std::vector<std::unique_ptr<LkPlan>> lk;
+    cudaStream_t stream() const { return user ? user : own; }
+};
+
+namespace {
+
+constexpr size_t kMaxPlans = 8;
+
+template <typename P> void keep_recent(std::vector<std::unique_ptr<P>> &v) {
+    while (v.size() > kMaxPlans) v.erase(v.begin());
+}
+
+bool same(const oflow_tvl1_params &a, const oflow_tvl1_params &b) {
+    return std::memcmp(&a, &b, sizeof(a)) == 0;
+}
+bool same(const oflow_hs_params &a, const oflow_hs_params &b) {
+    return std::memcmp(&a, &b, sizeof(a)) == 0;
+}
+bool same(const oflow_lk_params &a, const oflow_lk_params &b) {
+    return std::memcmp(&a, &b, sizeof(a)) == 0;
+}
+
+template <typename F> oflow_status guard(oflow_ctx *ctx, F &&f) {
+    try {
+        if (ctx) OF_CUDA(cudaSetDevice(ctx->device));
+        f();
+        if (ctx) ctx->err.clear();
+        return OFLOW_OK;
+    } catch (const Error &e) {
+        if (ctx) ctx->err = e.what();
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        if (ctx) ctx->err = "host allocation failed";
+        return OFLOW_ERR_OOM;
+    } catch (const std::exception &e) {
+        if (ctx) ctx->err = e.what();
+        return OFLOW_ERR_CUDA;
+    } catch (...) {
+        if (ctx) ctx->err = "unknown error";
+        return OFLOW_ERR_CUDA;
+    }
+}
+
+// Synchronous unless the caller supplied a stream and wants device outputs.
+void finish(oflow_ctx *ctx, bool device_only) {
+    if (ctx->user && device_only) return;
+    OF_CUDA(cudaStreamSynchronize(ctx->stream()));
+}
+
+TvPlan &tv_plan(oflow_ctx *ctx, int w, int h, int B, int dtype, const oflow_tvl1_params &p,
+                bool trace) {
+    for (auto &pl : ctx->tv)
+        if (pl->width() == w && pl->height() == h && pl->batch() == B && pl->dtype() == dtype &&
+            pl->traced() == trace && same(pl->params(), p))
+            return *pl;
+    ctx->tv.emplace_back(new TvPlan(w, h, B, dtype, p, trace));
+    keep_recent(ctx->tv);
+    return *ctx->tv.back();
+}
+
+void check_tvl1_params(const oflow_tvl1_params *p) {
+    OF_CHECK(p != nullptr, "tvl1: null params");
+    OF_CHECK(p->nscales >= 1, "tvl1: nscales must be >= 1");
+    OF_CHECK(p->tau > 0 && p->lambda >= 0 && p->theta > 0 && p->epsilon >= 0,
+             "tvl1: tau, theta must be > 0 and lambda, epsilon >= 0");
+}
+
+// Groups the pairs of a batch by (w, h, dtype); each group is one plan.
+struct Group {
+    int w, h, dtype;
+    std::vector<int> idx;
+};
+
+std::vector<Group> group_pairs(int n, const oflow_image *I0, const oflow_image *I1) {
+    std::vector<Group> g;
+    for (int i = 0; i < n; i++) {
+        check_image(&I0[i], "I0");
+        check_image(&I1[i], "I1");
+        OF_CHECK(I0[i].width == I1[i].width && I0[i].height == I1[i].height,
+                 "frames of a pair differ in size");
+        OF_CHECK(I0[i].dtype == I1[i].dtype, "frames of a pair differ in dtype");
+        auto it = std::find_if(g.begin(), g.end(), [&](const Group &x) {
+            return x.w == I0[i].width && x.h == I0[i].height && x.dtype == I0[i].dtype;
+        });
+        if (it == g.end()) {
+            g.push_back({I0[i].width, I0[i].height, I0[i].dtype, {}});
+            it = g.end() - 1;
+        }
+        it->idx.push_back(i);
+    }
+    return g;
+}
+
+void run_tvl1(oflow_ctx *ctx, int n, const oflow_image *I0, const oflow_image *I1,
+              const oflow_tvl1_params *p, const oflow_flow *out, oflow_tvl1_stats *stats,
+              double *energy_trace, oflow_tvl1_profile *prof = nullptr) {
+    OF_CHECK(ctx != nullptr, "null context");
+    OF_CHECK(n >= 1 && I0 && I1 && out, "tvl1: empty batch or null arrays");
+    check_tvl1_params(p);
+    for (int i = 0; i < n; i++) check_flow(&out[i], I0[i].width);
+    const cudaStream_t st = ctx->stream();
+    bool device_only = stats == nullptr && energy_trace == nullptr && prof == nullptr;
+    const std::vector<Group> groups = group_pairs(n, I0, I1);
+    OF_CHECK(prof == nullptr || groups.size() == 1, "tvl1 profile: pairs must share one size");
+    for (const Group &g : groups) {
+        TvPlan &pl = tv_plan(ctx, g.w, g.h, (int)g.idx.size(), g.dtype, *p, energy_trace != nullptr);
+        for (size_t b = 0; b < g.idx.size(); b++) {
+            stage_image(I0[g.idx[b]], pl.raw_input((int)b, 0), dtype_size(g.dtype), st);
+            stage_image(I1[g.idx[b]], pl.raw_input((int)b, 1), dtype_size(g.dtype), st);
+        }
+        if (prof)
+            pl.profile(st, prof);
+        else if (energy_trace)
+            pl.record(st);
+        else
+            pl.run(st);
+        for (size_t b = 0; b < g.idx.size(); b++) {
+            const oflow_flow &o = out[g.idx[b]];
+            unstage_plane(pl.out_u((int)b), g.w, g.h, o.u, o.pitch, o.location, st);
+            unstage_plane(pl.out_v((int)b), g.w, g.h, o.v, o.pitch, o.location, st);
+            if (o.location == OFLOW_HOST) device_only = false;
+            if (stats) pl.read_stats((int)b, &stats[g.idx[b]], st);
+        }
+        if (energy_trace) pl.read_energy_trace(0, energy_trace, st);
+    }
+    finish(ctx, device_only);
+}
+
+}  // namespace
+
+extern "C" {
+
+int oflow_abi_version(void) { return OFLOW_ABI_VERSION; }
+
+const char *oflow_status_string(int s) {
+    switch (s) {
+        case OFLOW_OK: return "ok";
+        case OFLOW_ERR_BAD_ARG: return "bad argument";
+        case OFLOW_ERR_CUDA: return "CUDA error";
+        case OFLOW_ERR_TIMEOUT: return "device wait timed out";
+        case OFLOW_ERR_NO_DEVICE: return "no CUDA device";
+        case OFLOW_ERR_OOM: return "out of memory";
+        case OFLOW_ERR_UNSUPPORTED: return "unsupported";
+        default: return "unknown status";
+    }
+}
+
+oflow_status oflow_ctx_create(int device, oflow_ctx **out) {
+    if (!out) return OFLOW_ERR_BAD_ARG;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return OFLOW_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= count) return OFLOW_ERR_BAD_ARG;
+    oflow_ctx *ctx = new (std::nothrow) oflow_ctx();
+    if (!ctx) return OFLOW_ERR_OOM;
+    ctx->device = device;
+    const oflow_status s = guard(ctx, [&] {
+        OF_CUDA(cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking));
+    });
+    if (s != OFLOW_OK) {
+        delete ctx;
+        return s;
+    }
+    *out = ctx;
+    return OFLOW_OK;
+}
+
+oflow_status oflow_ctx_destroy(oflow_ctx *ctx) {
+    if (!ctx) return OFLOW_ERR_BAD_ARG;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream());
+    ctx->tv.clear();
+    ctx->hs.clear();
+    ctx->pyrlk.clear();
+    ctx->lk.clear();
+    if (ctx->own) cudaStreamDestroy(ctx->own);
+    delete ctx;
+    return OFLOW_OK;
+}
+
+oflow_status oflow_ctx_set_stream(oflow_ctx *ctx, void *stream) {
+    if (!ctx) return OFLOW_ERR_BAD_ARG;
+    ctx->user = static_cast<cudaStream_t>(stream);
+    return OFLOW_OK;
+}
+
+oflow_status oflow_ctx_trim(oflow_ctx *ctx) {
+    if (!ctx) return OFLOW_ERR_BAD_ARG;
+    return guard(ctx, [&] {
+        OF_CUDA(cudaStreamSynchronize(ctx->stream()));
+        ctx->tv.clear();
+        ctx->hs.clear();
+        ctx->pyrlk.clear();
+        ctx->lk.clear();
+    });
+}
+
+const char *oflow_ctx_last_error(const oflow_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+void oflow_tvl1_default_params(oflow_tvl1_params *p) {
+    if (!p) return;
+    p->tau = 0.25f;
+    p->lambda = 0.15f;
+    p->theta = 0.3f;
+    p->nscales = 100;
+    p->zfactor = 0.5f;
+    p->warps = 5;
+    p->epsilon = 0.01f;
+    p->max_iterations = 300;
+}
+
+int oflow_tvl1_nscales(int w, int h, const oflow_tvl1_params *p) {
+    if (!p || w <= 0 || h <= 0 || !(p->zfactor > 0.0f && p->zfactor < 1.0f)) return -1;
+    return tvl1_nscales(w, h, p->nscales, p->zfactor);
+}
+
+oflow_status oflow_tvl1(oflow_ctx *ctx, const oflow_image *I0, const oflow_image *I1,
+                        const oflow_tvl1_params *p, const oflow_flow *out,
+                        oflow_tvl1_stats *stats) {
+    return guard(ctx, [&] { run_tvl1(ctx, 1, I0, I1, p, out, stats, nullptr); });
+}
+
+oflow_status oflow_tvl1_batch(oflow_ctx *ctx, int n, const oflow_image *I0,
+                              const oflow_image *I1, const oflow_tvl1_params *p,
+                              const oflow_flow *out, oflow_tvl1_stats *stats) {
+    return guard(ctx, [&] { run_tvl1(ctx, n, I0, I1, p, out, stats, nullptr); });
+}
+
+oflow_status oflow_tvl1_batch_profile(oflow_ctx *ctx, int n, const oflow_image *I0,
+                                      const oflow_image *I1, const oflow_tvl1_params *p,
+                                      const oflow_flow *out, oflow_tvl1_stats *stats,
+                                      oflow_tvl1_profile *prof) {
+    return guard(ctx, [&] {
+        OF_CHECK(prof != nullptr, "tvl1 profile: null profile");
+        run_tvl1(ctx, n, I0, I1, p, out, stats, nullptr, prof);
+    });
+}
+
+oflow_status oflow_tvl1_energy_trace(oflow_ctx *ctx, const oflow_image *I0,
+                                     const oflow_image *I1, const oflow_tvl1_params *p,
+                                     const oflow_flow *out, oflow_tvl1_stats *stats,
+                                     double *energy) {
+    return guard(ctx, [&] {
+        OF_CHECK(energy != nullptr, "tvl1 trace: null energy buffer");
+        run_tvl1(ctx, 1, I0, I1, p, out, stats, energy);
+    });
+}
+
+void oflow_hs_default_params(oflow_hs_params *p) {
+    if (!p) return;
+    p->alpha = 0.2f;
+    p->nlevels = 5;
+    p->nwarp = 3;
+    p->nsolver = 150;
+}
+
+oflow_status oflow_hs_batch(oflow_ctx *ctx, int n, const oflow_image *I0,
+                            const oflow_image *I1, const oflow_hs_params *p,
+                            const oflow_flow *out) {
+    return guard(ctx, [&] {
+        OF_CHECK(ctx != nullptr, "null context");
+        OF_CHECK(n >= 1 && I0 && I1 && out && p, "hs: empty batch or null arrays");
+        for (int i = 0; i < n; i++) check_flow(&out[i], I0[i].width);
+        const cudaStream_t st = ctx->stream();
+        bool device_only = true;
+        for (const Group &g : group_pairs(n, I0, I1)) {
+            HsPlan *pl = nullptr;
+            for (auto &q : ctx->hs)
+                if (q->width() == g.w && q->height() == g.h && q->batch() == (int)g.idx.size() &&
+                    q->dtype() == g.dtype && same(q->params(), *p))
+                    pl = q.get();
+            if (!pl) {
+                ctx->hs.emplace_back(new HsPlan(g.w, g.h, (int)g.idx.size(), g.dtype, *p));
+                pl = ctx->hs.back().get();
+                keep_recent(ctx->hs);
+                pl = ctx->hs.back().get();
+            }
+            for (size_t b = 0; b < g.idx.size(); b++) {
+                stage_image(I0[g.idx[b]], pl->raw_input((int)b, 0), dtype_size(g.dtype), st);
+                stage_image(I1[g.idx[b]], pl->raw_input((int)b, 1), dtype_size(g.dtype), st);
+            }
+            pl->run(st);
+            for (size_t b = 0; b < g.idx.size(); b++) {
+                const oflow_flow &o = out[g.idx[b]];
+                unstage_plane(pl->out_u((int)b), g.w, g.h, o.u, o.pitch, o.location, st);
+                unstage_plane(pl->out_v((int)b), g.w, g.h, o.v, o.pitch, o.location, st);
+                if (o.location == OFLOW_HOST) device_only = false;
+            }
+        }
+        finish(ctx, device_only);
+    });
+}
+
+oflow_status oflow_hs(oflow_ctx *ctx, const oflow_image *I0, const oflow_image *I1,
+                      const oflow_hs_params *p, const oflow_flow *out) {
+    return oflow_hs_batch(ctx, 1, I0, I1, p, out);
+}
+
+void oflow_lk_default_params(oflow_lk_params *p) {
+    if (!p) return;
+    p->spac = 3;
+    p->temp = 2;
+    p->window = 5;
+    p->levels = 3;
+    p->iters = 3;
+}
+
+oflow_status oflow_lk(oflow_ctx *ctx, const oflow_image *frames, int iframe,
+                      const oflow_lk_params *p, const oflow_flow *out) {
+    return guard(ctx, [&] {
+        OF_CHECK(ctx != nullptr && frames != nullptr && p != nullptr, "lk: null argument");
+        OF_CHECK(iframe >= 0, "lk: iframe < 0");
+        const int T = p->temp;
+        OF_CHECK(T >= 1 && T <= 9, "lk: temporal filter size out of range");
+        for (int k = 0; k < T; k++) {
+            check_image(&frames[k], "frame");
+            OF_CHECK(frames[k].dtype == OFLOW_U8, "lk: ring frames must be uint8");
+            OF_CHECK(frames[k].width == frames[0].width && frames[k].height == frames[0].height,
+                     "lk: ring frames differ in size");
+        }
+        const int w = frames[0].width, h = frames[0].height;
+        check_flow(out, w);
+        LkPlan *pl = nullptr;
+        for (auto &q : ctx->lk)
+            if (q->width() == w && q->height() == h && same(q->params(), *p)) pl = q.get();
+        if (!pl) {
+            ctx->lk.emplace_back(new LkPlan(w, h, *p));
+            keep_recent(ctx->lk);
+            pl = ctx->lk.back().get();
+        }
+        const cudaStream_t st = ctx->stream();
+        for (int k = 0; k < T; k++) stage_image(frames[k], pl->ring_slot(k), 1, st);
+        pl->run(iframe, st);
+        unstage_plane(pl->out_u(), w, h, out->u, out->pitch, out->location, st);
+        unstage_plane(pl->out_v(), w, h, out->v, out->pitch, out->location, st);
+        finish(ctx, out->location == OFLOW_DEVICE);
+    });
+}
+
+oflow_status oflow_pyrlk(oflow_ctx *ctx, const oflow_image *I0, const oflow_image *I1,
+                         const oflow_lk_params *p, const oflow_flow *out) {
+    return guard(ctx, [&] {
+        OF_CHECK(ctx != nullptr && p != nullptr, "pyrlk: null argument");
+        OF_CHECK(p->temp == 2, "pyrlk: temporal filter must be the 2-tap difference");
+        check_flow(out, I0 ? I0->width : 0);
+        const cudaStream_t st = ctx->stream();
+        for (const Group &g : group_pairs(1, I0, I1)) {
+            PyrLkPlan *pl = nullptr;
+            for (auto &q : ctx->pyrlk)
+                if (q->width() == g.w && q->height() == g.h && q->batch() == 1 &&
+                    q->dtype() == g.dtype && same(q->params(), *p))
+                    pl = q.get();
+            if (!pl) {
+                ctx->pyrlk.emplace_back(new PyrLkPlan(g.w, g.h, 1, g.dtype, *p));
+                keep_recent(ctx->pyrlk);
+                pl = ctx->pyrlk.back().get();
+            }
+            stage_image(*I0, pl->raw_input(0, 0), dtype_size(g.dtype), st);
+            stage_image(*I1, pl->raw_input(0, 1), dtype_size(g.dtype), st);
+            pl->run(st);
+            unstage_plane(pl->out_u(0), g.w, g.h, out->u, out->pitch, out->location, st);
+            unstage_plane(pl->out_v(0), g.w, g.h, out->v, out->pitch, out->location, st);
+        }
+        finish(ctx, out->location == OFLOW_DEVICE);
+    });
+}
+
+}  // extern "C"

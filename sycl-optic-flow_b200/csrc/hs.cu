@@ -1,0 +1,322 @@
+// Horn-Schunck on B200: kernels and the batched plan.  Restates
+// src/hs/cuda/flow.cu:112-208 and src/hs/cuda/kernels/*.cuh with the
+// semantics those kernels are written for (bilinear clamp-to-edge warp and
+// upscale, clamped derivative taps, every pixel written); the arithmetic
+// contract is in common.cuh.
+//
+// Layout per pair b (N = w*h at the finest level, levels packed):
+//   raw[b][2] staged frames, pyr_l[b][2] float pyramid (finest = nlevels-1),
+//   D[b] float4 (Ix, Iy, Iz, Ix^2+Iy^2+alpha), dU0/dU1[b] float2 ping-pong
+//   increments, Ua/Ub[b] float2 flow (alternating per level), out[2][b].
+// All ping-pong parities are known on the host, so the schedule is static and
+// captured into one CUDA graph.
+//
+// The Jacobi sweeps are temporally blocked: one launch runs up to K sweeps on
+// a TW x TH tile held in shared memory with a K-pixel halo; the halo shrinks
+// by one pixel per sweep, so after K sweeps the owned tile is exact (clamped
+// neighbours at the image border are exact at every sweep).
+#include "common.cuh"
+#include "hs.hpp"
+#include "internal.hpp"
+
+namespace oflow {
+
+template <typename In>
+__global__ void k_hs_ingest(const In *__restrict__ raw, float *dst, int N, int planes) {
+    const size_t total = (size_t)N * planes;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = (float)raw[i];
+}
+
+// 2x2 box average (downscaleKernel.cuh:27-29), every output pixel written.
+__global__ void k_hs_downscale(const float *__restrict__ src, size_t sstride, int w, int h,
+                               float *dst, size_t dstride) {
+    const int nw = w / 2, nh = h / 2;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= nw || y >= nh) return;
+    const float *s = src + (size_t)blockIdx.z * sstride + (size_t)(2 * y) * w + 2 * x;
+    dst[(size_t)blockIdx.z * dstride + (size_t)y * nw + x] = 0.25f * (s[0] + s[w] + s[1] + s[w + 1]);
+}
+
+__device__ __forceinline__ float hs_deriv5(float m2, float m1, float p1, float p2) {
+    float t = m2;
+    t -= m1 * 8.0f;
+    t += p1 * 8.0f;
+    t -= p2;
+    t /= 12.0f;
+    return t;
+}
+
+// Fused warp + derivatives (warpingKernel.cuh:28-44, derivativesKernel.cuh:
+// 29-73).  The tile plus a 2-pixel halo is filled with values at clamped
+// image coordinates, so a derivative tap at offset k reads the clamped
+// neighbour directly.
+constexpr int kDTW = 32, kDTH = 8;
+__global__ void __launch_bounds__(kDTW *kDTH) k_hs_warp_deriv(
+    const float *__restrict__ pyr, size_t lp, int w, int h, const float2 *__restrict__ U,
+    size_t ustride, int zero_flow, float alpha, float4 *D, size_t dstride) {
+    constexpr int RW = kDTW + 4, RH = kDTH + 4;
+    __shared__ float s0[RH * RW], s1[RH * RW];
+    const int b = blockIdx.z;
+    const float *I0 = pyr + (size_t)(2 * b) * lp;
+    const float *I1 = pyr + (size_t)(2 * b + 1) * lp;
+    const float2 *Ub = U + (size_t)b * ustride;
+    const int x0 = blockIdx.x * kDTW - 2, y0 = blockIdx.y * kDTH - 2;
+    const int tid = threadIdx.y * kDTW + threadIdx.x;
+    for (int i = tid; i < RW * RH; i += kDTW * kDTH) {
+        const int cx = imin(imax(x0 + i % RW, 0), w - 1);
+        const int cy = imin(imax(y0 + i / RW, 0), h - 1);
+        const size_t p = (size_t)cy * w + cx;
+        s0[i] = __ldg(I0 + p);
+        const float2 u = zero_flow ? make_float2(0.f, 0.f) : Ub[p];
+        s1[i] = bilinear_clamped(I1, w, h, (float)cx + u.x, (float)cy + u.y);
+    }
+    __syncthreads();
+    const int x = blockIdx.x * kDTW + threadIdx.x, y = blockIdx.y * kDTH + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const int c = (threadIdx.y + 2) * RW + threadIdx.x + 2;
+    float t0 = hs_deriv5(s0[c - 2], s0[c - 1], s0[c + 1], s0[c + 2]);
+    float t1 = hs_deriv5(s1[c - 2], s1[c - 1], s1[c + 1], s1[c + 2]);
+    const float Ix = (t0 + t1) * 0.5f;
+    const float Iz = s1[c] - s0[c];
+    t0 = hs_deriv5(s0[c - 2 * RW], s0[c - RW], s0[c + RW], s0[c + 2 * RW]);
+    t1 = hs_deriv5(s1[c - 2 * RW], s1[c - RW], s1[c + RW], s1[c + 2 * RW]);
+    const float Iy = (t0 + t1) * 0.5f;
+    const float den = Ix * Ix + Iy * Iy + alpha;
+    D[(size_t)b * dstride + (size_t)y * w + x] = make_float4(Ix, Iy, Iz, den);
+}
+
+// K Jacobi sweeps (solverKernel.cuh:41-153) on a tile with a KH-pixel halo.
+// sweeps <= KH.  first: increments start at 0 (flow.cu:168-171).  last: add
+// the increment to the flow (AddKernel, addKernel.cuh:28-36) instead of
+// storing it.
+template <int TW, int TH, int KH, int NT>
+__global__ void __launch_bounds__(NT) k_hs_jacobi(const float4 *__restrict__ D, size_t dstride,
+                                                  const float2 *__restrict__ dUin,
+                                                  float2 *dUout, float2 *U, size_t stride,
+                                                  int w, int h, int sweeps, int first, int last) {
+    constexpr int RW = TW + 2 * KH, RH = TH + 2 * KH, RN = RW * RH;
+    extern __shared__ float4 smem[];
+    float4 *sD = smem;                                   // RN
+    float2 *sA = reinterpret_cast<float2 *>(sD + RN);    // RN
+    float2 *sB = sA + RN;                                // RN
+    const int b = blockIdx.z;
+    const float4 *Db = D + (size_t)b * dstride;
+    const float2 *In = dUin + (size_t)b * stride;
+    const int x0 = blockIdx.x * TW - KH, y0 = blockIdx.y * TH - KH;
+    for (int i = threadIdx.x; i < RN; i += NT) {
+        const int x = x0 + i % RW, y = y0 + i / RW;
+        float4 d = make_float4(0.f, 0.f, 0.f, 1.f);
+        float2 a = make_float2(0.f, 0.f);
+        if (x >= 0 && x < w && y >= 0 && y < h) {
+            const size_t p = (size_t)y * w + x;
+            d = Db[p];
+            if (!first) a = In[p];
+        }
+        sD[i] = d;
+        sA[i] = a;
+    }
+    __syncthreads();
+    float2 *src = sA, *dst = sB;
+    for (int s = 0; s < sweeps; s++) {
+        for (int i = threadIdx.x; i < RN; i += NT) {
+            const int rx = i % RW, ry = i / RW;
+            const int x = x0 + rx, y = y0 + ry;
+            if (x < 0 || x >= w || y < 0 || y >= h) continue;
+            // clamped image neighbours; at the tile-region edge (not the image
+            // edge) the value is stale but never reaches the owned tile
+            const int l = (x > 0 && rx > 0) ? i - 1 : i;
+            const int r = (x < w - 1 && rx < RW - 1) ? i + 1 : i;
+            const int up = (y < h - 1 && ry < RH - 1) ? i + RW : i;
+            const int dn = (y > 0 && ry > 0) ? i - RW : i;
+            const float2 al = src[l], ar = src[r], au = src[up], ad = src[dn];
+            const float su = (al.x + ar.x + au.x + ad.x) * 0.25f;
+            const float sv = (al.y + ar.y + au.y + ad.y) * 0.25f;
+            const float4 d = sD[i];
+            const float frac = (d.x * su + d.y * sv + d.z) / d.w;
+            dst[i] = make_float2(su - d.x * frac, sv - d.y * frac);
+        }
+        __syncthreads();
+        float2 *t = src;
+        src = dst;
+        dst = t;
+    }
+    for (int i = threadIdx.x; i < TW * TH; i += NT) {
+        const int tx = i % TW, ty = i / TW;
+        const int x = x0 + KH + tx, y = y0 + KH + ty;
+        if (x >= w || y >= h) continue;
+        const float2 a = src[(ty + KH) * RW + tx + KH];
+        const size_t p = (size_t)b * stride + (size_t)y * w + x;
+        if (last) {
+            const float2 u = U[p];
+            U[p] = make_float2(u.x + a.x, u.y + a.y);
+        } else {
+            dUout[p] = a;
+        }
+    }
+}
+
+// Flow prolongation (upscaleKernel.cuh:26-40 as a filtering upscale):
+// bilinear, clamp-to-edge, centre-aligned, component-wise scale.
+__device__ __forceinline__ float2 bilinear2(const float2 *__restrict__ src, int w, int h,
+                                            float xf, float yf) {
+    xf = fminf(fmaxf(xf, -1.0f), (float)w);
+    yf = fminf(fmaxf(yf, -1.0f), (float)h);
+    const float x0f = floorf(xf), y0f = floorf(yf);
+    const float fx = xf - x0f, fy = yf - y0f;
+    const int x0 = (int)x0f, y0 = (int)y0f;
+    const int xa = imin(imax(x0, 0), w - 1), xb = imin(imax(x0 + 1, 0), w - 1);
+    const int ya = imin(imax(y0, 0), h - 1), yb = imin(imax(y0 + 1, 0), h - 1);
+    const float2 v00 = src[(size_t)ya * w + xa], v10 = src[(size_t)ya * w + xb];
+    const float2 v01 = src[(size_t)yb * w + xa], v11 = src[(size_t)yb * w + xb];
+    const float gx = 1.0f - fx, gy = 1.0f - fy;
+    float2 r;
+    float top = gx * v00.x + fx * v10.x, bot = gx * v01.x + fx * v11.x;
+    r.x = gy * top + fy * bot;
+    top = gx * v00.y + fx * v10.y;
+    bot = gx * v01.y + fx * v11.y;
+    r.y = gy * top + fy * bot;
+    return r;
+}
+
+__global__ void k_upscale2(const float2 *__restrict__ src, size_t sstride, int w, int h,
+                           float2 *dst, size_t dstride, int nw, int nh, float sx, float sy) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= nw || y >= nh) return;
+    const float rx = (float)w / (float)nw, ry = (float)h / (float)nh;
+    const float fx = ((float)x + 0.5f) * rx - 0.5f;
+    const float fy = ((float)y + 0.5f) * ry - 0.5f;
+    const float2 r = bilinear2(src + (size_t)blockIdx.z * sstride, w, h, fx, fy);
+    dst[(size_t)blockIdx.z * dstride + (size_t)y * nw + x] = make_float2(r.x * sx, r.y * sy);
+}
+
+__global__ void k_split2(const float2 *__restrict__ U, size_t stride, int N, float *ou, float *ov,
+                         int B) {
+    const int b = blockIdx.y;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const float2 u = U[(size_t)b * stride + i];
+        ou[(size_t)b * N + i] = u.x;  // ov already points at the v planes
+        ov[(size_t)b * N + i] = u.y;
+    }
+}
+
+void launch_upscale2(const float2 *src, size_t sstride, int w, int h, float2 *dst,
+                     size_t dstride, int nw, int nh, float sx, float sy, int B,
+                     cudaStream_t st) {
+    dim3 blk(32, 8), g(div_up(nw, 32), div_up(nh, 8), B);
+    k_upscale2<<<g, blk, 0, st>>>(src, sstride, w, h, dst, dstride, nw, nh, sx, sy);
+}
+
+void launch_split2(const float2 *U, size_t stride, int N, float *out, int B, cudaStream_t st) {
+    k_split2<<<dim3(imin(div_up(N, 1024), 1024), B), 256, 0, st>>>(U, stride, N, out,
+                                                                   out + (size_t)B * N, B);
+}
+
+// ================================================================ host plan
+constexpr int kJTW = 32, kJTH = 16, kJK = 4, kJNT = 256;
+
+HsPlan::HsPlan(int w, int h, int B, int dtype, const oflow_hs_params &prm)
+    : w_(w), h_(h), B_(B), dtype_(dtype), prm_(prm) {
+    OF_CHECK(B >= 1, "hs: empty batch");
+    OF_CHECK(prm.nlevels >= 1 && prm.nlevels <= 16, "hs: nlevels out of range");
+    OF_CHECK(prm.nwarp >= 0 && prm.nsolver >= 0, "hs: negative iteration count");
+    L_ = prm.nlevels;
+    W_[L_ - 1] = w;
+    H_[L_ - 1] = h;
+    for (int l = L_ - 1; l > 0; l--) {
+        W_[l - 1] = W_[l] / 2;
+        H_[l - 1] = H_[l] / 2;
+    }
+    OF_CHECK(W_[0] >= 1 && H_[0] >= 1, "hs: too many levels for the frame size");
+    N_ = (size_t)w * h;
+    size_t acc = 0;
+    for (int l = 0; l < L_; l++) {
+        pyr_off_[l] = acc;
+        acc += (size_t)2 * B * W_[l] * H_[l];
+    }
+    const size_t esz = dtype == OFLOW_U8 ? 1 : 4;
+    o_raw_ = ar_.reserve(2 * B * N_ * esz);
+    o_pyr_ = ar_.reserve(acc * 4);
+    o_D_ = ar_.reserve(B * N_ * 16);
+    o_dU0_ = ar_.reserve(B * N_ * 8);
+    o_dU1_ = ar_.reserve(B * N_ * 8);
+    o_Ua_ = ar_.reserve(B * N_ * 8);
+    o_Ub_ = ar_.reserve(B * N_ * 8);
+    o_out_ = ar_.reserve(2 * B * N_ * 4);
+    ar_.commit();
+    OF_CUDA(cudaFuncSetAttribute(k_hs_jacobi<kJTW, kJTH, kJK, kJNT>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (kJTW + 2 * kJK) * (kJTH + 2 * kJK) * 32));
+}
+
+void *HsPlan::raw_input(int b, int k) const {
+    const size_t esz = dtype_ == OFLOW_U8 ? 1 : 4;
+    return ar_.at<char>(o_raw_) + (size_t)(2 * b + k) * N_ * esz;
+}
+const float *HsPlan::out_u(int b) const { return ar_.at<float>(o_out_) + (size_t)b * N_; }
+const float *HsPlan::out_v(int b) const { return ar_.at<float>(o_out_) + (size_t)(B_ + b) * N_; }
+
+void HsPlan::record(cudaStream_t st) {
+    const int B = B_;
+    float *pyr = ar_.at<float>(o_pyr_);
+    float4 *D = ar_.at<float4>(o_D_);
+    float2 *dU[2] = {ar_.at<float2>(o_dU0_), ar_.at<float2>(o_dU1_)};
+    float2 *Ubuf[2] = {ar_.at<float2>(o_Ua_), ar_.at<float2>(o_Ub_)};
+    const int top = L_ - 1;
+    {
+        const int nb = imin(div_up((int)(2 * B * N_), 1024), 4096);
+        if (dtype_ == OFLOW_U8)
+            k_hs_ingest<uint8_t><<<nb, 256, 0, st>>>(ar_.at<uint8_t>(o_raw_), pyr + pyr_off_[top],
+                                                     (int)N_, 2 * B);
+        else
+            k_hs_ingest<float><<<nb, 256, 0, st>>>(ar_.at<float>(o_raw_), pyr + pyr_off_[top],
+                                                   (int)N_, 2 * B);
+    }
+    for (int l = top; l > 0; l--) {
+        dim3 blk(32, 8), g(div_up(W_[l - 1], 32), div_up(H_[l - 1], 8), 2 * B);
+        k_hs_downscale<<<g, blk, 0, st>>>(pyr + pyr_off_[l], (size_t)W_[l] * H_[l], W_[l], H_[l],
+                                          pyr + pyr_off_[l - 1], (size_t)W_[l - 1] * H_[l - 1]);
+    }
+    int ub = 0;  // Ubuf index holding the flow of the current level
+    OF_CUDA(cudaMemsetAsync(Ubuf[ub], 0, B * N_ * 8, st));
+    const size_t smem = (size_t)(kJTW + 2 * kJK) * (kJTH + 2 * kJK) * 32;
+    for (int l = 0; l < L_; l++) {
+        const int lw = W_[l], lh = H_[l];
+        const size_t lp = (size_t)lw * lh;
+        for (int wi = 0; wi < prm_.nwarp; wi++) {
+            dim3 dg(div_up(lw, kDTW), div_up(lh, kDTH), B);
+            k_hs_warp_deriv<<<dg, dim3(kDTW, kDTH), 0, st>>>(pyr + pyr_off_[l], lp, lw, lh,
+                                                             Ubuf[ub], N_, 0, prm_.alpha, D, N_);
+            dim3 jg(div_up(lw, kJTW), div_up(lh, kJTH), B);
+            int done = 0, cur = 0;
+            if (prm_.nsolver == 0) continue;  // du = 0: the flow is unchanged
+            while (done < prm_.nsolver) {
+                const int k = imin(kJK, prm_.nsolver - done);
+                const bool first = done == 0, last = done + k == prm_.nsolver;
+                k_hs_jacobi<kJTW, kJTH, kJK, kJNT><<<jg, kJNT, smem, st>>>(
+                    D, N_, dU[cur], dU[cur ^ 1], Ubuf[ub], N_, lw, lh, k, first, last);
+                cur ^= 1;
+                done += k;
+            }
+        }
+        if (l != top) {
+            const float sx = (float)W_[l + 1] / (float)lw;
+            const float sy = (float)H_[l + 1] / (float)lh;
+            launch_upscale2(Ubuf[ub], N_, lw, lh, Ubuf[ub ^ 1], N_, W_[l + 1], H_[l + 1], sx, sy, B,
+                            st);
+            ub ^= 1;
+        }
+    }
+    launch_split2(Ubuf[ub], N_, (int)N_, ar_.at<float>(o_out_), B, st);
+    OF_CUDA(cudaGetLastError());
+}
+
+void HsPlan::run(cudaStream_t st) {
+    if (!graph_.ready()) graph_.capture(st, [&](cudaStream_t s) { record(s); });
+    graph_.launch(st);
+}
+
+}  // namespace oflow

@@ -1,0 +1,40 @@
+// Batched Horn-Schunck plan (B equal-size pairs, one captured schedule).
+#pragma once
+
+#include "internal.hpp"
+
+namespace oflow {
+
+class HsPlan {
+  public:
+    HsPlan(int w, int h, int B, int dtype, const oflow_hs_params &prm);
+    void *raw_input(int b, int k) const;
+    const float *out_u(int b) const;
+    const float *out_v(int b) const;
+    void run(cudaStream_t st);
+    void record(cudaStream_t st);
+    int width() const { return w_; }
+    int height() const { return h_; }
+    int batch() const { return B_; }
+    int dtype() const { return dtype_; }
+    const oflow_hs_params &params() const { return prm_; }
+
+  private:
+    int w_, h_, B_, dtype_;
+    oflow_hs_params prm_;
+    int L_ = 0;
+    int W_[16] = {}, H_[16] = {};
+    size_t pyr_off_[16] = {};
+    size_t N_ = 0;
+    Arena ar_;
+    size_t o_raw_ = 0, o_pyr_ = 0, o_D_ = 0, o_dU0_ = 0, o_dU1_ = 0, o_Ua_ = 0, o_Ub_ = 0,
+           o_out_ = 0;
+    Graph graph_;
+};
+
+// Shared with the pyramidal LK plan.
+void launch_upscale2(const float2 *src, size_t sstride, int w, int h, float2 *dst,
+                     size_t dstride, int nw, int nh, float sx, float sy, int B, cudaStream_t st);
+void launch_split2(const float2 *U, size_t stride, int N, float *out, int B, cudaStream_t st);
+
+}  // namespace oflow

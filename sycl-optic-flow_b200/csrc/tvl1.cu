@@ -1,0 +1,835 @@
+// TV-L1 (Zach-Pock-Bischof duality TV-L1) on B200: kernels and the batched
+// plan.  Follows src/tvl1/sequential/tvl1.cpp and its helpers (mask/, zoom/,
+// bicubic_interpolation/) operation for operation; the arithmetic contract is
+// in common.cuh (no FMA, IEEE division, double where the reference uses double
+// literals).
+//
+// Data layout in HBM (per pair b of a plan of B equal-size pairs, N0 = w*h):
+//   raw[b][2]      staged input frames (u8 or f32)
+//   T[b][2]        float scratch planes (ingest output, blur output)
+//   pyr_s[b][2]    pyramid level s of I0 / I1, dense nx_s*ny_s
+//   I1g[b]         float4 (I1, I1x, I1y, 0) of the current level
+//   W[b]           float4 (I1wx, I1wy, rho_c, |grad I1w|^2) of the current warp
+//   U0/U1[b]       float2 (u1, u2) ping-pong; Uz[b] upsampled flow
+//   P0/P1[b]       float4 (p11, p12, p21, p22) ping-pong
+// Level planes are packed at the start of their level-0-sized buffers.
+//
+// Control: one TvCtrl per pair on the device.  The inner-iteration kernel is
+// launched max_iterations times per warp; its last block to finish reduces the
+// squared change in a fixed order, flips the ping-pong index and sets `stop`
+// once error <= epsilon^2 (tvl1.cpp:216), after which later launches of that
+// warp return at once.  The host never synchronises inside a solve, so the
+// whole schedule is captured into one CUDA graph.
+#include "common.cuh"
+#include "internal.hpp"
+#include "tvl1.hpp"
+
+#include <cmath>
+#include <cstring>
+
+namespace oflow {
+
+// ---------------------------------------------------------------- constants
+constexpr int kIterTW = 32, kIterTH = 8, kIterNT = 256;
+constexpr int kGaussTW = 32, kGaussTH = 16, kGaussNT = 256, kGaussMaxR = 15;
+constexpr int kIngestNT = 256, kIngestPPT = 8;
+
+// Half-kernel of mask.cpp:225-244 in double on the host.
+static GaussTaps make_taps(double sigma) {
+    GaussTaps t{};
+    const double den = 2 * sigma * sigma;
+    const double spi = sigma * std::sqrt(M_PI * 2);
+    t.size = (int)(5.0 * sigma) + 1;
+    if (t.size > kGaussMaxR + 1) throw Error(OFLOW_ERR_UNSUPPORTED, "Gaussian sigma too large");
+    for (int i = 0; i < t.size; i++) t.B[i] = 1 / spi * std::exp(-i * i / den);
+    double norm = 0.0;
+    for (int i = 0; i < t.size; i++) norm += std::fabs(t.B[i]);
+    norm = norm * 2 - t.B[0];
+    const double s = 1 / norm;
+    for (int i = 0; i < t.size; i++) t.B[i] = s * t.B[i];
+    return t;
+}
+
+static float zoom_sigma(float zfactor) {
+    return (float)(0.6f * std::sqrt(1.0 / (zfactor * zfactor) - 1.0));
+}
+
+int tvl1_nscales(int w, int h, int nscales, float zfactor) {
+    const float N = (float)(1 + std::log(std::hypot((double)w, (double)h) / 16.0) /
+                                    std::log(1 / zfactor));
+    return (N < nscales) ? (int)N : nscales;
+}
+
+void tvl1_zoom_size(int nx, int ny, int *nxx, int *nyy, float f) {
+    *nxx = (int)((float)nx * f + 0.5);
+    *nyy = (int)((float)ny * f + 0.5);
+}
+
+// ---------------------------------------------------------------- device state
+struct TvCtrl {
+    int cur;            // ping-pong index of the current (U, P)
+    int n;              // inner iterations done in the current warp
+    int stop;           // current warp finished
+    unsigned arrive;    // arrival counter of the last-block reduction
+    float norm_min, norm_den;
+    int norm_apply;
+    int pad0;
+    double energy;
+    double pad1[3];
+};
+
+struct NormRec {  // |x|, first index, signed value
+    float a;
+    int idx;
+    float val;
+    int pad;
+};
+
+__device__ __forceinline__ bool better_max(const NormRec &a, const NormRec &b) {
+    return a.a > b.a || (a.a == b.a && a.idx < b.idx);
+}
+__device__ __forceinline__ bool better_min(const NormRec &a, const NormRec &b) {
+    return a.a < b.a || (a.a == b.a && a.idx < b.idx);
+}
+
+// ---------------------------------------------------------------- ingest
+// raw frames -> float planes T[b][k], and per-block |x| extrema for the
+// normalisation (tvl1.cpp:118-123, :302-317).  grid (blocks, B).
+template <typename In>
+__global__ void __launch_bounds__(kIngestNT) k_ingest(const In *__restrict__ raw, float *T,
+                                                      int N, NormRec *recs, int nblk) {
+    const int b = blockIdx.y;
+    __shared__ NormRec sh[4][kIngestNT / 32];
+    NormRec r[4];
+    r[0] = {-1.0f, INT_MAX, 0.0f, 0}; r[1] = {INFINITY, INT_MAX, 0.0f, 0};
+    r[2] = r[0]; r[3] = r[1];
+    for (int k = 0; k < 2; k++) {
+        const In *src = raw + (size_t)(2 * b + k) * N;
+        float *dst = T + (size_t)(2 * b + k) * N;
+        for (int i = blockIdx.x * kIngestNT + threadIdx.x; i < N; i += nblk * kIngestNT) {
+            const float x = (float)src[i];
+            dst[i] = x;
+            const NormRec c{fabsf(x), i, x, 0};
+            if (better_max(c, r[2 * k])) r[2 * k] = c;
+            if (better_min(c, r[2 * k + 1])) r[2 * k + 1] = c;
+        }
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            NormRec c;
+            c.a = __shfl_down_sync(0xffffffffu, r[q].a, o);
+            c.idx = __shfl_down_sync(0xffffffffu, r[q].idx, o);
+            c.val = __shfl_down_sync(0xffffffffu, r[q].val, o);
+            c.pad = 0;
+            if ((q & 1) ? better_min(c, r[q]) : better_max(c, r[q])) r[q] = c;
+        }
+        if (lane == 0) sh[q][wid] = r[q];
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        const int q = threadIdx.x;
+        NormRec best = sh[q][0];
+        for (int w = 1; w < kIngestNT / 32; w++)
+            if ((q & 1) ? better_min(sh[q][w], best) : better_max(sh[q][w], best)) best = sh[q][w];
+        recs[((size_t)b * nblk + blockIdx.x) * 4 + q] = best;
+    }
+}
+
+// One block per pair: joint range of both frames (std::max / std::min of the
+// per-frame |x| extrema, tvl1.cpp:316-321).
+__global__ void k_norm_finalize(const NormRec *recs, int nblk, TvCtrl *ctrl) {
+    const int b = blockIdx.x;
+    __shared__ NormRec sh[4];
+    if (threadIdx.x < 4) {
+        const int q = threadIdx.x;
+        NormRec best = recs[((size_t)b * nblk) * 4 + q];
+        for (int i = 1; i < nblk; i++) {
+            const NormRec c = recs[((size_t)b * nblk + i) * 4 + q];
+            if ((q & 1) ? better_min(c, best) : better_max(c, best)) best = c;
+        }
+        sh[q] = best;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const float a0 = sh[0].val, a1 = sh[2].val, b0 = sh[1].val, b1 = sh[3].val;
+        const float mx = (a0 < a1) ? a1 : a0;
+        const float mn = (b1 < b0) ? b1 : b0;
+        const float den = mx - mn;
+        ctrl[b].norm_min = mn;
+        ctrl[b].norm_den = den;
+        ctrl[b].norm_apply = (den <= 0) ? 0 : 1;  // tvl1.cpp:320-321
+        ctrl[b].cur = 0;
+        ctrl[b].n = 0;
+        ctrl[b].stop = 0;
+        ctrl[b].arrive = 0;
+    }
+}
+
+// ---------------------------------------------------------------- Gaussian
+// Separable Gaussian with the reference's mirror (mask.cpp:246-286): rows then
+// columns, double taps and sums, each pass rounded to float.  Not in place:
+// src planes -> dst planes, gridDim.z = number of planes.  With `normalize`,
+// the loaded samples first get 255*(x-min)/den in double (tvl1.cpp:326-327).
+__device__ __forceinline__ int gauss_mirror(int x, int n) {
+    if (x < 0) return -x;
+    if (x >= n) return 2 * n - 1 - x;
+    return x;
+}
+
+__global__ void __launch_bounds__(kGaussNT) k_gauss(const float *__restrict__ src, float *dst,
+                                                    int nx, int ny, size_t plane_stride,
+                                                    GaussTaps taps, const TvCtrl *ctrl,
+                                                    int normalize) {
+    constexpr int LW = kGaussTW + 2 * kGaussMaxR;
+    __shared__ float sIn[(kGaussTH + 2 * kGaussMaxR) * LW];
+    __shared__ float sRow[(kGaussTH + 2 * kGaussMaxR) * kGaussTW];
+    const int R = taps.size - 1;
+    const int z = blockIdx.z;
+    const float *in = src + (size_t)z * plane_stride;
+    float *out = dst + (size_t)z * plane_stride;
+    const int x0 = blockIdx.x * kGaussTW, y0 = blockIdx.y * kGaussTH;
+    bool apply = false;
+    float mn = 0.0f, den = 1.0f;
+    if (normalize) {
+        const TvCtrl &c = ctrl[z >> 1];
+        apply = c.norm_apply != 0;
+        mn = c.norm_min;
+        den = c.norm_den;
+    }
+    const int lw = kGaussTW + 2 * R, lh = kGaussTH + 2 * R;
+    for (int i = threadIdx.x; i < lw * lh; i += kGaussNT) {
+        const int ly = i / lw, lx = i % lw;
+        const int my = gauss_mirror(y0 - R + ly, ny), mx = gauss_mirror(x0 - R + lx, nx);
+        float v = 0.0f;
+        if (mx >= 0 && mx < nx && my >= 0 && my < ny) {
+            v = __ldg(in + (size_t)my * nx + mx);
+            if (apply) v = (float)(255.0 * (double)(v - mn) / (double)den);
+        }
+        sIn[ly * LW + lx] = v;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kGaussTW * lh; i += kGaussNT) {
+        const int ly = i / kGaussTW, cx = i % kGaussTW;
+        const float *row = sIn + ly * LW + cx + R;
+        double sum = taps.B[0] * (double)row[0];
+        for (int j = 1; j <= R; j++) {
+            const float pair = row[-j] + row[j];
+            sum += taps.B[j] * (double)pair;
+        }
+        sRow[ly * kGaussTW + cx] = (float)sum;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kGaussTW * kGaussTH; i += kGaussNT) {
+        const int cy = i / kGaussTW, cx = i % kGaussTW;
+        const int x = x0 + cx, y = y0 + cy;
+        if (x >= nx || y >= ny) continue;
+        const float *col = sRow + (cy + R) * kGaussTW + cx;
+        double sum = taps.B[0] * (double)col[0];
+        for (int j = 1; j <= R; j++) {
+            const float pair = col[-j * kGaussTW] + col[j * kGaussTW];
+            sum += taps.B[j] * (double)pair;
+        }
+        out[(size_t)y * nx + x] = (float)sum;
+    }
+}
+
+// ---------------------------------------------------------------- resampling
+// Bicubic resample without border zeroing (zoom.cpp:20-53 and :61-85):
+// out(j, i) = in((float)j / dx, (float)i / dy).  gridDim.z = planes.
+__global__ void k_resample(const float *__restrict__ src, size_t src_stride, int nx, int ny,
+                           float *dst, size_t dst_stride, int nxx, int nyy, float dx, float dy) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+    if (j >= nxx || i >= nyy) return;
+    const float *in = src + (size_t)blockIdx.z * src_stride;
+    const float i2 = (float)i / dy, j2 = (float)j / dx;
+    dst[(size_t)blockIdx.z * dst_stride + (size_t)i * nxx + j] = bicubic_at(in, j2, i2, nx, ny, false);
+}
+
+// Flow upsampling to the next finer scale (tvl1.cpp:167-172): bicubic of both
+// components at (j*nx/nxx, i*ny/nyy) then times 1/zfactor.  Reads U[cur].
+__global__ void k_zoom_flow(const float2 *U0, const float2 *U1, size_t stride, int nx, int ny,
+                            float2 *Uz, int nxx, int nyy, float fx, float fy, float inv,
+                            const TvCtrl *ctrl) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+    const int b = blockIdx.z;
+    if (j >= nxx || i >= nyy) return;
+    const float2 *U = (ctrl[b].cur ? U1 : U0) + (size_t)b * stride;
+    const float i2 = (float)i / fy, j2 = (float)j / fx;
+    BicubicStencil s;
+    bicubic_stencil(j2, i2, nx, ny, false, s);
+    float a[4], c[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const float2 *col = U + s.col[k];
+        const float2 t0 = col[(size_t)nx * s.row[0]], t1 = col[(size_t)nx * s.row[1]];
+        const float2 t2 = col[(size_t)nx * s.row[2]], t3 = col[(size_t)nx * s.row[3]];
+        a[k] = cubic_cell(t0.x, t1.x, t2.x, t3.x, s.ty);
+        c[k] = cubic_cell(t0.y, t1.y, t2.y, t3.y, s.ty);
+    }
+    const float u = cubic_cell(a[0], a[1], a[2], a[3], s.tx);
+    const float v = cubic_cell(c[0], c[1], c[2], c[3], s.tx);
+    Uz[(size_t)b * stride + (size_t)i * nxx + j] = make_float2(inv * u, inv * v);
+}
+
+// ---------------------------------------------------------------- gradient
+// Centered gradient of I1 (mask.cpp:139-196) packed with I1 itself so a warp
+// sample reads all three channels with one 16-byte load per tap.
+__global__ void k_grad_pack(const float *__restrict__ pyr, size_t pyr_stride, int nx, int ny,
+                            float4 *I1g, size_t stride) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int b = blockIdx.z;
+    if (x >= nx || y >= ny) return;
+    const float *I = pyr + (size_t)(2 * b + 1) * pyr_stride;
+    const size_t row = (size_t)y * nx;
+    const float ddx = __ldg(I + row + imin(x + 1, nx - 1)) - __ldg(I + row + imax(x - 1, 0));
+    const float ddy = __ldg(I + (size_t)imin(y + 1, ny - 1) * nx + x) -
+                      __ldg(I + (size_t)imax(y - 1, 0) * nx + x);
+    I1g[(size_t)b * stride + row + x] =
+        make_float4(__ldg(I + row + x), (float)(0.5 * (double)ddx), (float)(0.5 * (double)ddy), 0.0f);
+}
+
+// ---------------------------------------------------------------- warping
+// Per warp (tvl1.cpp:197-212): bicubic samples of I1, I1x, I1y at (x+u1,
+// y+u2) with border zeroing, then rho_c and |grad|^2.  mode 0: u from U[cur];
+// 1: u from the upsampled Uz (copied into U[cur]); 2: u = 0 (coarsest scale).
+// With first_warp, p is zeroed (tvl1.cpp:190-193).
+enum { kWarpFromU = 0, kWarpFromUz = 1, kWarpZero = 2 };
+
+__global__ void k_warp(const float *__restrict__ pyr, size_t pyr_stride, const float4 *I1g,
+                       float4 *W, float2 *U0, float2 *U1, const float2 *Uz, float4 *P0,
+                       float4 *P1, size_t stride, int nx, int ny, int mode, int first_warp,
+                       TvCtrl *ctrl) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int b = blockIdx.z;
+    if (x == 0 && y == 0) {
+        ctrl[b].n = 0;
+        ctrl[b].stop = 0;
+        ctrl[b].arrive = 0;
+    }
+    if (x >= nx || y >= ny) return;
+    const int cur = ctrl[b].cur;
+    const size_t off = (size_t)b * stride, p = (size_t)y * nx + x;
+    float2 *U = (cur ? U1 : U0) + off;
+    float2 u;
+    if (mode == kWarpFromU) {
+        u = U[p];
+    } else if (mode == kWarpFromUz) {
+        u = Uz[off + p];
+        U[p] = u;
+    } else {
+        u = make_float2(0.0f, 0.0f);
+        U[p] = u;
+    }
+    if (first_warp) ((cur ? P1 : P0) + off)[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float uu = (float)x + u.x, vv = (float)y + u.y;
+    float Iw = 0.0f, Iwx = 0.0f, Iwy = 0.0f;
+    BicubicStencil s;
+    if (bicubic_stencil(uu, vv, nx, ny, true, s)) {
+        const float4 *G = I1g + off;
+        float a[4], bx[4], by[4];
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const float4 *col = G + s.col[c];
+            const float4 t0 = __ldg(col + (size_t)nx * s.row[0]);
+            const float4 t1 = __ldg(col + (size_t)nx * s.row[1]);
+            const float4 t2 = __ldg(col + (size_t)nx * s.row[2]);
+            const float4 t3 = __ldg(col + (size_t)nx * s.row[3]);
+            a[c] = cubic_cell(t0.x, t1.x, t2.x, t3.x, s.ty);
+            bx[c] = cubic_cell(t0.y, t1.y, t2.y, t3.y, s.ty);
+            by[c] = cubic_cell(t0.z, t1.z, t2.z, t3.z, s.ty);
+        }
+        Iw = cubic_cell(a[0], a[1], a[2], a[3], s.tx);
+        Iwx = cubic_cell(bx[0], bx[1], bx[2], bx[3], s.tx);
+        Iwy = cubic_cell(by[0], by[1], by[2], by[3], s.tx);
+    }
+    const float I0v = __ldg(pyr + (size_t)(2 * b) * pyr_stride + p);
+    const float grad = (Iwx * Iwx) + (Iwy * Iwy);
+    const float rho_c = (Iw - Iwx * u.x - Iwy * u.y - I0v);
+    W[off + p] = make_float4(Iwx, Iwy, rho_c, grad);
+}
+
+// ---------------------------------------------------------------- iteration
+// Divergence of (a1, a2) at one pixel from its value c and its left / upper
+// neighbours, with the border forms and evaluation order of mask.cpp:31-90.
+__device__ __forceinline__ float div_border(float a1c, float a1l, float a2c, float a2u, bool L,
+                                            bool R, bool T, bool B) {
+    if (!(L | R | T | B)) return (a1c - a1l) + (a2c - a2u);
+    if (T && !L && !R) return a1c - a1l + a2c;
+    if (B && !L && !R) return a1c - a1l - a2u;
+    if (L && !T && !B) return a1c + a2c - a2u;
+    if (R && !T && !B) return -a1l + a2c - a2u;
+    if (L && T) return a1c + a2c;
+    if (R && T) return -a1l + a2c;
+    if (L && B) return a1c - a2u;
+    return -a1l - a2u;
+}
+
+struct IterArgs {
+    const float4 *W;
+    float2 *U0, *U1;
+    float4 *P0, *P1;
+    size_t stride;  // elements between pairs
+    int nx, ny;
+    float l_t, theta, taut, eps2;
+    TvCtrl *ctrl;
+    double *partials;  // [B][max_blocks]
+    int max_blocks;
+    int *iters;        // [B][iter_stride]
+    int iter_stride, stage;
+};
+
+// One inner iteration (tvl1.cpp:218-291) on a TW x TH tile:
+//  A: p(old) on the tile plus a one-pixel ring -> smem
+//  B: TH step, divergence and u update on the tile plus one column to the
+//     right and one row below (those are recomputed by the neighbour tile the
+//     same way), u(new) -> smem; owned pixels add their squared change
+//  C: forward gradient of u(new), g = 1 + tau/theta*|grad u|, p update.
+// The last block of a pair finishes the error reduction and the loop control.
+template <int TW, int TH, int NT>
+__global__ void __launch_bounds__(NT) k_tvl1_iter(IterArgs a) {
+    const int b = blockIdx.z;
+    TvCtrl *ctrl = a.ctrl + b;
+    if (*((volatile int *)&ctrl->stop)) return;
+    const int cur = *((volatile int *)&ctrl->cur);
+    const int nx = a.nx, ny = a.ny;
+    const size_t off = (size_t)b * a.stride;
+    const float2 *__restrict__ Uin = (cur ? a.U1 : a.U0) + off;
+    float2 *__restrict__ Uout = (cur ? a.U0 : a.U1) + off;
+    const float4 *__restrict__ Pin = (cur ? a.P1 : a.P0) + off;
+    float4 *__restrict__ Pout = (cur ? a.P0 : a.P1) + off;
+    const float4 *__restrict__ W = a.W + off;
+    const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
+
+    __shared__ float4 sP[(TH + 2) * (TW + 2)];
+    __shared__ float2 sU[(TH + 1) * (TW + 1)];
+    __shared__ double sred[NT / 32];
+    __shared__ int s_last;
+
+    for (int i = threadIdx.x; i < (TH + 2) * (TW + 2); i += NT) {
+        const int x = x0 + i % (TW + 2) - 1, y = y0 + i / (TW + 2) - 1;
+        float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (x >= 0 && x < nx && y >= 0 && y < ny) p = Pin[(size_t)y * nx + x];
+        sP[i] = p;
+    }
+    __syncthreads();
+
+    double err = 0.0;
+    for (int i = threadIdx.x; i < (TH + 1) * (TW + 1); i += NT) {
+        const int rx = i % (TW + 1), ry = i / (TW + 1);
+        const int x = x0 + rx, y = y0 + ry;
+        if (x >= nx || y >= ny) continue;
+        const size_t p = (size_t)y * nx + x;
+        const float2 u = Uin[p];
+        const float4 w = W[p];
+        const float rho = w.z + (w.x * u.x + w.y * u.y);
+        const float lg = a.l_t * w.w;
+        float d1, d2;
+        if (!(rho >= -lg)) {
+            d1 = a.l_t * w.x;
+            d2 = a.l_t * w.y;
+        } else if (rho > lg) {
+            d1 = -a.l_t * w.x;
+            d2 = -a.l_t * w.y;
+        } else if (w.w < 1E-10f) {
+            d1 = d2 = 0.0f;
+        } else {
+            const float fi = -rho / w.w;
+            d1 = fi * w.x;
+            d2 = fi * w.y;
+        }
+        const float v1 = u.x + d1, v2 = u.y + d2;
+        const float4 *c = sP + (ry + 1) * (TW + 2) + (rx + 1);
+        const float4 pc = c[0], pl = c[-1], pu = c[-(TW + 2)];
+        const bool L = x == 0, R = x == nx - 1, T = y == 0, B = y == ny - 1;
+        const float div1 = div_border(pc.x, pl.x, pc.y, pu.y, L, R, T, B);
+        const float div2 = div_border(pc.z, pl.z, pc.w, pu.w, L, R, T, B);
+        const float2 un = make_float2(v1 + a.theta * div1, v2 + a.theta * div2);
+        sU[i] = un;
+        if (rx < TW && ry < TH) {
+            Uout[p] = un;
+            const float e1 = un.x - u.x, e2 = un.y - u.y;
+            const float term = e1 * e1 + e2 * e2;
+            err += (double)term;
+        }
+    }
+    __syncthreads();
+
+    for (int i = threadIdx.x; i < TW * TH; i += NT) {
+        const int rx = i % TW, ry = i / TW;
+        const int x = x0 + rx, y = y0 + ry;
+        if (x >= nx || y >= ny) continue;
+        const float2 uc = sU[ry * (TW + 1) + rx];
+        float f1x = 0.0f, f2x = 0.0f, f1y = 0.0f, f2y = 0.0f;
+        if (x < nx - 1) {
+            const float2 ur = sU[ry * (TW + 1) + rx + 1];
+            f1x = ur.x - uc.x;
+            f2x = ur.y - uc.y;
+        }
+        if (y < ny - 1) {
+            const float2 ud = sU[(ry + 1) * (TW + 1) + rx];
+            f1y = ud.x - uc.x;
+            f2y = ud.y - uc.y;
+        }
+        const float g1 = 1.0f + a.taut * hypot_ref(f1x, f1y);
+        const float g2 = 1.0f + a.taut * hypot_ref(f2x, f2y);
+        const float4 po = sP[(ry + 1) * (TW + 2) + rx + 1];
+        float4 pn;
+        pn.x = (a.taut * f1x + po.x) / g1;
+        pn.y = (a.taut * f1y + po.y) / g1;
+        pn.z = (a.taut * f2x + po.z) / g2;
+        pn.w = (a.taut * f2y + po.w) / g2;
+        Pout[(size_t)y * nx + x] = pn;
+    }
+
+    // ---- error reduction and loop control (tvl1.cpp:252-265, :216)
+    const double bsum = block_sum_double<NT>(err, sred);
+    const int nblk = gridDim.x * gridDim.y;
+    double *part = a.partials + (size_t)b * a.max_blocks;
+    if (threadIdx.x == 0) {
+        part[blockIdx.y * gridDim.x + blockIdx.x] = bsum;
+        __threadfence();
+        const unsigned prev = atomicAdd(&ctrl->arrive, 1u);
+        s_last = (prev == (unsigned)nblk - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    double acc = 0.0;
+    for (int k = threadIdx.x; k < nblk; k += NT) acc += __ldcg(part + k);
+    const double tot = block_sum_double<NT>(acc, sred);
+    if (threadIdx.x == 0) {
+        float e = (float)tot;
+        e = e / (float)(nx * ny);
+        const int n = ctrl->n + 1;
+        ctrl->n = n;
+        a.iters[(size_t)b * a.iter_stride + a.stage] = n;
+        ctrl->cur = cur ^ 1;
+        if (!(e > a.eps2)) ctrl->stop = 1;
+        ctrl->arrive = 0;
+        __threadfence();
+    }
+}
+
+// ---------------------------------------------------------------- energy
+// E = sum |grad u1| + |grad u2| (forward differences, double) + lambda *
+// sum |rho(u)| with rho linearised at the current warp.  Last block of a pair
+// writes ctrl.energy and, if slot >= 0, energy_out[b * slots + slot].
+constexpr int kEnNT = 256;
+__global__ void __launch_bounds__(kEnNT) k_energy(const float4 *W, const float2 *U0,
+                                                  const float2 *U1, size_t stride, int nx,
+                                                  int ny, float lambda, TvCtrl *ctrl,
+                                                  double *partials, int max_blocks,
+                                                  double *energy_out, int slots, int slot,
+                                                  int expect_n) {
+    const int b = blockIdx.y;
+    const size_t off = (size_t)b * stride;
+    const float2 *U = (ctrl[b].cur ? U1 : U0) + off;
+    const int N = nx * ny;
+    double tv = 0.0, data = 0.0;
+    for (int i = blockIdx.x * kEnNT + threadIdx.x; i < N; i += gridDim.x * kEnNT) {
+        const int x = i % nx, y = i / nx;
+        const float2 uc = U[i];
+        double f1x = 0, f1y = 0, f2x = 0, f2y = 0;
+        if (x < nx - 1) { const float2 r = U[i + 1]; f1x = (double)(r.x - uc.x); f2x = (double)(r.y - uc.y); }
+        if (y < ny - 1) { const float2 d = U[i + nx]; f1y = (double)(d.x - uc.x); f2y = (double)(d.y - uc.y); }
+        tv += sqrt(f1x * f1x + f1y * f1y) + sqrt(f2x * f2x + f2y * f2y);
+        const float4 w = W[off + i];
+        const float rho = w.z + (w.x * uc.x + w.y * uc.y);
+        data += fabs((double)rho);
+    }
+    __shared__ double sred[kEnNT / 32];
+    __shared__ int s_last;
+    const double s = block_sum_double<kEnNT>(tv + (double)lambda * data, sred);
+    double *part = partials + (size_t)b * max_blocks;
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = s;
+        __threadfence();
+        const unsigned prev = atomicAdd(&ctrl[b].arrive, 1u);
+        s_last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    double acc = 0.0;
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += kEnNT) acc += __ldcg(part + k);
+    const double tot = block_sum_double<kEnNT>(acc, sred);
+    if (threadIdx.x == 0) {
+        ctrl[b].energy = tot;
+        // a trace slot is written only if iteration `expect_n` really ran
+        if (slot >= 0 && (expect_n < 0 || ctrl[b].n == expect_n))
+            energy_out[(size_t)b * slots + slot] = tot;
+        ctrl[b].arrive = 0;
+    }
+}
+
+// ---------------------------------------------------------------- output
+__global__ void k_split(const float2 *U0, const float2 *U1, size_t stride, int N, float *ou,
+                        float *ov, const TvCtrl *ctrl) {
+    const int b = blockIdx.y;
+    const float2 *U = (ctrl[b].cur ? U1 : U0) + (size_t)b * stride;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const float2 u = U[i];
+        ou[(size_t)b * stride + i] = u.x;
+        ov[(size_t)b * stride + i] = u.y;
+    }
+}
+
+// ================================================================ launchers
+GaussTaps make_zoom_taps(float zfactor) { return make_taps(zoom_sigma(zfactor)); }
+
+void launch_gauss(const float *src, float *dst, int nx, int ny, size_t stride,
+                  const GaussTaps &t, int planes, cudaStream_t st) {
+    dim3 g(div_up(nx, kGaussTW), div_up(ny, kGaussTH), planes);
+    k_gauss<<<g, kGaussNT, 0, st>>>(src, dst, nx, ny, stride, t, nullptr, 0);
+}
+
+void launch_resample(const float *src, size_t sstride, int nx, int ny, float *dst,
+                     size_t dstride, int nxx, int nyy, float dx, float dy, int planes,
+                     cudaStream_t st) {
+    dim3 blk(32, 8), g(div_up(nxx, 32), div_up(nyy, 8), planes);
+    k_resample<<<g, blk, 0, st>>>(src, sstride, nx, ny, dst, dstride, nxx, nyy, dx, dy);
+}
+
+// ================================================================ host plan
+TvPlan::TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, bool trace)
+    : w_(w), h_(h), B_(B), dtype_(dtype), prm_(prm), trace_(trace) {
+    OF_CHECK(w >= 8 && h >= 8, "tvl1: frames must be at least 8x8");
+    OF_CHECK(B >= 1, "tvl1: empty batch");
+    OF_CHECK(prm.zfactor > 0.0f && prm.zfactor < 1.0f, "tvl1: zfactor must be in (0,1)");
+    OF_CHECK(prm.warps >= 1 && prm.warps <= OFLOW_MAX_WARPS, "tvl1: warps out of range");
+    OF_CHECK(prm.max_iterations >= 0, "tvl1: max_iterations < 0");
+    OF_CHECK(prm.theta > 0.0f, "tvl1: theta must be > 0");
+    ns_ = tvl1_nscales(w, h, prm.nscales, prm.zfactor);
+    OF_CHECK(ns_ >= 1 && ns_ <= OFLOW_MAX_SCALES, "tvl1: number of scales out of range");
+    nx_[0] = w;
+    ny_[0] = h;
+    for (int s = 1; s < ns_; s++) tvl1_zoom_size(nx_[s - 1], ny_[s - 1], &nx_[s], &ny_[s], prm.zfactor);
+    taps0_ = make_taps(0.8f);
+    tapsz_ = make_taps(zoom_sigma(prm.zfactor));
+    // every blurred level must hold the whole window (mask.cpp:231)
+    OF_CHECK(taps0_.size <= w && taps0_.size <= h, "tvl1: frame smaller than the Gaussian window");
+    for (int s = 0; s + 1 < ns_; s++)
+        OF_CHECK(tapsz_.size <= nx_[s] && tapsz_.size <= ny_[s],
+                 "tvl1: pyramid level smaller than the Gaussian window");
+    for (int s = 0; s < ns_; s++) OF_CHECK(nx_[s] >= 2 && ny_[s] >= 2, "tvl1: level below 2x2");
+
+    const size_t N0 = (size_t)w * h;
+    N0_ = N0;
+    iter_blocks_ = div_up(w, kIterTW) * div_up(h, kIterTH);
+    ingest_blocks_ = imin(div_up((int)N0, kIngestNT * kIngestPPT), 1024);
+    energy_blocks_ = imin(div_up((int)N0, kEnNT * 4), 512);
+    max_blocks_ = imax(iter_blocks_, energy_blocks_);
+    pyr_off_[0] = 0;
+    for (int s = 1; s < ns_; s++) pyr_off_[s] = pyr_off_[s - 1] + (size_t)2 * B * nx_[s - 1] * ny_[s - 1];
+    const size_t pyr_total = pyr_off_[ns_ - 1] + (size_t)2 * B * nx_[ns_ - 1] * ny_[ns_ - 1];
+    const size_t esz = dtype == OFLOW_U8 ? 1 : 4;
+
+    o_raw_ = ar_.reserve(2 * B * N0 * esz);
+    o_T_ = ar_.reserve(2 * B * N0 * 4);
+    o_pyr_ = ar_.reserve(pyr_total * 4);
+    o_I1g_ = ar_.reserve(B * N0 * 16);
+    o_W_ = ar_.reserve(B * N0 * 16);
+    o_U0_ = ar_.reserve(B * N0 * 8);
+    o_U1_ = ar_.reserve(B * N0 * 8);
+    o_Uz_ = ar_.reserve(B * N0 * 8);
+    o_P0_ = ar_.reserve(B * N0 * 16);
+    o_P1_ = ar_.reserve(B * N0 * 16);
+    o_out_ = ar_.reserve(2 * B * N0 * 4);
+    o_ctrl_ = ar_.reserve(B * sizeof(TvCtrl));
+    o_part_ = ar_.reserve((size_t)B * max_blocks_ * 8);
+    o_recs_ = ar_.reserve((size_t)B * ingest_blocks_ * 4 * sizeof(NormRec));
+    iter_stride_ = ns_ * prm.warps;
+    o_iters_ = ar_.reserve((size_t)B * iter_stride_ * 4);
+    energy_slots_ = trace ? ns_ * prm.warps * prm.max_iterations : 1;
+    o_energy_ = ar_.reserve((size_t)B * energy_slots_ * 8);
+    ar_.commit();
+    OF_CUDA(cudaMemset(ar_.at<char>(o_ctrl_), 0, B * sizeof(TvCtrl)));
+}
+
+void *TvPlan::raw_input(int b, int k) const {
+    const size_t esz = dtype_ == OFLOW_U8 ? 1 : 4;
+    return ar_.at<char>(o_raw_) + (size_t)(2 * b + k) * N0_ * esz;
+}
+const float *TvPlan::out_u(int b) const { return ar_.at<float>(o_out_) + (size_t)b * N0_; }
+const float *TvPlan::out_v(int b) const { return ar_.at<float>(o_out_) + (size_t)(B_ + b) * N0_; }
+const int *TvPlan::iters_dev() const { return ar_.at<int>(o_iters_); }
+
+void TvPlan::record(cudaStream_t st) {
+    launches_ = 0;
+    const int B = B_;
+    const size_t N0 = N0_;
+    float *T = ar_.at<float>(o_T_);
+    float *pyr = ar_.at<float>(o_pyr_);
+    float4 *I1g = ar_.at<float4>(o_I1g_);
+    float4 *W = ar_.at<float4>(o_W_);
+    float2 *U0 = ar_.at<float2>(o_U0_), *U1 = ar_.at<float2>(o_U1_), *Uz = ar_.at<float2>(o_Uz_);
+    float4 *P0 = ar_.at<float4>(o_P0_), *P1 = ar_.at<float4>(o_P1_);
+    TvCtrl *ctrl = ar_.at<TvCtrl>(o_ctrl_);
+    double *part = ar_.at<double>(o_part_);
+    NormRec *recs = ar_.at<NormRec>(o_recs_);
+    int *iters = ar_.at<int>(o_iters_);
+    double *energy = ar_.at<double>(o_energy_);
+
+    OF_CUDA(cudaMemsetAsync(iters, 0, sizeof(int) * (size_t)B * iter_stride_, st));
+    // ingest + normalisation range
+    {
+        dim3 g(ingest_blocks_, B);
+        if (dtype_ == OFLOW_U8)
+            k_ingest<uint8_t><<<g, kIngestNT, 0, st>>>(ar_.at<uint8_t>(o_raw_), T, (int)N0, recs,
+                                                       ingest_blocks_);
+        else
+            k_ingest<float><<<g, kIngestNT, 0, st>>>(ar_.at<float>(o_raw_), T, (int)N0, recs,
+                                                     ingest_blocks_);
+        k_norm_finalize<<<B, 32, 0, st>>>(recs, ingest_blocks_, ctrl);
+        launches_ += 2;
+    }
+    // normalised, pre-smoothed level 0 (tvl1.cpp:140-144)
+    {
+        dim3 g(div_up(w_, kGaussTW), div_up(h_, kGaussTH), 2 * B);
+        k_gauss<<<g, kGaussNT, 0, st>>>(T, pyr + pyr_off_[0], w_, h_, N0, taps0_, ctrl, 1);
+        launches_ += 1;
+    }
+    // pyramid (tvl1.cpp:147-154)
+    for (int s = 1; s < ns_; s++) {
+        const int nx = nx_[s - 1], ny = ny_[s - 1];
+        const size_t sp = (size_t)nx * ny, dp = (size_t)nx_[s] * ny_[s];
+        dim3 g(div_up(nx, kGaussTW), div_up(ny, kGaussTH), 2 * B);
+        k_gauss<<<g, kGaussNT, 0, st>>>(pyr + pyr_off_[s - 1], T, nx, ny, sp, tapsz_, ctrl, 0);
+        dim3 blk(32, 8), gr(div_up(nx_[s], 32), div_up(ny_[s], 8), 2 * B);
+        k_resample<<<gr, blk, 0, st>>>(T, sp, nx, ny, pyr + pyr_off_[s], dp, nx_[s], ny_[s],
+                                       prm_.zfactor, prm_.zfactor);
+        launches_ += 2;
+    }
+    const float l_t = prm_.lambda * prm_.theta;
+    const float taut = prm_.tau / prm_.theta;
+    const float eps2 = prm_.epsilon * prm_.epsilon;
+    const float inv = 1 / prm_.zfactor;
+    for (int s = ns_ - 1; s >= 0; s--) {
+        const int nx = nx_[s], ny = ny_[s];
+        const size_t lp = (size_t)nx * ny;
+        dim3 blk(32, 8), gr(div_up(nx, 32), div_up(ny, 8), B);
+        if (s < ns_ - 1) {
+            const int cx = nx_[s + 1], cy = ny_[s + 1];
+            k_zoom_flow<<<gr, blk, 0, st>>>(U0, U1, N0, cx, cy, Uz, nx, ny, (float)nx / cx,
+                                            (float)ny / cy, inv, ctrl);
+            launches_ += 1;
+        }
+        k_grad_pack<<<gr, blk, 0, st>>>(pyr + pyr_off_[s], lp, nx, ny, I1g, N0);
+        launches_ += 1;
+        IterArgs ia{W, U0, U1, P0, P1, N0, nx, ny, l_t, prm_.theta, taut, eps2, ctrl, part,
+                    max_blocks_, iters, iter_stride_, 0};
+        dim3 ig(div_up(nx, kIterTW), div_up(ny, kIterTH), B);
+        for (int wi = 0; wi < prm_.warps; wi++) {
+            const int mode = wi > 0 ? kWarpFromU : (s == ns_ - 1 ? kWarpZero : kWarpFromUz);
+            if (prof_) OF_CUDA(cudaEventRecord(prof_->ev[prof_->n_ev++], st));
+            k_warp<<<gr, blk, 0, st>>>(pyr + pyr_off_[s], lp, I1g, W, U0, U1, Uz, P0, P1, N0, nx,
+                                       ny, mode, wi == 0, ctrl);
+            if (prof_) OF_CUDA(cudaEventRecord(prof_->ev[prof_->n_ev++], st));
+            launches_ += 1;
+            ia.stage = s * prm_.warps + wi;
+            for (int it = 0; it < prm_.max_iterations; it++) {
+                if (prof_) OF_CUDA(cudaEventRecord(prof_->ev[prof_->n_ev++], st));
+                k_tvl1_iter<kIterTW, kIterTH, kIterNT><<<ig, kIterNT, 0, st>>>(ia);
+                if (prof_) OF_CUDA(cudaEventRecord(prof_->ev[prof_->n_ev++], st));
+                launches_ += 1;
+                if (trace_) {
+                    const int slot = (s * prm_.warps + wi) * prm_.max_iterations + it;
+                    k_energy<<<dim3(imin(energy_blocks_, div_up(nx * ny, kEnNT * 4)), B), kEnNT, 0,
+                               st>>>(W, U0, U1, N0, nx, ny, prm_.lambda, ctrl, part, max_blocks_,
+                                     energy, energy_slots_, slot, it + 1);
+                    launches_ += 1;
+                }
+            }
+        }
+    }
+    // final energy at the finest scale, last warp
+    k_energy<<<dim3(energy_blocks_, B), kEnNT, 0, st>>>(W, U0, U1, N0, w_, h_, prm_.lambda, ctrl,
+                                                        part, max_blocks_, energy,
+                                                        energy_slots_, trace_ ? -1 : 0, -1);
+    k_split<<<dim3(imin(div_up((int)N0, 256 * 4), 1024), B), 256, 0, st>>>(
+        U0, U1, N0, (int)N0, ar_.at<float>(o_out_), ar_.at<float>(o_out_) + (size_t)B * N0, ctrl);
+    launches_ += 2;
+    OF_CUDA(cudaGetLastError());
+}
+
+// Eager run with CUDA events around every warp and inner-iteration launch on
+// `st`; returns per-kind totals (ms) and launch counts.
+void TvPlan::profile(cudaStream_t st, oflow_tvl1_profile *out) {
+    Prof p;
+    const int stages = ns_ * prm_.warps;
+    p.ev.resize((size_t)2 * stages * (1 + prm_.max_iterations) + 2);
+    for (auto &e : p.ev) OF_CUDA(cudaEventCreate(&e));
+    cudaEvent_t t0, t1;
+    OF_CUDA(cudaEventCreate(&t0));
+    OF_CUDA(cudaEventCreate(&t1));
+    prof_ = &p;
+    try {
+        OF_CUDA(cudaEventRecord(t0, st));
+        record(st);
+        OF_CUDA(cudaEventRecord(t1, st));
+        OF_CUDA(cudaStreamSynchronize(st));
+    } catch (...) {
+        prof_ = nullptr;
+        for (auto &e : p.ev) cudaEventDestroy(e);
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        throw;
+    }
+    prof_ = nullptr;
+    std::memset(out, 0, sizeof(*out));
+    float ms = 0.0f;
+    OF_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+    out->total_ms = ms;
+    int k = 0;
+    for (int st_i = 0; st_i < stages; st_i++) {
+        OF_CUDA(cudaEventElapsedTime(&ms, p.ev[k], p.ev[k + 1]));
+        out->warp_ms += ms;
+        out->warp_launches += 1;
+        k += 2;
+        for (int it = 0; it < prm_.max_iterations; it++) {
+            OF_CUDA(cudaEventElapsedTime(&ms, p.ev[k], p.ev[k + 1]));
+            out->iter_ms += ms;
+            out->iter_launches += 1;
+            k += 2;
+        }
+    }
+    out->launches = launches_;
+    for (auto &e : p.ev) cudaEventDestroy(e);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+}
+
+void TvPlan::run(cudaStream_t st) {
+    if (!graph_.ready()) graph_.capture(st, [&](cudaStream_t s) { record(s); });
+    graph_.launch(st);
+}
+
+void TvPlan::read_stats(int b, oflow_tvl1_stats *out, cudaStream_t st) const {
+    std::vector<int> it(iter_stride_);
+    OF_CUDA(cudaMemcpyAsync(it.data(), iters_dev() + (size_t)b * iter_stride_,
+                            sizeof(int) * iter_stride_, cudaMemcpyDeviceToHost, st));
+    TvCtrl c;
+    OF_CUDA(cudaMemcpyAsync(&c, ar_.at<TvCtrl>(o_ctrl_) + b, sizeof(TvCtrl), cudaMemcpyDeviceToHost, st));
+    OF_CUDA(cudaStreamSynchronize(st));
+    std::memset(out, 0, sizeof(*out));
+    out->nscales = ns_;
+    out->warps = prm_.warps;
+    for (int i = 0; i < iter_stride_; i++) out->iterations[i] = it[i];
+    out->energy = c.energy;
+}
+
+void TvPlan::read_energy_trace(int b, double *dst, cudaStream_t st) const {
+    OF_CHECK(trace_, "tvl1: plan was built without the energy trace");
+    OF_CUDA(cudaMemcpyAsync(dst, ar_.at<double>(o_energy_) + (size_t)b * energy_slots_,
+                            sizeof(double) * energy_slots_, cudaMemcpyDeviceToHost, st));
+    OF_CUDA(cudaStreamSynchronize(st));
+}
+
+}  // namespace oflow

@@ -1,0 +1,83 @@
+// Batched TV-L1 plan: device buffers for B equal-size pairs and the captured
+// schedule (ingest, normalisation, pyramid, coarse-to-fine warps and inner
+// iterations, output split).
+#pragma once
+
+#include "internal.hpp"
+
+namespace oflow {
+
+// Normalised Gaussian half-kernel (centre + radius taps), double precision.
+struct GaussTaps {
+    double B[16];
+    int size;  // taps including the centre; radius = size - 1
+};
+
+int tvl1_nscales(int w, int h, int nscales, float zfactor);
+void tvl1_zoom_size(int nx, int ny, int *nxx, int *nyy, float f);
+// Taps of the pre-decimation blur, sigma = 0.6*sqrt(1/f^2 - 1) (zoom.cpp:39).
+GaussTaps make_zoom_taps(float zfactor);
+// Separable Gaussian of `planes` dense nx*ny planes (stride apart), src -> dst.
+void launch_gauss(const float *src, float *dst, int nx, int ny, size_t stride,
+                  const GaussTaps &t, int planes, cudaStream_t st);
+// Bicubic resample (no border zeroing) at ((float)j/dx, (float)i/dy).
+void launch_resample(const float *src, size_t sstride, int nx, int ny, float *dst,
+                     size_t dstride, int nxx, int nyy, float dx, float dy, int planes,
+                     cudaStream_t st);
+
+class TvPlan {
+  public:
+    TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, bool trace = false);
+    // Device destination of input frame k (0: I0, 1: I1) of pair b: a dense
+    // w*h plane of the plan's dtype.
+    void *raw_input(int b, int k) const;
+    const float *out_u(int b) const;
+    const float *out_v(int b) const;
+    const int *iters_dev() const;
+    // Enqueue the whole solve (captured into a graph on first use).
+    void run(cudaStream_t st);
+    // Enqueue the launches directly on `st` (also what the graph captures).
+    void record(cudaStream_t st);
+    void read_stats(int b, oflow_tvl1_stats *out, cudaStream_t st) const;
+    // Eager run with events around each warp / inner-iteration launch.
+    void profile(cudaStream_t st, oflow_tvl1_profile *out);
+    int launches() const { return launches_; }
+    void read_energy_trace(int b, double *dst, cudaStream_t st) const;
+
+    int width() const { return w_; }
+    int height() const { return h_; }
+    int batch() const { return B_; }
+    int dtype() const { return dtype_; }
+    int nscales() const { return ns_; }
+    int level_w(int s) const { return nx_[s]; }
+    int level_h(int s) const { return ny_[s]; }
+    int energy_slots() const { return energy_slots_; }
+    bool traced() const { return trace_; }
+    const oflow_tvl1_params &params() const { return prm_; }
+    size_t device_bytes() const { return ar_.size(); }
+
+  private:
+    int w_, h_, B_, dtype_;
+    oflow_tvl1_params prm_;
+    bool trace_;
+    int ns_ = 0;
+    int nx_[OFLOW_MAX_SCALES] = {}, ny_[OFLOW_MAX_SCALES] = {};
+    size_t pyr_off_[OFLOW_MAX_SCALES] = {};
+    size_t N0_ = 0;
+    int iter_blocks_ = 0, ingest_blocks_ = 0, energy_blocks_ = 0, max_blocks_ = 0;
+    int iter_stride_ = 0, energy_slots_ = 0;
+    GaussTaps taps0_{}, tapsz_{};
+    struct Prof {
+        std::vector<cudaEvent_t> ev;
+        int n_ev = 0;
+    };
+    Prof *prof_ = nullptr;
+    int launches_ = 0;
+    Arena ar_;
+    size_t o_raw_ = 0, o_T_ = 0, o_pyr_ = 0, o_I1g_ = 0, o_W_ = 0, o_U0_ = 0, o_U1_ = 0,
+           o_Uz_ = 0, o_P0_ = 0, o_P1_ = 0, o_out_ = 0, o_ctrl_ = 0, o_part_ = 0, o_recs_ = 0,
+           o_iters_ = 0, o_energy_ = 0;
+    Graph graph_;
+};
+
+}  // namespace oflow

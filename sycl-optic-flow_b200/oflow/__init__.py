@@ -1,0 +1,326 @@
+"""oflow: dense optical flow (TV-L1, Horn-Schunck, Lucas-Kanade) on B200.
+
+Python side of the C ABI in include/oflow.h (liboflow.so, sm_100a kernels).
+There is no CPU fallback: importing works anywhere, but every solve needs the
+built library and a CUDA device and raises otherwise.
+
+Two layers:
+
+* functions ``tvl1``, ``tvl1_batch``, ``hs``, ``hs_batch``, ``lk``,
+  ``pyrlk`` taking numpy arrays (host) or CUDA torch tensors (device) and
+  returning (u, v);
+* classes mirroring the reference entry points: ``TV_L1``
+  (src/tvl1/sequential/tvl1.hpp:10-17, src/tvl1/cuda/tvl1.cuh:12-20),
+  ``initFlow`` / ``ComputeFlow`` / ``deleteFlow_mem`` (src/hs/cuda/flow.cuh:
+  19-33) and ``LucasKanade`` (src/lk/cuda/lucaskanade.cuh:6-12).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+from .capi import (LIB_PATH, OflowError, Flow, Image, HsParams, LkParams, Tvl1Params,
+                   Tvl1Profile, Tvl1Stats, lib, status_string)
+
+__all__ = [
+    "Context", "OflowError", "TVL1Params", "HSParams", "LKParams", "tvl1", "tvl1_batch",
+    "tvl1_energy_trace", "hs", "hs_batch", "lk", "pyrlk", "TV_L1", "initFlow", "ComputeFlow",
+    "deleteFlow_mem", "LucasKanade", "nscales", "LIB_PATH",
+]
+
+
+@dataclass
+class TVL1Params:
+    """Defaults of src/tvl1/sequential/tvl1.hpp:6,12-14."""
+    tau: float = 0.25
+    lambda_: float = 0.15
+    theta: float = 0.3
+    nscales: int = 100
+    zfactor: float = 0.5
+    warps: int = 5
+    epsilon: float = 0.01
+    max_iterations: int = 300
+
+    def c(self) -> Tvl1Params:
+        return Tvl1Params(self.tau, self.lambda_, self.theta, self.nscales, self.zfactor,
+                          self.warps, self.epsilon, self.max_iterations)
+
+
+@dataclass
+class HSParams:
+    """Defaults of the reference demo (src/hs/cuda/main.cu:140-148)."""
+    alpha: float = 0.2
+    nlevels: int = 5
+    nwarp: int = 3
+    nsolver: int = 150
+
+    def c(self) -> HsParams:
+        return HsParams(self.alpha, self.nlevels, self.nwarp, self.nsolver)
+
+
+@dataclass
+class LKParams:
+    """Defaults of the reference demo (src/lk/cuda/main.cu:132-134) plus the
+    pyramid shape used by oflow_pyrlk."""
+    spac: int = 3
+    temp: int = 2
+    window: int = 5
+    levels: int = 3
+    iters: int = 3
+
+    def c(self) -> LkParams:
+        return LkParams(self.spac, self.temp, self.window, self.levels, self.iters)
+
+
+def _check(status, ctx=None):
+    if status != 0:
+        msg = status_string(status)
+        if ctx is not None:
+            detail = lib().oflow_ctx_last_error(ctx).decode()
+            if detail:
+                msg += ": " + detail
+        raise OflowError(status, msg)
+
+
+class Context:
+    """One oflow context (device, stream, cached plans).  Use from one thread."""
+
+    def __init__(self, device: int = 0):
+        self._h = C.c_void_p()
+        _check(lib().oflow_ctx_create(device, C.byref(self._h)))
+        self.device = device
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_stream(self, stream_ptr: int | None):
+        _check(lib().oflow_ctx_set_stream(self._h, C.c_void_p(stream_ptr or 0)), self._h)
+
+    def trim(self):
+        _check(lib().oflow_ctx_trim(self._h), self._h)
+
+    def close(self):
+        if self._h:
+            lib().oflow_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx: Context | None = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+# ------------------------------------------------------------------ marshalling
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+def _image(x) -> tuple[Image, object]:
+    """numpy (host) or torch CUDA tensor (device) -> oflow_image, keep-alive."""
+    if _is_torch(x):
+        import torch
+        if x.dim() != 2:
+            raise ValueError("frames must be 2-D")
+        if x.dtype == torch.uint8:
+            dt = 0
+        elif x.dtype == torch.float32:
+            dt = 1
+        else:
+            raise TypeError("frames must be uint8 or float32")
+        if x.stride(1) != 1:
+            x = x.contiguous()
+        loc = 1 if x.is_cuda else 0
+        return Image(C.c_void_p(x.data_ptr()), x.shape[1], x.shape[0], x.stride(0), dt, loc), x
+    a = np.asarray(x)
+    if a.ndim != 2:
+        raise ValueError("frames must be 2-D")
+    if a.dtype == np.uint8:
+        dt = 0
+    elif a.dtype == np.float32:
+        dt = 1
+    else:
+        a = a.astype(np.float32)
+        dt = 1
+    a = np.ascontiguousarray(a)
+    return Image(a.ctypes.data_as(C.c_void_p), a.shape[1], a.shape[0], a.shape[1], dt, 0), a
+
+
+def _outputs(like, h, w, out=None):
+    """Allocate (u, v) on the same side as `like` unless given."""
+    if out is not None:
+        u, v = out
+    elif _is_torch(like) and like.is_cuda:
+        import torch
+        u = torch.empty((h, w), dtype=torch.float32, device=like.device)
+        v = torch.empty((h, w), dtype=torch.float32, device=like.device)
+    else:
+        u = np.empty((h, w), np.float32)
+        v = np.empty((h, w), np.float32)
+    if _is_torch(u):
+        f = Flow(C.cast(C.c_void_p(u.data_ptr()), C.POINTER(C.c_float)),
+                 C.cast(C.c_void_p(v.data_ptr()), C.POINTER(C.c_float)), u.stride(0),
+                 1 if u.is_cuda else 0)
+    else:
+        f = Flow(u.ctypes.data_as(C.POINTER(C.c_float)), v.ctypes.data_as(C.POINTER(C.c_float)),
+                 u.shape[1], 0)
+    return f, (u, v)
+
+
+def _ctx(ctx):
+    return (ctx or default_context()).handle
+
+
+# ------------------------------------------------------------------ TV-L1
+def nscales(width, height, params: TVL1Params | None = None) -> int:
+    p = (params or TVL1Params()).c()
+    return lib().oflow_tvl1_nscales(width, height, C.byref(p))
+
+
+def _stats_dict(s: Tvl1Stats):
+    its = np.ctypeslib.as_array(s.iterations)[: s.nscales * s.warps].reshape(s.nscales, s.warps)
+    return {"nscales": s.nscales, "warps": s.warps, "iterations": its.copy(), "energy": s.energy}
+
+
+def tvl1_batch(pairs, params: TVL1Params | None = None, ctx: Context | None = None,
+               stats: bool = False, out=None):
+    """Solve a list of (I0, I1) pairs in one schedule.  Returns a list of
+    (u, v) (and a list of stats dicts if stats=True)."""
+    p = (params or TVL1Params()).c()
+    n = len(pairs)
+    I0 = (Image * n)()
+    I1 = (Image * n)()
+    O = (Flow * n)()
+    keep, res = [], []
+    for i, (a, b) in enumerate(pairs):
+        I0[i], ka = _image(a)
+        I1[i], kb = _image(b)
+        keep += [ka, kb]
+        O[i], uv = _outputs(a, I0[i].height, I0[i].width, None if out is None else out[i])
+        res.append(uv)
+    st = (Tvl1Stats * n)() if stats else None
+    h = _ctx(ctx)
+    _check(lib().oflow_tvl1_batch(h, n, I0, I1, C.byref(p), O, st), h)
+    if stats:
+        return res, [_stats_dict(s) for s in st]
+    return res
+
+
+def tvl1_batch_profile(pairs, params: TVL1Params | None = None, ctx: Context | None = None,
+                       out=None):
+    """tvl1_batch (equal sizes) run eagerly with CUDA events around every warp
+    and inner-iteration launch.  Returns (results, stats, profile dict)."""
+    p = (params or TVL1Params()).c()
+    n = len(pairs)
+    I0 = (Image * n)()
+    I1 = (Image * n)()
+    O = (Flow * n)()
+    keep, res = [], []
+    for i, (a, b) in enumerate(pairs):
+        I0[i], ka = _image(a)
+        I1[i], kb = _image(b)
+        keep += [ka, kb]
+        O[i], uv = _outputs(a, I0[i].height, I0[i].width, None if out is None else out[i])
+        res.append(uv)
+    st = (Tvl1Stats * n)()
+    pr = Tvl1Profile()
+    h = _ctx(ctx)
+    _check(lib().oflow_tvl1_batch_profile(h, n, I0, I1, C.byref(p), O, st, C.byref(pr)), h)
+    prof = {k: getattr(pr, k) for k, _ in Tvl1Profile._fields_}
+    return res, [_stats_dict(s) for s in st], prof
+
+
+def tvl1(I0, I1, params: TVL1Params | None = None, ctx: Context | None = None,
+         stats: bool = False, out=None):
+    r = tvl1_batch([(I0, I1)], params, ctx, stats, None if out is None else [out])
+    if stats:
+        return r[0][0][0], r[0][0][1], r[1][0]
+    return r[0]
+
+
+def tvl1_energy_trace(I0, I1, params: TVL1Params | None = None, ctx: Context | None = None):
+    """Solve one pair and return (u, v, stats, energy[nscales, warps, max_iterations])
+    with the energy after every inner iteration (NaN where a stage stopped)."""
+    prm = params or TVL1Params()
+    p = prm.c()
+    a, ka = _image(I0)
+    b, kb = _image(I1)
+    f, (u, v) = _outputs(I0, a.height, a.width)
+    ns = nscales(a.width, a.height, prm)
+    en = np.full(ns * prm.warps * max(prm.max_iterations, 1), np.nan, np.float64)
+    st = Tvl1Stats()
+    h = _ctx(ctx)
+    _check(lib().oflow_tvl1_energy_trace(h, C.byref(a), C.byref(b), C.byref(p), C.byref(f),
+                                         C.byref(st), en.ctypes.data_as(C.POINTER(C.c_double))), h)
+    return u, v, _stats_dict(st), en.reshape(ns, prm.warps, max(prm.max_iterations, 1))
+
+
+# ------------------------------------------------------------------ Horn-Schunck
+def hs_batch(pairs, params: HSParams | None = None, ctx: Context | None = None, out=None):
+    p = (params or HSParams()).c()
+    n = len(pairs)
+    I0 = (Image * n)()
+    I1 = (Image * n)()
+    O = (Flow * n)()
+    keep, res = [], []
+    for i, (a, b) in enumerate(pairs):
+        I0[i], ka = _image(a)
+        I1[i], kb = _image(b)
+        keep += [ka, kb]
+        O[i], uv = _outputs(a, I0[i].height, I0[i].width, None if out is None else out[i])
+        res.append(uv)
+    h = _ctx(ctx)
+    _check(lib().oflow_hs_batch(h, n, I0, I1, C.byref(p), O), h)
+    return res
+
+
+def hs(I0, I1, params: HSParams | None = None, ctx: Context | None = None, out=None):
+    return hs_batch([(I0, I1)], params, ctx, None if out is None else [out])[0]
+
+
+# ------------------------------------------------------------------ Lucas-Kanade
+def lk(frames, iframe: int, params: LKParams | None = None, ctx: Context | None = None,
+       out=None):
+    """Single-step LK over a ring of `params.temp` uint8 frames (frames[k] = ring
+    slot k, newest frame in slot iframe % temp)."""
+    prm = params or LKParams()
+    p = prm.c()
+    T = prm.temp
+    if len(frames) != T:
+        raise ValueError("lk: need exactly `temp` ring frames")
+    arr = (Image * T)()
+    keep = []
+    for k in range(T):
+        arr[k], kk = _image(frames[k])
+        keep.append(kk)
+    f, uv = _outputs(frames[0], arr[0].height, arr[0].width, out)
+    h = _ctx(ctx)
+    _check(lib().oflow_lk(h, arr, iframe, C.byref(p), C.byref(f)), h)
+    return uv
+
+
+def pyrlk(I0, I1, params: LKParams | None = None, ctx: Context | None = None, out=None):
+    p = (params or LKParams()).c()
+    a, ka = _image(I0)
+    b, kb = _image(I1)
+    f, uv = _outputs(I0, a.height, a.width, out)
+    h = _ctx(ctx)
+    _check(lib().oflow_pyrlk(h, C.byref(a), C.byref(b), C.byref(p), C.byref(f)), h)
+    return uv
+
+
+from .compat import TV_L1, ComputeFlow, LucasKanade, deleteFlow_mem, initFlow  # noqa: E402

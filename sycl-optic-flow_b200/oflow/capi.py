@@ -1,0 +1,113 @@
+"""ctypes declarations of include/oflow.h and the loader of liboflow.so.
+
+The library is built in-tree (``make -C sycl-optic-flow_b200``) and loaded
+from there; there is no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.environ.get("OFLOW_LIB", os.path.join(os.path.dirname(HERE), "liboflow.so"))
+
+MAX_SCALES = 16
+MAX_WARPS = 32
+
+
+class OflowError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(msg)
+        self.status = status
+
+
+class Image(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("width", C.c_int), ("height", C.c_int),
+                ("pitch", C.c_int), ("dtype", C.c_int), ("location", C.c_int)]
+
+
+class Flow(C.Structure):
+    _fields_ = [("u", C.POINTER(C.c_float)), ("v", C.POINTER(C.c_float)),
+                ("pitch", C.c_int), ("location", C.c_int)]
+
+
+class Tvl1Params(C.Structure):
+    _fields_ = [("tau", C.c_float), ("lambda_", C.c_float), ("theta", C.c_float),
+                ("nscales", C.c_int), ("zfactor", C.c_float), ("warps", C.c_int),
+                ("epsilon", C.c_float), ("max_iterations", C.c_int)]
+
+
+class Tvl1Stats(C.Structure):
+    _fields_ = [("nscales", C.c_int), ("warps", C.c_int),
+                ("iterations", C.c_int * (MAX_SCALES * MAX_WARPS)), ("energy", C.c_double)]
+
+
+class Tvl1Profile(C.Structure):
+    _fields_ = [("total_ms", C.c_double), ("iter_ms", C.c_double), ("warp_ms", C.c_double),
+                ("iter_launches", C.c_int), ("warp_launches", C.c_int), ("launches", C.c_int)]
+
+
+class HsParams(C.Structure):
+    _fields_ = [("alpha", C.c_float), ("nlevels", C.c_int), ("nwarp", C.c_int),
+                ("nsolver", C.c_int)]
+
+
+class LkParams(C.Structure):
+    _fields_ = [("spac", C.c_int), ("temp", C.c_int), ("window", C.c_int), ("levels", C.c_int),
+                ("iters", C.c_int)]
+
+
+# every entry point of include/oflow.h: name -> (restype, argtypes)
+_VP, _I = C.c_void_p, C.c_int
+SIGNATURES = {
+    "oflow_abi_version": (_I, []),
+    "oflow_status_string": (C.c_char_p, [_I]),
+    "oflow_ctx_create": (_I, [_I, C.POINTER(C.c_void_p)]),
+    "oflow_ctx_destroy": (_I, [_VP]),
+    "oflow_ctx_set_stream": (_I, [_VP, _VP]),
+    "oflow_ctx_trim": (_I, [_VP]),
+    "oflow_ctx_last_error": (C.c_char_p, [_VP]),
+    "oflow_tvl1_default_params": (None, [C.POINTER(Tvl1Params)]),
+    "oflow_tvl1_nscales": (_I, [_I, _I, C.POINTER(Tvl1Params)]),
+    "oflow_tvl1": (_I, [_VP, C.POINTER(Image), C.POINTER(Image), C.POINTER(Tvl1Params),
+                        C.POINTER(Flow), C.POINTER(Tvl1Stats)]),
+    "oflow_tvl1_batch": (_I, [_VP, _I, C.POINTER(Image), C.POINTER(Image),
+                              C.POINTER(Tvl1Params), C.POINTER(Flow), C.POINTER(Tvl1Stats)]),
+    "oflow_tvl1_energy_trace": (_I, [_VP, C.POINTER(Image), C.POINTER(Image),
+                                     C.POINTER(Tvl1Params), C.POINTER(Flow),
+                                     C.POINTER(Tvl1Stats), C.POINTER(C.c_double)]),
+    "oflow_tvl1_batch_profile": (_I, [_VP, _I, C.POINTER(Image), C.POINTER(Image),
+                                      C.POINTER(Tvl1Params), C.POINTER(Flow),
+                                      C.POINTER(Tvl1Stats), C.POINTER(Tvl1Profile)]),
+    "oflow_hs_default_params": (None, [C.POINTER(HsParams)]),
+    "oflow_hs": (_I, [_VP, C.POINTER(Image), C.POINTER(Image), C.POINTER(HsParams),
+                      C.POINTER(Flow)]),
+    "oflow_hs_batch": (_I, [_VP, _I, C.POINTER(Image), C.POINTER(Image), C.POINTER(HsParams),
+                            C.POINTER(Flow)]),
+    "oflow_lk_default_params": (None, [C.POINTER(LkParams)]),
+    "oflow_lk": (_I, [_VP, C.POINTER(Image), _I, C.POINTER(LkParams), C.POINTER(Flow)]),
+    "oflow_pyrlk": (_I, [_VP, C.POINTER(Image), C.POINTER(Image), C.POINTER(LkParams),
+                         C.POINTER(Flow)]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load liboflow.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"liboflow.so not built (expected at {LIB_PATH}); "
+                          "run `make -C sycl-optic-flow_b200`")
+        h = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(h, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = h
+    return _lib
+
+
+def status_string(s: int) -> str:
+    return lib().oflow_status_string(s).decode()

@@ -1,0 +1,99 @@
+"""Horn-Schunck and Lucas-Kanade on the GPU through the C ABI against the
+oracle restatements (bit-identical by construction: same operation order, no
+FMA) and the golden fixtures."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+
+def _same(a, b):
+    return np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("alpha,L,nw,ns,w,h", [(15.0, 1, 1, 200, 320, 240), (0.2, 3, 2, 30, 320, 240),
+                                               (5.0, 2, 3, 7, 131, 77), (1.0, 1, 1, 1, 33, 17)])
+def test_hs_bit_identical_to_oracle(of, orc, ctx, alpha, L, nw, ns, w, h):
+    from oflow import synth
+    q = synth.hs_pair(seed=w + h, w=w, h=h)
+    u, v = of.hs(q.I0, q.I1, of.HSParams(alpha, L, nw, ns), ctx)
+    ou, ov = orc.hs(q.I0, q.I1, alpha, L, nw, ns)
+    assert _same(u, ou) and _same(v, ov)
+
+
+def test_hs_golden(of, ctx):
+    d = dict(np.load(os.path.join(GOLDEN, "hs_64x48.npz")))
+    u, v = of.hs(d["I0"], d["I1"], of.HSParams(15.0, 1, 1, 50), ctx)
+    assert _same(u, d["u"]) and _same(v, d["v"])
+    u, v = of.hs(d["I0"], d["I1"], of.HSParams(0.2, 3, 2, 20), ctx)
+    assert _same(u, d["u3"]) and _same(v, d["v3"])
+
+
+def test_hs_batch_and_compat(of, ctx):
+    from oflow import synth
+    qs = [synth.hs_pair(seed=s, w=160, h=120) for s in range(3)]
+    res = of.hs_batch([(q.I0, q.I1) for q in qs], of.HSParams(15.0, 1, 1, 40), ctx)
+    for q, (u, v) in zip(qs, res):
+        su, sv = of.hs(q.I0, q.I1, of.HSParams(15.0, 1, 1, 40), ctx)
+        assert _same(u, su) and _same(v, sv)
+    # ComputeFlow with a stride (src/hs/cuda/flow.cuh:21-31)
+    q = qs[0]
+    stride = 192
+    I0 = np.zeros((120, stride), np.float32)
+    I1 = np.zeros((120, stride), np.float32)
+    I0[:, :160], I1[:, :160] = q.I0, q.I1
+    U = np.zeros((120, stride), np.float32)
+    V = np.zeros((120, stride), np.float32)
+    of.initFlow(1, stride, 160, 120)
+    of.ComputeFlow(I0, I1, 160, 120, stride, 15.0, 1, 1, 40, U, V)
+    of.deleteFlow_mem(1)
+    assert _same(U[:, :160], res[0][0]) and _same(V[:, :160], res[0][1])
+
+
+@pytest.mark.parametrize("spac,temp,window", [(3, 2, 5), (1, 1, 3), (5, 3, 7), (7, 5, 9), (9, 9, 5)])
+def test_lk_single_step_bit_identical(of, orc, ctx, spac, temp, window):
+    from oflow import synth
+    rng = np.random.default_rng(spac * 10 + temp)
+    base = synth.value_noise(rng, 70, 110)
+    frames = [synth.quantize(base + rng.normal(0, 2, base.shape) + k) for k in range(temp)]
+    for iframe in (0, temp - 1, 2 * temp + 1):
+        u, v = of.lk(frames, iframe, of.LKParams(spac, temp, window), ctx)
+        ou, ov = orc.lk_ring(frames, iframe, spac, temp, window)
+        assert _same(u, ou) and _same(v, ov), iframe
+
+
+def test_lk_golden_and_compat(of, ctx):
+    d = dict(np.load(os.path.join(GOLDEN, "lk_80x60.npz")))
+    u, v = of.lk([d["f0"], d["f1"]], 1, of.LKParams(3, 2, 5), ctx)
+    assert _same(u, d["su"]) and _same(v, d["sv"])
+    lk = of.LucasKanade(3, 2, 5, 80, 60)
+    lk.copy_frames_circularbuffer_GPU_wrapper(d["f0"].ravel(), 2, 0, 80 * 60)
+    lk.copy_frames_circularbuffer_GPU_wrapper(d["f1"].ravel(), 2, 1, 80 * 60)
+    Vx = np.zeros(80 * 60, np.float32)
+    Vy = np.zeros(80 * 60, np.float32)
+    lk.lucas_kanade(Vx, Vy, 1)
+    assert _same(Vx.reshape(60, 80), d["su"]) and _same(Vy.reshape(60, 80), d["sv"])
+
+
+@pytest.mark.parametrize("levels,iters,window,w,h", [(3, 3, 5, 640, 480), (2, 1, 3, 97, 61),
+                                                     (4, 2, 7, 320, 240)])
+def test_pyrlk_bit_identical(of, orc, ctx, levels, iters, window, w, h):
+    from oflow import synth
+    l = synth.lk_pair(seed=w, w=w, h=h)
+    u, v = of.pyrlk(l.I0, l.I1, of.LKParams(3, 2, window, levels, iters), ctx)
+    ou, ov = orc.pyrlk(l.I0, l.I1, levels, iters, 3, window)
+    assert _same(u, ou) and _same(v, ov)
+
+
+def test_pyrlk_golden_and_accuracy(of, ctx):
+    from oflow import synth
+    d = dict(np.load(os.path.join(GOLDEN, "lk_80x60.npz")))
+    u, v = of.pyrlk(d["I0"], d["I1"], of.LKParams(3, 2, 5, 3, 3), ctx)
+    assert _same(u, d["pu"]) and _same(v, d["pv"])
+    l = synth.lk_pair(seed=0)
+    u, v = of.pyrlk(l.I0, l.I1, of.LKParams(), ctx)
+    assert synth.epe(u, v, l.u, l.v, l.valid, 8) < 1.0

@@ -1,0 +1,184 @@
+"""TV-L1 on the GPU through the C ABI against the oracle and the reference.
+
+Tolerances (north star): max |du|,|dv| <= 1e-3 px and |dEPE| <= 1e-4 px after
+the full solve; per-iteration energy within 1e-5 relative.  Against the C
+restatement with the same error-sum rounding (one rounding of a double sum)
+the kernels are bit-identical, and that is asserted where it holds by
+construction."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+TOL_FLOW = 1e-3
+TOL_EPE = 1e-4
+TOL_ENERGY = 1e-5
+
+
+def _pair(seed, w, h, **kw):
+    from oflow import synth
+    p = synth.tvl1_pair(seed=seed, w=w, h=h, radius=kw.pop("radius", min(w, h) / 5.0), **kw)
+    return p, synth.quantize(p.I0), synth.quantize(p.I1)
+
+
+def _oracle(orc, a, b, prm, mode=1):
+    return orc.tvl1(a.astype(np.float32), b.astype(np.float32),
+                    orc.TVL1Params(prm.tau, prm.lambda_, prm.theta, prm.nscales, prm.zfactor,
+                                   prm.warps, prm.epsilon, prm.max_iterations),
+                    error_mode=mode, trace=True)
+
+
+@pytest.mark.parametrize("w,h,ns,mi", [(97, 61, 100, 50), (64, 48, 3, 10), (131, 77, 4, 30),
+                                       (200, 150, 5, 50), (33, 17, 2, 5)])
+def test_bit_identical_to_oracle(of, orc, ctx, w, h, ns, mi):
+    _, a, b = _pair(w * h, w, h)
+    prm = of.TVL1Params(nscales=ns, max_iterations=mi)
+    u, v, st = of.tvl1(a, b, prm, ctx, stats=True)
+    ou, ov, its, _ = _oracle(orc, a, b, prm)
+    assert np.array_equal(st["iterations"], its)
+    assert np.array_equal(u, ou) and np.array_equal(v, ov)
+
+
+@pytest.mark.parametrize("zf,warps,eps", [(0.6, 3, 0.01), (0.75, 2, 0.0), (0.5, 1, 0.5)])
+def test_other_parameters(of, orc, ctx, zf, warps, eps):
+    _, a, b = _pair(17, 120, 90)
+    prm = of.TVL1Params(nscales=4, zfactor=zf, warps=warps, epsilon=eps, max_iterations=15)
+    u, v, st = of.tvl1(a, b, prm, ctx, stats=True)
+    ou, ov, its, _ = _oracle(orc, a, b, prm)
+    assert np.array_equal(st["iterations"], its)
+    assert np.array_equal(u, ou) and np.array_equal(v, ov)
+
+
+@pytest.mark.parametrize("name", ["tvl1_97x61.npz", "tvl1_160x96.npz", "tvl1_128x64_w2.npz"])
+def test_golden_reference_outputs(of, ctx, name):
+    d = dict(np.load(os.path.join(GOLDEN, name)))
+    prm = of.TVL1Params(float(d["tau"]), float(d["lambda_"]), float(d["theta"]),
+                        int(d["nscales"]), float(d["zfactor"]), int(d["warps"]),
+                        float(d["epsilon"]), int(d["max_iterations"]))
+    u, v = of.tvl1(d["I0"], d["I1"], prm, ctx)
+    assert max(np.abs(u - d["u"]).max(), np.abs(v - d["v"]).max()) <= TOL_FLOW
+
+
+def test_energy_per_iteration(of, orc, ctx):
+    _, a, b = _pair(23, 128, 96)
+    prm = of.TVL1Params(nscales=3, max_iterations=12)
+    u, v, st, en = of.tvl1_energy_trace(a, b, prm, ctx)
+    ou, ov, its, oen = _oracle(orc, a, b, prm)
+    assert np.array_equal(np.isnan(en), np.isnan(oen))
+    m = ~np.isnan(oen)
+    assert m.sum() == its.sum()
+    assert np.max(np.abs(en[m] - oen[m]) / np.abs(oen[m])) <= TOL_ENERGY
+    assert np.array_equal(u, ou)
+
+
+def test_stats_energy_is_final_energy(of, orc, ctx):
+    _, a, b = _pair(29, 96, 64)
+    prm = of.TVL1Params(nscales=3, max_iterations=8)
+    _, _, st = of.tvl1(a, b, prm, ctx, stats=True)
+    _, _, _, en = of.tvl1_energy_trace(a, b, prm, ctx)
+    last = en[0, -1][~np.isnan(en[0, -1])][-1]
+    assert abs(st["energy"] - last) <= TOL_ENERGY * abs(last)
+
+
+def test_batch_equals_single_and_mixed_sizes(of, ctx):
+    specs = [(31, 96, 64), (32, 96, 64), (33, 120, 80), (34, 96, 64), (35, 64, 64)]
+    pairs = [_pair(s, w, h)[1:] for s, w, h in specs]
+    prm = of.TVL1Params(nscales=3, max_iterations=20)
+    batch, stats = of.tvl1_batch(pairs, prm, ctx, stats=True)
+    for (a, b), (u, v), st in zip(pairs, batch, stats):
+        su, sv, ss = of.tvl1(a, b, prm, ctx, stats=True)
+        assert np.array_equal(u, su) and np.array_equal(v, sv)
+        assert np.array_equal(st["iterations"], ss["iterations"])
+
+
+def test_u8_and_f32_inputs_agree(of, ctx):
+    _, a, b = _pair(41, 100, 70)
+    prm = of.TVL1Params(nscales=3, max_iterations=10)
+    u1, v1 = of.tvl1(a, b, prm, ctx)
+    u2, v2 = of.tvl1(a.astype(np.float32), b.astype(np.float32), prm, ctx)
+    assert np.array_equal(u1, u2) and np.array_equal(v1, v2)
+
+
+def test_device_and_pitched_buffers(of, ctx):
+    import torch
+    _, a, b = _pair(43, 100, 70)
+    prm = of.TVL1Params(nscales=3, max_iterations=10)
+    u, v = of.tvl1(a, b, prm, ctx)
+    # pitched host frames
+    pa = np.zeros((70, 128), np.uint8)
+    pb = np.zeros((70, 128), np.uint8)
+    pa[:, :100], pb[:, :100] = a, b
+    up, vp = of.tvl1(pa[:, :100], pb[:, :100], prm, ctx)
+    assert np.array_equal(u, up) and np.array_equal(v, vp)
+    # device frames, device (pitched) outputs
+    da = torch.from_numpy(pa).cuda()[:, :100]
+    db = torch.from_numpy(pb).cuda()[:, :100]
+    ou = torch.zeros((70, 112), dtype=torch.float32, device="cuda")[:, :100]
+    ov = torch.zeros((70, 112), dtype=torch.float32, device="cuda")[:, :100]
+    of.tvl1(da, db, prm, ctx, out=(ou, ov))
+    torch.cuda.synchronize()
+    assert np.array_equal(ou.cpu().numpy(), u) and np.array_equal(ov.cpu().numpy(), v)
+
+
+def test_full_size_workload_against_oracle_and_reference(of, orc, ctx):
+    """1024x436, 5 scales x 5 warps x 50 iterations (the benchmark workload)."""
+    from oflow import synth
+    p, a, b = _pair(0, 1024, 436, radius=80.0)
+    prm = of.TVL1Params(nscales=5, max_iterations=50)
+    u, v, st = of.tvl1(a, b, prm, ctx, stats=True)
+    ou, ov, its, _ = _oracle(orc, a, b, prm, mode=1)
+    assert np.array_equal(st["iterations"], its)
+    assert np.array_equal(u, ou) and np.array_equal(v, ov)
+    if orc.ref_available():
+        ru, rv = orc.ref_tvl1(a, b, orc.TVL1Params(nscales=5, max_iterations=50))
+        assert max(np.abs(u - ru).max(), np.abs(v - rv).max()) <= TOL_FLOW
+        e_gpu = synth.epe(u, v, p.u, p.v, p.valid, 8)
+        e_ref = synth.epe(ru, rv, p.u, p.v, p.valid, 8)
+        assert abs(e_gpu - e_ref) <= TOL_EPE
+    assert synth.epe(u, v, p.u, p.v, p.valid, 8) < 0.5
+
+
+def test_known_answers_on_gpu(of, ctx):
+    I = np.full((96, 128), 90, np.uint8)
+    u, v = of.tvl1(I, I, of.TVL1Params(nscales=3, max_iterations=20), ctx)
+    assert np.all(u == 0) and np.all(v == 0)
+    from oflow import synth
+    rng = np.random.default_rng(2)
+    big = synth._blur(rng.uniform(0, 255, (160, 220)), 2.0)
+    I0 = synth.quantize(big[10:150, 10:210])
+    I1 = synth.quantize(big[10:150, 7:207])   # I1(x + 3) = I0(x)
+    u, v = of.tvl1(I0, I1, of.TVL1Params(nscales=4, max_iterations=50), ctx)
+    assert abs(float(np.median(u[16:-16, 16:-16])) - 3.0) < 0.05
+
+
+def test_errors_are_status_codes(of, ctx):
+    small = np.zeros((4, 4), np.uint8)
+    with pytest.raises(of.OflowError) as e:
+        of.tvl1(small, small, of.TVL1Params(), ctx)
+    assert e.value.status == 1
+    with pytest.raises(of.OflowError) as e:
+        of.tvl1(np.zeros((32, 32), np.uint8), np.zeros((32, 40), np.uint8), of.TVL1Params(), ctx)
+    assert e.value.status == 1
+    # the context stays usable
+    u, v = of.tvl1(np.zeros((32, 32), np.uint8), np.zeros((32, 32), np.uint8),
+                   of.TVL1Params(nscales=2, max_iterations=3), ctx)
+    assert np.all(u == 0)
+
+
+def test_reference_class_mirror(of, orc):
+    """TV_L1 with both reference call forms (sequential uint8 pair; streaming
+    float frames paired with the previous call)."""
+    _, a, b = _pair(51, 96, 64)
+    t = of.TV_L1(96, 64, nscales=3, max_iterations=10)
+    t.runDualTVL1Multiscale(a, b)
+    U = t.getU().copy()
+    u, v = of.tvl1(a, b, of.TVL1Params(nscales=3, max_iterations=10))
+    assert np.array_equal(U[: 96 * 64], u.ravel()) and np.array_equal(U[96 * 64:], v.ravel())
+    s = of.TV_L1(96, 64, nscales=3, max_iterations=10)
+    s.runDualTVL1Multiscale(a.astype(np.float32).ravel())
+    s.runDualTVL1Multiscale(b.astype(np.float32).ravel())
+    assert np.array_equal(s.getU(), U)
