@@ -346,12 +346,30 @@ def our_arm(args, rank, world, local_rank):
                      "algorithmic_bytes_per_launch": alg_iter / max(prof["iter_launches"], 1),
                      "launch_ms_avg": prof["iter_ms"] / max(prof["iter_launches"], 1),
                      "iter_share_of_step": prof["iter_ms"] / prof["total_ms"]
-                     if prof["total_ms"] else None},
+                     if prof["total_ms"] else None,
+                     "iter_ms_per_scale": [round(x, 3) for x in
+                                           prof["iter_ms_scale"][:stats[0]["nscales"]]],
+                     "profile_total_ms": round(prof["total_ms"], 3)},
         "clocks": clocks,
     }
     if cpu:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
+    return 0
+
+
+def once(args):
+    """Profiling case: one solve of --batch pairs with --nscales / --iters."""
+    import torch
+    import oflow
+    pairs = make_pairs(args.batch, 0)
+    dev = torch.device("cuda", 0)
+    d_in = [(torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)) for a, b, _ in pairs]
+    prm = oflow.TVL1Params(nscales=args.nscales, max_iterations=args.iters)
+    ctx = oflow.Context(0)
+    res, st = oflow.tvl1_batch(d_in, prm, ctx, stats=True)
+    torch.cuda.synchronize()
+    log("iterations per pair:", [int(s["iterations"].sum()) for s in st])
     return 0
 
 
@@ -366,6 +384,10 @@ def main():
     ap.add_argument("--cpu-pairs", type=int, default=30)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--cpu-worker", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--once", action="store_true",
+                    help="one solve of --batch device-resident pairs and exit (profiling case)")
+    ap.add_argument("--nscales", type=int, default=PARAMS["nscales"])
+    ap.add_argument("--iters", type=int, default=PARAMS["max_iterations"])
     args = ap.parse_args()
     if args.cpu_worker:
         return cpu_worker(args)
@@ -377,6 +399,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         return reference_arm(args, rank)
+    if args.once:
+        return once(args)
     return our_arm(args, rank, world, local_rank)
 
 

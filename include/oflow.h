@@ -140,6 +140,7 @@ typedef struct {
     int iter_launches;
     int warp_launches;
     int launches;          /* all kernel launches of the schedule */
+    double iter_ms_scale[OFLOW_MAX_SCALES]; /* inner-iteration time per scale */
 } oflow_tvl1_profile;
 
 /* Like oflow_tvl1_batch (outputs and stats included) with the timings above. */

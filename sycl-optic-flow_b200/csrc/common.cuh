@@ -10,12 +10,17 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "exact_math.cuh"
+
 #include <climits>
+#include <cmath>
 #include <cstddef>
+#include <cstring>
 
 namespace oflow {
 
 constexpr int kNumSMs = 148;
+
 
 __host__ __device__ inline int div_up(int a, int b) { return (a + b - 1) / b; }
 __host__ __device__ inline int imin(int a, int b) { return a < b ? a : b; }
@@ -103,13 +108,6 @@ __device__ __forceinline__ float bicubic_at(const float *__restrict__ in, float 
                           s.ty);
     }
     return cubic_cell(v[0], v[1], v[2], v[3], s.tx);
-}
-
-// Single-precision hypot exactly as glibc's hypotf: the squares are exact in
-// double, one rounding for the sum, one for the square root, one to single.
-__device__ __forceinline__ float hypot_ref(float a, float b) {
-    const double da = a, db = b;
-    return (float)sqrt(da * da + db * db);
 }
 
 // Bilinear sample, clamp-to-edge taps, coordinate first limited to [-1, n].

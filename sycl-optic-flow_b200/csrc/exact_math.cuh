@@ -1,0 +1,78 @@
+// Exactly rounded single-precision helpers shared by host and device code.
+// Each function returns bit-for-bit what the reference's x86 build computes
+// for the same expression (IEEE single/double, no contraction), but with
+// cheaper instruction sequences on the GPU.  They are compiled on the host as
+// well, so tests can check them against the plain expressions on the CPU.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+
+namespace oflow {
+
+#ifdef __CUDA_ARCH__
+__device__ __forceinline__ float __int_as_float_hd(int i) { return __int_as_float(i); }
+__device__ __forceinline__ int __float_as_int_hd(float f) { return __float_as_int(f); }
+#else
+inline float __int_as_float_hd(int i) { float f; memcpy(&f, &i, 4); return f; }
+inline int __float_as_int_hd(float f) { int i; memcpy(&i, &f, 4); return i; }
+#endif
+
+// Single-precision hypot exactly as glibc's hypotf: the squares are exact in
+// double, one rounding for the sum, one for the square root, one to single.
+__host__ __device__ __forceinline__ float hypot_ref(float a, float b) {
+    const double da = a, db = b;
+    return (float)sqrt(da * da + db * db);
+}
+
+#ifdef __CUDA_ARCH__
+#define OF_FMAF(a, b, c) __fmaf_rn(a, b, c)
+#define OF_RCP(x) __frcp_rn(x)
+#else
+#define OF_FMAF(a, b, c) fmaf(a, b, c)
+#define OF_RCP(x) (1.0f / (x))
+#endif
+
+// hypot_ref without double arithmetic on the common path.  With S = a^2+b^2
+// held exactly as float pairs, y0 = sqrt(RN(ah+bh)) is within one ulp of the
+// result.  The residual e = S - y0^2 (error < 2^-46 S) places sqrt(S) relative
+// to the midpoints y0 +- ulp/2 (at |e| = y0*ulp to first order).  When it is
+// more than 2^-20 of that distance away, single rounding of sqrt(S) and the
+// reference's double-then-single rounding agree, and the fast answer is
+// returned; otherwise (and for zero, tiny, huge or non-finite input) the
+// double formula decides.
+__host__ __device__ __forceinline__ float hypot_fast(float a, float b) {
+    a = fabsf(a);
+    b = fabsf(b);
+    const float big = fmaxf(a, b), small = fminf(a, b);
+    if (small == 0.0f && big == big) return big;  // sqrt(x^2) = |x| exactly
+    if (!(big < 0x1p60f) || !(small > 0x1p-60f)) return hypot_ref(a, b);
+    const float bh = big * big, bl = OF_FMAF(big, big, -bh);
+    const float sh = small * small, sl = OF_FMAF(small, small, -sh);
+    const float y0 = sqrtf(bh + sh);
+    const float yh = y0 * y0, yl = OF_FMAF(y0, y0, -yh);
+    // (bh - yh) and the following add are exact (Sterbenz); the low parts
+    // carry errors far below the threshold
+    const float e = ((bh - yh) + sh) + ((bl + sl) - yl);
+    const float ulp = __int_as_float_hd((__float_as_int_hd(y0) & 0x7f800000) - (23 << 23));
+    const float T = y0 * ulp;
+    const float margin = T * 0x1p-20f;
+    if (fabsf(e) < T - margin) return y0;
+    if (e > T + margin) return __int_as_float_hd(__float_as_int_hd(y0) + 1);
+    if (e < -(T + margin)) return __int_as_float_hd(__float_as_int_hd(y0) - 1);
+    return hypot_ref(a, b);
+}
+
+// p / g correctly rounded (IEEE division) from y = RN(1/g): q0 = RN(p*y),
+// r = p - q0*g (exact by FMA), q = RN(q0 + r*y) (Markstein).  Valid while
+// neither the quotient nor p underflows; smaller p take the plain division.
+__host__ __device__ __forceinline__ float div_by_rcp(float p, float g, float y) {
+    if (!(fabsf(p) > 0x1p-100f)) return p / g;
+    const float q0 = p * y;
+    const float r = OF_FMAF(-q0, g, p);
+    return OF_FMAF(r, y, q0);
+}
+
+}  // namespace oflow

@@ -31,6 +31,9 @@ namespace oflow {
 
 // ---------------------------------------------------------------- constants
 constexpr int kIterTW = 32, kIterTH = 8, kIterNT = 256;
+// blocked inner iterations: tile, halo = iterations per launch, threads
+constexpr int kTbTW = 64, kTbTH = 16, kTbK = 4, kTbNT = 256;
+constexpr size_t kTbSmem = (size_t)(kTbTW + 2 * kTbK) * (kTbTH + 2 * kTbK) * 40;
 constexpr int kGaussTW = 32, kGaussTH = 16, kGaussNT = 256, kGaussMaxR = 15;
 constexpr int kIngestNT = 256, kIngestPPT = 8;
 
@@ -73,7 +76,7 @@ struct TvCtrl {
     unsigned arrive;    // arrival counter of the last-block reduction
     float norm_min, norm_den;
     int norm_apply;
-    int pad0;
+    int redo;           // >0: the next launch re-runs this many iterations (early stop mid-block)
     double energy;
     double pad1[3];
 };
@@ -165,6 +168,7 @@ __global__ void k_norm_finalize(const NormRec *recs, int nblk, TvCtrl *ctrl) {
         ctrl[b].n = 0;
         ctrl[b].stop = 0;
         ctrl[b].arrive = 0;
+        ctrl[b].redo = 0;
     }
 }
 
@@ -312,6 +316,7 @@ __global__ void k_warp(const float *__restrict__ pyr, size_t pyr_stride, const f
         ctrl[b].n = 0;
         ctrl[b].stop = 0;
         ctrl[b].arrive = 0;
+        ctrl[b].redo = 0;
     }
     if (x >= nx || y >= ny) return;
     const int cur = ctrl[b].cur;
@@ -371,6 +376,48 @@ __device__ __forceinline__ float div_border(float a1c, float a1l, float a2c, flo
     return -a1l - a2u;
 }
 
+// TH step (tvl1.cpp:221-245) and u update (:252-265) for one pixel.
+__device__ __forceinline__ float2 th_u_update(float2 u, float4 w, float4 pc, float4 pl,
+                                              float4 pu, bool L, bool R, bool T, bool B,
+                                              float l_t, float theta) {
+    const float rho = w.z + (w.x * u.x + w.y * u.y);
+    const float lg = l_t * w.w;
+    float d1, d2;
+    if (!(rho >= -lg)) {
+        d1 = l_t * w.x;
+        d2 = l_t * w.y;
+    } else if (rho > lg) {
+        d1 = -l_t * w.x;
+        d2 = -l_t * w.y;
+    } else if (w.w < 1E-10f) {
+        d1 = d2 = 0.0f;
+    } else {
+        const float fi = -rho / w.w;
+        d1 = fi * w.x;
+        d2 = fi * w.y;
+    }
+    const float v1 = u.x + d1, v2 = u.y + d2;
+    const float div1 = div_border(pc.x, pl.x, pc.y, pu.y, L, R, T, B);
+    const float div2 = div_border(pc.z, pl.z, pc.w, pu.w, L, R, T, B);
+    return make_float2(v1 + theta * div1, v2 + theta * div2);
+}
+
+// Dual update (tvl1.cpp:268-291) from the forward differences of u(new):
+// g = 1 + tau/theta*hypot(grad u), p = (p + tau/theta*grad u) / g, with the
+// hypot and the divisions in their exact fast forms (exact_math.cuh).
+__device__ __forceinline__ float4 dual_update(float4 po, float f1x, float f1y, float f2x,
+                                              float f2y, float taut) {
+    const float g1 = 1.0f + taut * hypot_fast(f1x, f1y);
+    const float g2 = 1.0f + taut * hypot_fast(f2x, f2y);
+    const float r1 = OF_RCP(g1), r2 = OF_RCP(g2);
+    float4 pn;
+    pn.x = div_by_rcp(taut * f1x + po.x, g1, r1);
+    pn.y = div_by_rcp(taut * f1y + po.y, g1, r1);
+    pn.z = div_by_rcp(taut * f2x + po.z, g2, r2);
+    pn.w = div_by_rcp(taut * f2y + po.w, g2, r2);
+    return pn;
+}
+
 struct IterArgs {
     const float4 *W;
     float2 *U0, *U1;
@@ -428,29 +475,9 @@ __global__ void __launch_bounds__(NT) k_tvl1_iter(IterArgs a) {
         const size_t p = (size_t)y * nx + x;
         const float2 u = Uin[p];
         const float4 w = W[p];
-        const float rho = w.z + (w.x * u.x + w.y * u.y);
-        const float lg = a.l_t * w.w;
-        float d1, d2;
-        if (!(rho >= -lg)) {
-            d1 = a.l_t * w.x;
-            d2 = a.l_t * w.y;
-        } else if (rho > lg) {
-            d1 = -a.l_t * w.x;
-            d2 = -a.l_t * w.y;
-        } else if (w.w < 1E-10f) {
-            d1 = d2 = 0.0f;
-        } else {
-            const float fi = -rho / w.w;
-            d1 = fi * w.x;
-            d2 = fi * w.y;
-        }
-        const float v1 = u.x + d1, v2 = u.y + d2;
         const float4 *c = sP + (ry + 1) * (TW + 2) + (rx + 1);
-        const float4 pc = c[0], pl = c[-1], pu = c[-(TW + 2)];
-        const bool L = x == 0, R = x == nx - 1, T = y == 0, B = y == ny - 1;
-        const float div1 = div_border(pc.x, pl.x, pc.y, pu.y, L, R, T, B);
-        const float div2 = div_border(pc.z, pl.z, pc.w, pu.w, L, R, T, B);
-        const float2 un = make_float2(v1 + a.theta * div1, v2 + a.theta * div2);
+        const float2 un = th_u_update(u, w, c[0], c[-1], c[-(TW + 2)], x == 0, x == nx - 1,
+                                      y == 0, y == ny - 1, a.l_t, a.theta);
         sU[i] = un;
         if (rx < TW && ry < TH) {
             Uout[p] = un;
@@ -477,14 +504,7 @@ __global__ void __launch_bounds__(NT) k_tvl1_iter(IterArgs a) {
             f1y = ud.x - uc.x;
             f2y = ud.y - uc.y;
         }
-        const float g1 = 1.0f + a.taut * hypot_ref(f1x, f1y);
-        const float g2 = 1.0f + a.taut * hypot_ref(f2x, f2y);
-        const float4 po = sP[(ry + 1) * (TW + 2) + rx + 1];
-        float4 pn;
-        pn.x = (a.taut * f1x + po.x) / g1;
-        pn.y = (a.taut * f1y + po.y) / g1;
-        pn.z = (a.taut * f2x + po.z) / g2;
-        pn.w = (a.taut * f2y + po.w) / g2;
+        const float4 pn = dual_update(sP[(ry + 1) * (TW + 2) + rx + 1], f1x, f1y, f2x, f2y, a.taut);
         Pout[(size_t)y * nx + x] = pn;
     }
 
@@ -512,6 +532,224 @@ __global__ void __launch_bounds__(NT) k_tvl1_iter(IterArgs a) {
         a.iters[(size_t)b * a.iter_stride + a.stage] = n;
         ctrl->cur = cur ^ 1;
         if (!(e > a.eps2)) ctrl->stop = 1;
+        ctrl->arrive = 0;
+        __threadfence();
+    }
+}
+
+
+// ---------------------------------------------------------------- blocked iterations
+// Up to K inner iterations per launch on a TW x TH tile held in shared memory
+// with a K-pixel halo (the dependency cone of one iteration is one pixel in
+// every direction, so after K iterations the owned tile is exact).  The state
+// is loaded once and stored once per launch, so HBM traffic per iteration
+// drops by about K.  Each iteration's squared change over the owned pixels is
+// kept; the last block of a pair finds the first iteration that meets the
+// stopping rule (tvl1.cpp:216).  If that is not the last iteration of the
+// launch, nothing is accepted and the next launch re-runs exactly that many
+// iterations from the untouched input buffers.
+struct TbArgs {
+    const float4 *W;
+    float2 *U0, *U1;
+    float4 *P0, *P1;
+    size_t stride;
+    int nx, ny, max_it;
+    float l_t, theta, taut, eps2;
+    TvCtrl *ctrl;
+    double *partials;  // [B][max_tiles][K]
+    int max_tiles;
+    int *iters;
+    int iter_stride, stage;
+};
+
+// Visits the inclusive rectangle [x0,x1] x [y0,y1] of a region of width RW
+// with NT threads, one pixel per step (one division per call).
+template <int NT, typename F>
+__device__ __forceinline__ void for_rect(int x0, int x1, int y0, int y1, F &&f) {
+    const int w = x1 - x0 + 1, n = w * (y1 - y0 + 1);
+    if (n <= 0) return;
+    const int t = threadIdx.x;
+    int rx = x0 + t % w, ry = y0 + t / w;
+    const int sx = NT % w, sy = NT / w;
+    for (int k = t; k < n; k += NT) {
+        f(rx, ry);
+        rx += sx;
+        ry += sy;
+        if (rx > x1) {
+            rx -= w;
+            ry += 1;
+        }
+    }
+}
+
+// One blocked iteration j (1-based) over the region.  Phase B (TH + u update)
+// covers [j, RW-j]^2 and phase C (dual update) [j, RW-1-j]^2: exactly the
+// pixels whose values reach the owned tile after K iterations, so no read
+// ever leaves the region.  INTERIOR: no region pixel lies on the image border
+// (no bounds or border tests).
+template <int TW, int TH, int K, int NT, bool INTERIOR>
+__device__ __forceinline__ void tb_iteration(int j, float4 *sP, const float4 *sW, float2 *sU,
+                                             int ox, int oy, int nx, int ny, float l_t,
+                                             float theta, float taut, double &err) {
+    constexpr int RW = TW + 2 * K, RH = TH + 2 * K;
+    for_rect<NT>(j, RW - j, j, RH - j, [&](int rx, int ry) {
+        const int i = ry * RW + rx;
+        const int x = ox + rx, y = oy + ry;
+        if (!INTERIOR && (x >= nx || y >= ny || x < 0 || y < 0)) return;
+        const float2 u = sU[i];
+        const float2 un = th_u_update(u, sW[i], sP[i], sP[i - 1], sP[i - RW],
+                                      !INTERIOR && x == 0, !INTERIOR && x == nx - 1,
+                                      !INTERIOR && y == 0, !INTERIOR && y == ny - 1, l_t, theta);
+        sU[i] = un;
+        if (rx >= K && rx < K + TW && ry >= K && ry < K + TH) {
+            const float e1 = un.x - u.x, e2 = un.y - u.y;
+            const float term = e1 * e1 + e2 * e2;
+            err += (double)term;
+        }
+    });
+    __syncthreads();
+    for_rect<NT>(j, RW - 1 - j, j, RH - 1 - j, [&](int rx, int ry) {
+        const int i = ry * RW + rx;
+        const int x = ox + rx, y = oy + ry;
+        if (!INTERIOR && (x >= nx || y >= ny || x < 0 || y < 0)) return;
+        const float2 uc = sU[i];
+        float f1x = 0.0f, f2x = 0.0f, f1y = 0.0f, f2y = 0.0f;
+        if (INTERIOR || x < nx - 1) {
+            const float2 ur = sU[i + 1];
+            f1x = ur.x - uc.x;
+            f2x = ur.y - uc.y;
+        }
+        if (INTERIOR || y < ny - 1) {
+            const float2 ud = sU[i + RW];
+            f1y = ud.x - uc.x;
+            f2y = ud.y - uc.y;
+        }
+        sP[i] = dual_update(sP[i], f1x, f1y, f2x, f2y, taut);
+    });
+    __syncthreads();
+}
+
+template <int TW, int TH, int K, int NT>
+__global__ void __launch_bounds__(NT) k_tvl1_tb(TbArgs a) {
+    constexpr int RW = TW + 2 * K, RH = TH + 2 * K, RN = RW * RH;
+    extern __shared__ float4 tb_smem[];
+    float4 *sP = tb_smem;                                  // RN
+    float4 *sW = sP + RN;                                  // RN
+    float2 *sU = reinterpret_cast<float2 *>(sW + RN);      // RN
+    __shared__ double sred[NT / 32];
+    __shared__ double sE[K];
+    __shared__ int s_last;
+
+    const int b = blockIdx.z;
+    TvCtrl *ctrl = a.ctrl + b;
+    if (*((volatile int *)&ctrl->stop)) return;
+    const int cur = *((volatile int *)&ctrl->cur);
+    const int redo = *((volatile int *)&ctrl->redo);
+    const int n0 = *((volatile int *)&ctrl->n);
+    const int kk = redo > 0 ? redo : imin(K, a.max_it - n0);
+    const int nx = a.nx, ny = a.ny;
+    const size_t off = (size_t)b * a.stride;
+    const float2 *__restrict__ Uin = (cur ? a.U1 : a.U0) + off;
+    float2 *__restrict__ Uout = (cur ? a.U0 : a.U1) + off;
+    const float4 *__restrict__ Pin = (cur ? a.P1 : a.P0) + off;
+    float4 *__restrict__ Pout = (cur ? a.P0 : a.P1) + off;
+    const float4 *__restrict__ Wg = a.W + off;
+    const int ox = blockIdx.x * TW - K, oy = blockIdx.y * TH - K;
+    const bool interior = ox >= 1 && oy >= 1 && ox + RW <= nx - 1 && oy + RH <= ny - 1;
+
+    // all loads of the region issued before any use
+    for (int i = threadIdx.x; i < RN; i += NT) {
+        const int x = ox + i % RW, y = oy + i / RW;
+        float4 p = make_float4(0.f, 0.f, 0.f, 0.f), w = p;
+        float2 u = make_float2(0.f, 0.f);
+        if (x >= 0 && x < nx && y >= 0 && y < ny) {
+            const size_t q = (size_t)y * nx + x;
+            p = Pin[q];
+            w = Wg[q];
+            u = Uin[q];
+        }
+        sP[i] = p;
+        sW[i] = w;
+        sU[i] = u;
+    }
+    __syncthreads();
+
+    double err[K];
+#pragma unroll
+    for (int j = 0; j < K; j++) {
+        err[j] = 0.0;
+        if (j < kk) {  // uniform over the block
+            if (interior)
+                tb_iteration<TW, TH, K, NT, true>(j + 1, sP, sW, sU, ox, oy, nx, ny, a.l_t,
+                                                  a.theta, a.taut, err[j]);
+            else
+                tb_iteration<TW, TH, K, NT, false>(j + 1, sP, sW, sU, ox, oy, nx, ny, a.l_t,
+                                                   a.theta, a.taut, err[j]);
+        }
+    }
+    for (int i = threadIdx.x; i < TW * TH; i += NT) {
+        const int tx = i % TW, ty = i / TW;
+        const int x = ox + K + tx, y = oy + K + ty;
+        if (x >= nx || y >= ny) continue;
+        const int r = (ty + K) * RW + tx + K;
+        const size_t q = (size_t)y * nx + x;
+        Uout[q] = sU[r];
+        Pout[q] = sP[r];
+    }
+
+    // ---- per-iteration error sums and the stopping decision
+    const int ntiles = gridDim.x * gridDim.y;
+    const int tile = blockIdx.y * gridDim.x + blockIdx.x;
+    double *part = a.partials + (size_t)b * a.max_tiles * K;
+#pragma unroll
+    for (int j = 0; j < K; j++) {
+        if (j < kk) {  // kk is uniform over the block
+            const double s = block_sum_double<NT>(err[j], sred);
+            if (threadIdx.x == 0) part[(size_t)tile * K + j] = s;
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned prev = atomicAdd(&ctrl->arrive, 1u);
+        s_last = (prev == (unsigned)ntiles - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    for (int j = 0; j < kk; j++) {
+        double acc = 0.0;
+        for (int t = threadIdx.x; t < ntiles; t += NT) acc += __ldcg(part + (size_t)t * K + j);
+        const double tot = block_sum_double<NT>(acc, sred);
+        if (threadIdx.x == 0) sE[j] = tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const float npx = (float)(nx * ny);
+        if (redo > 0) {
+            ctrl->n = n0 + redo;
+            ctrl->cur = cur ^ 1;
+            ctrl->stop = 1;
+            ctrl->redo = 0;
+        } else {
+            int stopj = 0;
+            for (int j = 0; j < kk; j++) {
+                float e = (float)sE[j];
+                e = e / npx;
+                if (!(e > a.eps2) || n0 + j + 1 >= a.max_it) {
+                    stopj = j + 1;
+                    break;
+                }
+            }
+            if (stopj == 0 || stopj == kk) {
+                ctrl->n = n0 + kk;
+                ctrl->cur = cur ^ 1;
+                if (stopj) ctrl->stop = 1;
+            } else {
+                ctrl->redo = stopj;
+            }
+        }
+        a.iters[(size_t)b * a.iter_stride + a.stage] = ctrl->n;
         ctrl->arrive = 0;
         __threadfence();
     }
@@ -622,7 +860,8 @@ TvPlan::TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, boo
 
     const size_t N0 = (size_t)w * h;
     N0_ = N0;
-    iter_blocks_ = div_up(w, kIterTW) * div_up(h, kIterTH);
+    iter_blocks_ = imax(div_up(w, kIterTW) * div_up(h, kIterTH),
+                        div_up(w, kTbTW) * div_up(h, kTbTH) * kTbK);
     ingest_blocks_ = imin(div_up((int)N0, kIngestNT * kIngestPPT), 1024);
     energy_blocks_ = imin(div_up((int)N0, kEnNT * 4), 512);
     max_blocks_ = imax(iter_blocks_, energy_blocks_);
@@ -651,6 +890,8 @@ TvPlan::TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, boo
     o_energy_ = ar_.reserve((size_t)B * energy_slots_ * 8);
     ar_.commit();
     OF_CUDA(cudaMemset(ar_.at<char>(o_ctrl_), 0, B * sizeof(TvCtrl)));
+    OF_CUDA(cudaFuncSetAttribute(k_tvl1_tb<kTbTW, kTbTH, kTbK, kTbNT>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTbSmem));
 }
 
 void *TvPlan::raw_input(int b, int k) const {
@@ -734,6 +975,22 @@ void TvPlan::record(cudaStream_t st) {
             if (prof_) OF_CUDA(cudaEventRecord(prof_->ev[prof_->n_ev++], st));
             launches_ += 1;
             ia.stage = s * prm_.warps + wi;
+            if (!trace_) {
+                // blocked schedule: ceil(max/K) launches plus one for a
+                // possible re-run after a mid-block stop
+                TbArgs ta{W, U0, U1, P0, P1, N0, nx, ny, prm_.max_iterations, l_t, prm_.theta,
+                          taut, eps2, ctrl, part, max_blocks_ / kTbK, iters, iter_stride_,
+                          ia.stage};
+                dim3 tg(div_up(nx, kTbTW), div_up(ny, kTbTH), B);
+                const int nl = prm_.max_iterations > 0 ? div_up(prm_.max_iterations, kTbK) + 1 : 0;
+                for (int it = 0; it < nl; it++) {
+                    if (prof_) OF_CUDA(cudaEventRecord(prof_->ev[prof_->n_ev++], st));
+                    k_tvl1_tb<kTbTW, kTbTH, kTbK, kTbNT><<<tg, kTbNT, kTbSmem, st>>>(ta);
+                    if (prof_) OF_CUDA(cudaEventRecord(prof_->ev[prof_->n_ev++], st));
+                    launches_ += 1;
+                }
+                continue;
+            }
             for (int it = 0; it < prm_.max_iterations; it++) {
                 if (prof_) OF_CUDA(cudaEventRecord(prof_->ev[prof_->n_ev++], st));
                 k_tvl1_iter<kIterTW, kIterTH, kIterNT><<<ig, kIterNT, 0, st>>>(ia);
@@ -789,13 +1046,18 @@ void TvPlan::profile(cudaStream_t st, oflow_tvl1_profile *out) {
     out->total_ms = ms;
     int k = 0;
     for (int st_i = 0; st_i < stages; st_i++) {
+        // stages are recorded coarse to fine: stage index -> scale
+        const int scale = ns_ - 1 - st_i / prm_.warps;
         OF_CUDA(cudaEventElapsedTime(&ms, p.ev[k], p.ev[k + 1]));
         out->warp_ms += ms;
         out->warp_launches += 1;
         k += 2;
-        for (int it = 0; it < prm_.max_iterations; it++) {
+        const int nl = trace_ ? prm_.max_iterations
+                              : (prm_.max_iterations > 0 ? div_up(prm_.max_iterations, kTbK) + 1 : 0);
+        for (int it = 0; it < nl; it++) {
             OF_CUDA(cudaEventElapsedTime(&ms, p.ev[k], p.ev[k + 1]));
             out->iter_ms += ms;
+            out->iter_ms_scale[scale] += ms;
             out->iter_launches += 1;
             k += 2;
         }

@@ -241,6 +241,7 @@ def tvl1_batch_profile(pairs, params: TVL1Params | None = None, ctx: Context | N
     h = _ctx(ctx)
     _check(lib().oflow_tvl1_batch_profile(h, n, I0, I1, C.byref(p), O, st, C.byref(pr)), h)
     prof = {k: getattr(pr, k) for k, _ in Tvl1Profile._fields_}
+    prof["iter_ms_scale"] = list(pr.iter_ms_scale)
     return res, [_stats_dict(s) for s in st], prof
 
 

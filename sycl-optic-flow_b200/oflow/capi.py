@@ -44,7 +44,8 @@ class Tvl1Stats(C.Structure):
 
 class Tvl1Profile(C.Structure):
     _fields_ = [("total_ms", C.c_double), ("iter_ms", C.c_double), ("warp_ms", C.c_double),
-                ("iter_launches", C.c_int), ("warp_launches", C.c_int), ("launches", C.c_int)]
+                ("iter_launches", C.c_int), ("warp_launches", C.c_int), ("launches", C.c_int),
+                ("iter_ms_scale", C.c_double * MAX_SCALES)]
 
 
 class HsParams(C.Structure):
