@@ -166,6 +166,29 @@ oflow_status oflow_hs_batch(oflow_ctx *ctx, int n, const oflow_image *I0,
                             const oflow_image *I1, const oflow_hs_params *p,
                             const oflow_flow *out);
 
+/* Horn-Schunck for callers that cannot allocate device memory: code running
+ * while a CUDA graph is captured, real-time frame loops that cannot afford the
+ * synchronisation of cudaMalloc/cudaFree, hosts with a fixed memory budget.
+ * This entry point has no counterpart in the reference.
+ *
+ * It allocates nothing and needs no context.  Its scratch is one static
+ * device array of 8 MiB, held by every GPU that loads the library until the
+ * process exits.  With nlevels = 1 that covers frames up to about 125,000
+ * pixels (320x240 uses 5.2 MB); larger requests return OFLOW_ERR_BAD_ARG.
+ * I0, I1 are device float frames, u and v device float planes; pitches are in
+ * elements (0 means width).  The work is enqueued on `stream` (a
+ * cudaStream_t; NULL is the default stream) and the call returns without
+ * waiting.  The result equals oflow_hs with the same parameters.
+ *
+ * The first call on a device looks up the array's device address (with that
+ * device current) and caches it; make that first call before any stream
+ * capture.  All calls share the one array: calls that overlap on the GPU (on
+ * different streams, or from several threads without ordering) race and give
+ * wrong results.  Order them on one stream. */
+oflow_status oflow_hs_noalloc(const float *I0, const float *I1, int width, int height,
+                              int pitch, const oflow_hs_params *p, float *u, float *v,
+                              int out_pitch, void *stream);
+
 /* ------------------------------------------------------------ Lucas-Kanade */
 /* spac: spatial derivative taps (1,3,5,7,9); temp: temporal taps
  * (1,2,3,5,7,9); window: odd window side (src/lk/cuda/lucaskanade.cuh:8).

@@ -319,4 +319,109 @@ void HsPlan::run(cudaStream_t st) {
     graph_.launch(st);
 }
 
+// ================================================================ caller scratch
+// The Horn-Schunck schedule of HsPlan::record for one pair, enqueued on
+// scratch the caller provides (no allocation here).  Frames and flows are
+// device float planes with row pitches in elements.
+static size_t hs_carve(size_t &off, size_t bytes) {
+    const size_t at = (off + 255) & ~size_t(255);
+    off = at + bytes;
+    return at;
+}
+
+size_t hs_scratch_bytes(int w, int h, int nlevels) {
+    if (w < 1 || h < 1 || nlevels < 1 || nlevels > 16) return 0;
+    int W = w, H = h;
+    size_t pyr = 0;
+    for (int l = nlevels - 1; l >= 0; l--) {
+        if (W < 1 || H < 1) return 0;
+        pyr += (size_t)2 * W * H;
+        W /= 2;
+        H /= 2;
+    }
+    const size_t N = (size_t)w * h;
+    size_t off = 0;
+    hs_carve(off, pyr * 4);   // pyramid
+    hs_carve(off, N * 16);    // D
+    hs_carve(off, N * 8);     // dU0
+    hs_carve(off, N * 8);     // dU1
+    hs_carve(off, N * 8);     // Ua
+    hs_carve(off, N * 8);     // Ub
+    hs_carve(off, 2 * N * 4); // u | v
+    return off;
+}
+
+void hs_enqueue_into(void *scratch, const float *I0, const float *I1, int w, int h, int pitch,
+                     const oflow_hs_params &prm, float *u, float *v, int out_pitch,
+                     cudaStream_t st) {
+    const int L = prm.nlevels;
+    int Wl[16], Hl[16];
+    Wl[L - 1] = w;
+    Hl[L - 1] = h;
+    for (int l = L - 1; l > 0; l--) {
+        Wl[l - 1] = Wl[l] / 2;
+        Hl[l - 1] = Hl[l] / 2;
+    }
+    size_t pyr_off[16], acc = 0;
+    for (int l = 0; l < L; l++) {
+        pyr_off[l] = acc;
+        acc += (size_t)2 * Wl[l] * Hl[l];
+    }
+    const size_t N = (size_t)w * h;
+    size_t off = 0;
+    char *base = static_cast<char *>(scratch);
+    float *pyr = reinterpret_cast<float *>(base + hs_carve(off, acc * 4));
+    float4 *D = reinterpret_cast<float4 *>(base + hs_carve(off, N * 16));
+    float2 *dU[2];
+    dU[0] = reinterpret_cast<float2 *>(base + hs_carve(off, N * 8));
+    dU[1] = reinterpret_cast<float2 *>(base + hs_carve(off, N * 8));
+    float2 *Ubuf[2];
+    Ubuf[0] = reinterpret_cast<float2 *>(base + hs_carve(off, N * 8));
+    Ubuf[1] = reinterpret_cast<float2 *>(base + hs_carve(off, N * 8));
+    float *out = reinterpret_cast<float *>(base + hs_carve(off, 2 * N * 4));
+    const int top = L - 1;
+    const size_t rowb = (size_t)w * 4, pb = (size_t)(pitch ? pitch : w) * 4;
+    OF_CUDA(cudaMemcpy2DAsync(pyr + pyr_off[top], rowb, I0, pb, rowb, h, cudaMemcpyDeviceToDevice, st));
+    OF_CUDA(cudaMemcpy2DAsync(pyr + pyr_off[top] + N, rowb, I1, pb, rowb, h,
+                              cudaMemcpyDeviceToDevice, st));
+    for (int l = top; l > 0; l--) {
+        dim3 blk(32, 8), g(div_up(Wl[l - 1], 32), div_up(Hl[l - 1], 8), 2);
+        k_hs_downscale<<<g, blk, 0, st>>>(pyr + pyr_off[l], (size_t)Wl[l] * Hl[l], Wl[l], Hl[l],
+                                          pyr + pyr_off[l - 1], (size_t)Wl[l - 1] * Hl[l - 1]);
+    }
+    int ub = 0;
+    OF_CUDA(cudaMemsetAsync(Ubuf[ub], 0, N * 8, st));  // the flow starts at zero
+    const size_t smem = (size_t)(kJTW + 2 * kJK) * (kJTH + 2 * kJK) * 32;
+    for (int l = 0; l < L; l++) {
+        const int lw = Wl[l], lh = Hl[l];
+        const size_t lp = (size_t)lw * lh;
+        for (int wi = 0; wi < prm.nwarp; wi++) {
+            dim3 dg(div_up(lw, kDTW), div_up(lh, kDTH), 1);
+            k_hs_warp_deriv<<<dg, dim3(kDTW, kDTH), 0, st>>>(pyr + pyr_off[l], lp, lw, lh,
+                                                             Ubuf[ub], N, 0, prm.alpha, D, N);
+            dim3 jg(div_up(lw, kJTW), div_up(lh, kJTH), 1);
+            int done = 0, cur = 0;
+            while (done < prm.nsolver) {
+                const int k = imin(kJK, prm.nsolver - done);
+                k_hs_jacobi<kJTW, kJTH, kJK, kJNT><<<jg, kJNT, smem, st>>>(
+                    D, N, dU[cur], dU[cur ^ 1], Ubuf[ub], N, lw, lh, k, done == 0,
+                    done + k == prm.nsolver);
+                cur ^= 1;
+                done += k;
+            }
+        }
+        if (l != top) {
+            const float sx = (float)Wl[l + 1] / (float)lw;
+            const float sy = (float)Hl[l + 1] / (float)lh;
+            launch_upscale2(Ubuf[ub], N, lw, lh, Ubuf[ub ^ 1], N, Wl[l + 1], Hl[l + 1], sx, sy, 1, st);
+            ub ^= 1;
+        }
+    }
+    launch_split2(Ubuf[ub], N, (int)N, out, 1, st);
+    OF_CUDA(cudaGetLastError());
+    const size_t ob = (size_t)(out_pitch ? out_pitch : w) * 4;
+    OF_CUDA(cudaMemcpy2DAsync(u, ob, out, rowb, rowb, h, cudaMemcpyDeviceToDevice, st));
+    OF_CUDA(cudaMemcpy2DAsync(v, ob, out + N, rowb, rowb, h, cudaMemcpyDeviceToDevice, st));
+}
+
 }  // namespace oflow

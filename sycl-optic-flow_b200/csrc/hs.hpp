@@ -32,6 +32,13 @@ class HsPlan {
     Graph graph_;
 };
 
+// Bytes of scratch hs_enqueue_into needs for one w x h pair (0: bad sizes).
+size_t hs_scratch_bytes(int w, int h, int nlevels);
+// One pair's Horn-Schunck schedule on caller scratch (device frames / flows).
+void hs_enqueue_into(void *scratch, const float *I0, const float *I1, int w, int h, int pitch,
+                     const oflow_hs_params &prm, float *u, float *v, int out_pitch,
+                     cudaStream_t st);
+
 // Shared with the pyramidal LK plan.
 void launch_upscale2(const float2 *src, size_t sstride, int w, int h, float2 *dst,
                      size_t dstride, int nw, int nh, float sx, float sy, int B, cudaStream_t st);

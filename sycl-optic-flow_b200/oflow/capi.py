@@ -85,6 +85,7 @@ SIGNATURES = {
                       C.POINTER(Flow)]),
     "oflow_hs_batch": (_I, [_VP, _I, C.POINTER(Image), C.POINTER(Image), C.POINTER(HsParams),
                             C.POINTER(Flow)]),
+    "oflow_hs_noalloc": (_I, [_VP, _VP, _I, _I, _I, C.POINTER(HsParams), _VP, _VP, _I, _VP]),
     "oflow_lk_default_params": (None, [C.POINTER(LkParams)]),
     "oflow_lk": (_I, [_VP, C.POINTER(Image), _I, C.POINTER(LkParams), C.POINTER(Flow)]),
     "oflow_pyrlk": (_I, [_VP, C.POINTER(Image), C.POINTER(Image), C.POINTER(LkParams),
