@@ -263,6 +263,8 @@ def our_arm(args, rank, world, local_rank):
     def max_over_ranks(x):
         return multigpu.max_over_ranks(x, dev)
 
+    # --- tile shapes per scale from the autotuner (before warm-up, untimed)
+    tuned = oflow.tvl1_autotune(d_in, prm, ctx) if not args.no_autotune else None
     # --- device-resident inputs (value)
     for _ in range(args.warmup):
         oflow.tvl1_batch(d_in, prm, ctx, out=d_out)
@@ -341,6 +343,7 @@ def our_arm(args, rank, world, local_rank):
                    "batch_pairs_per_gpu": P, "parallelism": f"independent pairs x{world}",
                    "l2": f"inputs larger than L2 (per-step state ~{P * 0.052:.1f} GB)",
                    "inner_iterations_per_step": iters_total,
+                   "tile_config_per_scale": tuned,
                    "epe_vs_ground_truth": round(epe, 5)},
         "e2e": {"value": world * P * e2e_steps / t_e2e, "unit": "pairs/s",
                 "h2d_bytes_per_step": P * 2 * W * H, "d2h_bytes_per_step": P * 2 * W * H * 4},
@@ -391,6 +394,7 @@ def main():
     ap.add_argument("--batch", type=int, default=32, help="pairs per GPU per step")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--cpu-pairs", type=int, default=30)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--cpu-worker", action="store_true", help=argparse.SUPPRESS)

@@ -149,6 +149,19 @@ oflow_status oflow_tvl1_batch_profile(oflow_ctx *ctx, int n, const oflow_image *
                                       const oflow_flow *out, oflow_tvl1_stats *stats,
                                       oflow_tvl1_profile *prof);
 
+/* Autotuner: solves the n given pairs (one size) once, then times every
+ * blocked inner-iteration configuration (tile shape and threads) at every
+ * scale on the device and keeps the fastest for plans of this size and batch.
+ * cfg_per_scale (OFLOW_MAX_SCALES ints, may be NULL) receives the choice per
+ * scale, -1 past the last scale.  The table lives in the context; it can be
+ * saved to / loaded from a text file (lines: solver width height batch config)
+ * keyed by the level size, so plans built later pick it up. */
+oflow_status oflow_tvl1_autotune(oflow_ctx *ctx, int n, const oflow_image *I0,
+                                 const oflow_image *I1, const oflow_tvl1_params *p,
+                                 int *cfg_per_scale);
+oflow_status oflow_ctx_save_tuning(oflow_ctx *ctx, const char *path);
+oflow_status oflow_ctx_load_tuning(oflow_ctx *ctx, const char *path);
+
 /* ------------------------------------------------------------ Horn-Schunck */
 /* Parameters of ComputeFlow (src/hs/cuda/flow.cuh:21-31).  nlevels pyramid
  * levels (2x2 box downscale), nwarp warps per level, nsolver Jacobi sweeps. */

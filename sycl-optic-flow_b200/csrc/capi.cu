@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -68,6 +69,7 @@ struct oflow_ctx {
     std::vector<std::unique_ptr<HsPlan>> hs;
     std::vector<std::unique_ptr<PyrLkPlan>> pyrlk;
     std::vector<std::unique_ptr<LkPlan>> lk;
+    TuneTable tune;  // autotuned kernel configurations, consulted by new plans
     cudaStream_t stream() const { return user ? user : own; }
 };
 
@@ -122,7 +124,7 @@ TvPlan &tv_plan(oflow_ctx *ctx, int w, int h, int B, int dtype, const oflow_tvl1
         if (pl->width() == w && pl->height() == h && pl->batch() == B && pl->dtype() == dtype &&
             pl->traced() == trace && same(pl->params(), p))
             return *pl;
-    ctx->tv.emplace_back(new TvPlan(w, h, B, dtype, p, trace));
+    ctx->tv.emplace_back(new TvPlan(w, h, B, dtype, p, trace, &ctx->tune));
     keep_recent(ctx->tv);
     return *ctx->tv.back();
 }
@@ -315,6 +317,67 @@ oflow_status oflow_tvl1_energy_trace(oflow_ctx *ctx, const oflow_image *I0,
     return guard(ctx, [&] {
         OF_CHECK(energy != nullptr, "tvl1 trace: null energy buffer");
         run_tvl1(ctx, 1, I0, I1, p, out, stats, energy);
+    });
+}
+
+oflow_status oflow_tvl1_autotune(oflow_ctx *ctx, int n, const oflow_image *I0,
+                                 const oflow_image *I1, const oflow_tvl1_params *p,
+                                 int *cfg_per_scale) {
+    return guard(ctx, [&] {
+        OF_CHECK(ctx != nullptr, "null context");
+        OF_CHECK(n >= 1 && I0 && I1, "tvl1 autotune: empty batch");
+        check_tvl1_params(p);
+        const std::vector<Group> groups = group_pairs(n, I0, I1);
+        OF_CHECK(groups.size() == 1, "tvl1 autotune: pairs must share one size");
+        const Group &g = groups[0];
+        const cudaStream_t st = ctx->stream();
+        TvPlan &pl = tv_plan(ctx, g.w, g.h, n, g.dtype, *p, false);
+        for (int b = 0; b < n; b++) {
+            stage_image(I0[b], pl.raw_input(b, 0), dtype_size(g.dtype), st);
+            stage_image(I1[b], pl.raw_input(b, 1), dtype_size(g.dtype), st);
+        }
+        pl.run(st);
+        pl.autotune(st, &ctx->tune);
+        OF_CUDA(cudaStreamSynchronize(st));
+        if (cfg_per_scale)
+            for (int s = 0; s < OFLOW_MAX_SCALES; s++)
+                cfg_per_scale[s] = s < pl.nscales() ? pl.tb_config(s) : -1;
+    });
+}
+
+oflow_status oflow_ctx_save_tuning(oflow_ctx *ctx, const char *path) {
+    return guard(ctx, [&] {
+        OF_CHECK(ctx != nullptr && path != nullptr, "save tuning: null argument");
+        FILE *f = fopen(path, "w");
+        OF_CHECK(f != nullptr, std::string("save tuning: cannot open ") + path);
+        fprintf(f, "# oflow tuning table: solver level_width level_height batch config\n");
+        for (const auto &kv : ctx->tune)
+            fprintf(f, "%s %d %d %d %d\n", std::get<0>(kv.first) == kTuneHs ? "hs" : "tvl1",
+                    std::get<1>(kv.first), std::get<2>(kv.first), std::get<3>(kv.first), kv.second);
+        fclose(f);
+    });
+}
+
+oflow_status oflow_ctx_load_tuning(oflow_ctx *ctx, const char *path) {
+    return guard(ctx, [&] {
+        OF_CHECK(ctx != nullptr && path != nullptr, "load tuning: null argument");
+        FILE *f = fopen(path, "r");
+        OF_CHECK(f != nullptr, std::string("load tuning: cannot open ") + path);
+        char line[256], solver[16];
+        int w, h, B, c, bad = 0;
+        while (fgets(line, sizeof line, f)) {
+            if (line[0] == '#' || line[0] == '\n') continue;
+            if (sscanf(line, "%15s %d %d %d %d", solver, &w, &h, &B, &c) != 5 || c < 0) {
+                bad = 1;
+                break;
+            }
+            const int kind = std::string(solver) == "hs" ? kTuneHs : kTuneTvl1;
+            ctx->tune[tune_key(w, h, B, kind)] = c;
+        }
+        fclose(f);
+        OF_CHECK(!bad, "load tuning: malformed line");
+        ctx->tv.clear();  // plans pick the table up when rebuilt
+        ctx->hs.clear();
     });
 }
 

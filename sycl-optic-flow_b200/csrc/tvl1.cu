@@ -31,9 +31,16 @@ namespace oflow {
 
 // ---------------------------------------------------------------- constants
 constexpr int kIterTW = 32, kIterTH = 8, kIterNT = 256;
-// blocked inner iterations: tile, halo = iterations per launch, threads
-constexpr int kTbTW = 64, kTbTH = 16, kTbK = 4, kTbNT = 256;
-constexpr size_t kTbSmem = (size_t)(kTbTW + 2 * kTbK) * (kTbTH + 2 * kTbK) * 40;
+// blocked inner iterations: iterations per launch (= halo) and the tile
+// configurations, largest first (tile TW x TH, threads); shared memory is
+// 36 B per region pixel (p 16, u 8, I1wx/I1wy 8, rho_c 4)
+constexpr int kTbK = 4;
+struct TbCfg {
+    int tw, th, nt;
+};
+constexpr TbCfg kTbCfgs[] = {{64, 32, 512}, {64, 16, 256}, {32, 16, 256}, {16, 8, 128}};
+constexpr int kTbNumCfgs = 4;
+constexpr size_t tb_smem_bytes(int tw, int th) { return (size_t)(tw + 2 * kTbK) * (th + 2 * kTbK) * 36; }
 constexpr int kGaussTW = 32, kGaussTH = 16, kGaussNT = 256, kGaussMaxR = 15;
 constexpr int kIngestNT = 256, kIngestPPT = 8;
 
@@ -300,13 +307,14 @@ __global__ void k_grad_pack(const float *__restrict__ pyr, size_t pyr_stride, in
 
 // ---------------------------------------------------------------- warping
 // Per warp (tvl1.cpp:197-212): bicubic samples of I1, I1x, I1y at (x+u1,
-// y+u2) with border zeroing, then rho_c and |grad|^2.  mode 0: u from U[cur];
+// y+u2) with border zeroing, then rho_c.  |grad I1w|^2 (tvl1.cpp:202-206) is
+// recomputed from (I1wx, I1wy) where it is used, with the same expression.  mode 0: u from U[cur];
 // 1: u from the upsampled Uz (copied into U[cur]); 2: u = 0 (coarsest scale).
 // With first_warp, p is zeroed (tvl1.cpp:190-193).
 enum { kWarpFromU = 0, kWarpFromUz = 1, kWarpZero = 2 };
 
 __global__ void k_warp(const float *__restrict__ pyr, size_t pyr_stride, const float4 *I1g,
-                       float4 *W, float2 *U0, float2 *U1, const float2 *Uz, float4 *P0,
+                       float2 *Wxy, float *Rc, float2 *U0, float2 *U1, const float2 *Uz, float4 *P0,
                        float4 *P1, size_t stride, int nx, int ny, int mode, int first_warp,
                        TvCtrl *ctrl) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -355,9 +363,9 @@ __global__ void k_warp(const float *__restrict__ pyr, size_t pyr_stride, const f
         Iwy = cubic_cell(by[0], by[1], by[2], by[3], s.tx);
     }
     const float I0v = __ldg(pyr + (size_t)(2 * b) * pyr_stride + p);
-    const float grad = (Iwx * Iwx) + (Iwy * Iwy);
     const float rho_c = (Iw - Iwx * u.x - Iwy * u.y - I0v);
-    W[off + p] = make_float4(Iwx, Iwy, rho_c, grad);
+    Wxy[off + p] = make_float2(Iwx, Iwy);
+    Rc[off + p] = rho_c;
 }
 
 // ---------------------------------------------------------------- iteration
@@ -377,11 +385,12 @@ __device__ __forceinline__ float div_border(float a1c, float a1l, float a2c, flo
 }
 
 // TH step (tvl1.cpp:221-245) and u update (:252-265) for one pixel.
-__device__ __forceinline__ float2 th_u_update(float2 u, float4 w, float4 pc, float4 pl,
-                                              float4 pu, bool L, bool R, bool T, bool B,
-                                              float l_t, float theta) {
-    const float rho = w.z + (w.x * u.x + w.y * u.y);
-    const float lg = l_t * w.w;
+__device__ __forceinline__ float2 th_u_update(float2 u, float2 w, float rc, float4 pc,
+                                              float4 pl, float4 pu, bool L, bool R, bool T,
+                                              bool B, float l_t, float theta) {
+    const float grad = (w.x * w.x) + (w.y * w.y);
+    const float rho = rc + (w.x * u.x + w.y * u.y);
+    const float lg = l_t * grad;
     float d1, d2;
     if (!(rho >= -lg)) {
         d1 = l_t * w.x;
@@ -389,10 +398,10 @@ __device__ __forceinline__ float2 th_u_update(float2 u, float4 w, float4 pc, flo
     } else if (rho > lg) {
         d1 = -l_t * w.x;
         d2 = -l_t * w.y;
-    } else if (w.w < 1E-10f) {
+    } else if (grad < 1E-10f) {
         d1 = d2 = 0.0f;
     } else {
-        const float fi = -rho / w.w;
+        const float fi = -rho / grad;
         d1 = fi * w.x;
         d2 = fi * w.y;
     }
@@ -419,7 +428,8 @@ __device__ __forceinline__ float4 dual_update(float4 po, float f1x, float f1y, f
 }
 
 struct IterArgs {
-    const float4 *W;
+    const float2 *Wxy;
+    const float *Rc;
     float2 *U0, *U1;
     float4 *P0, *P1;
     size_t stride;  // elements between pairs
@@ -451,7 +461,8 @@ __global__ void __launch_bounds__(NT) k_tvl1_iter(IterArgs a) {
     float2 *__restrict__ Uout = (cur ? a.U0 : a.U1) + off;
     const float4 *__restrict__ Pin = (cur ? a.P1 : a.P0) + off;
     float4 *__restrict__ Pout = (cur ? a.P0 : a.P1) + off;
-    const float4 *__restrict__ W = a.W + off;
+    const float2 *__restrict__ Wxy = a.Wxy + off;
+    const float *__restrict__ Rc = a.Rc + off;
     const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
 
     __shared__ float4 sP[(TH + 2) * (TW + 2)];
@@ -474,10 +485,9 @@ __global__ void __launch_bounds__(NT) k_tvl1_iter(IterArgs a) {
         if (x >= nx || y >= ny) continue;
         const size_t p = (size_t)y * nx + x;
         const float2 u = Uin[p];
-        const float4 w = W[p];
         const float4 *c = sP + (ry + 1) * (TW + 2) + (rx + 1);
-        const float2 un = th_u_update(u, w, c[0], c[-1], c[-(TW + 2)], x == 0, x == nx - 1,
-                                      y == 0, y == ny - 1, a.l_t, a.theta);
+        const float2 un = th_u_update(u, Wxy[p], Rc[p], c[0], c[-1], c[-(TW + 2)], x == 0,
+                                      x == nx - 1, y == 0, y == ny - 1, a.l_t, a.theta);
         sU[i] = un;
         if (rx < TW && ry < TH) {
             Uout[p] = un;
@@ -549,7 +559,8 @@ __global__ void __launch_bounds__(NT) k_tvl1_iter(IterArgs a) {
 // launch, nothing is accepted and the next launch re-runs exactly that many
 // iterations from the untouched input buffers.
 struct TbArgs {
-    const float4 *W;
+    const float2 *Wxy;
+    const float *Rc;
     float2 *U0, *U1;
     float4 *P0, *P1;
     size_t stride;
@@ -588,16 +599,17 @@ __device__ __forceinline__ void for_rect(int x0, int x1, int y0, int y1, F &&f) 
 // ever leaves the region.  INTERIOR: no region pixel lies on the image border
 // (no bounds or border tests).
 template <int TW, int TH, int K, int NT, bool INTERIOR>
-__device__ __forceinline__ void tb_iteration(int j, float4 *sP, const float4 *sW, float2 *sU,
-                                             int ox, int oy, int nx, int ny, float l_t,
-                                             float theta, float taut, double &err) {
+__device__ __forceinline__ void tb_iteration(int j, float4 *sP, const float2 *sW,
+                                             const float *sR, float2 *sU, int ox, int oy, int nx,
+                                             int ny, float l_t, float theta, float taut,
+                                             double &err) {
     constexpr int RW = TW + 2 * K, RH = TH + 2 * K;
     for_rect<NT>(j, RW - j, j, RH - j, [&](int rx, int ry) {
         const int i = ry * RW + rx;
         const int x = ox + rx, y = oy + ry;
         if (!INTERIOR && (x >= nx || y >= ny || x < 0 || y < 0)) return;
         const float2 u = sU[i];
-        const float2 un = th_u_update(u, sW[i], sP[i], sP[i - 1], sP[i - RW],
+        const float2 un = th_u_update(u, sW[i], sR[i], sP[i], sP[i - 1], sP[i - RW],
                                       !INTERIOR && x == 0, !INTERIOR && x == nx - 1,
                                       !INTERIOR && y == 0, !INTERIOR && y == ny - 1, l_t, theta);
         sU[i] = un;
@@ -634,8 +646,9 @@ __global__ void __launch_bounds__(NT) k_tvl1_tb(TbArgs a) {
     constexpr int RW = TW + 2 * K, RH = TH + 2 * K, RN = RW * RH;
     extern __shared__ float4 tb_smem[];
     float4 *sP = tb_smem;                                  // RN
-    float4 *sW = sP + RN;                                  // RN
-    float2 *sU = reinterpret_cast<float2 *>(sW + RN);      // RN
+    float2 *sU = reinterpret_cast<float2 *>(sP + RN);      // RN
+    float2 *sW = sU + RN;                                  // RN
+    float *sR = reinterpret_cast<float *>(sW + RN);        // RN
     __shared__ double sred[NT / 32];
     __shared__ double sE[K];
     __shared__ int s_last;
@@ -653,23 +666,27 @@ __global__ void __launch_bounds__(NT) k_tvl1_tb(TbArgs a) {
     float2 *__restrict__ Uout = (cur ? a.U0 : a.U1) + off;
     const float4 *__restrict__ Pin = (cur ? a.P1 : a.P0) + off;
     float4 *__restrict__ Pout = (cur ? a.P0 : a.P1) + off;
-    const float4 *__restrict__ Wg = a.W + off;
+    const float2 *__restrict__ Wg = a.Wxy + off;
+    const float *__restrict__ Rg = a.Rc + off;
     const int ox = blockIdx.x * TW - K, oy = blockIdx.y * TH - K;
     const bool interior = ox >= 1 && oy >= 1 && ox + RW <= nx - 1 && oy + RH <= ny - 1;
 
     // all loads of the region issued before any use
     for (int i = threadIdx.x; i < RN; i += NT) {
         const int x = ox + i % RW, y = oy + i / RW;
-        float4 p = make_float4(0.f, 0.f, 0.f, 0.f), w = p;
-        float2 u = make_float2(0.f, 0.f);
+        float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+        float2 u = make_float2(0.f, 0.f), w = u;
+        float r = 0.0f;
         if (x >= 0 && x < nx && y >= 0 && y < ny) {
             const size_t q = (size_t)y * nx + x;
             p = Pin[q];
             w = Wg[q];
+            r = Rg[q];
             u = Uin[q];
         }
         sP[i] = p;
         sW[i] = w;
+        sR[i] = r;
         sU[i] = u;
     }
     __syncthreads();
@@ -680,10 +697,10 @@ __global__ void __launch_bounds__(NT) k_tvl1_tb(TbArgs a) {
         err[j] = 0.0;
         if (j < kk) {  // uniform over the block
             if (interior)
-                tb_iteration<TW, TH, K, NT, true>(j + 1, sP, sW, sU, ox, oy, nx, ny, a.l_t,
+                tb_iteration<TW, TH, K, NT, true>(j + 1, sP, sW, sR, sU, ox, oy, nx, ny, a.l_t,
                                                   a.theta, a.taut, err[j]);
             else
-                tb_iteration<TW, TH, K, NT, false>(j + 1, sP, sW, sU, ox, oy, nx, ny, a.l_t,
+                tb_iteration<TW, TH, K, NT, false>(j + 1, sP, sW, sR, sU, ox, oy, nx, ny, a.l_t,
                                                    a.theta, a.taut, err[j]);
         }
     }
@@ -760,7 +777,8 @@ __global__ void __launch_bounds__(NT) k_tvl1_tb(TbArgs a) {
 // sum |rho(u)| with rho linearised at the current warp.  Last block of a pair
 // writes ctrl.energy and, if slot >= 0, energy_out[b * slots + slot].
 constexpr int kEnNT = 256;
-__global__ void __launch_bounds__(kEnNT) k_energy(const float4 *W, const float2 *U0,
+__global__ void __launch_bounds__(kEnNT) k_energy(const float2 *Wxy, const float *Rc,
+                                                  const float2 *U0,
                                                   const float2 *U1, size_t stride, int nx,
                                                   int ny, float lambda, TvCtrl *ctrl,
                                                   double *partials, int max_blocks,
@@ -778,8 +796,8 @@ __global__ void __launch_bounds__(kEnNT) k_energy(const float4 *W, const float2 
         if (x < nx - 1) { const float2 r = U[i + 1]; f1x = (double)(r.x - uc.x); f2x = (double)(r.y - uc.y); }
         if (y < ny - 1) { const float2 d = U[i + nx]; f1y = (double)(d.x - uc.x); f2y = (double)(d.y - uc.y); }
         tv += sqrt(f1x * f1x + f1y * f1y) + sqrt(f2x * f2x + f2y * f2y);
-        const float4 w = W[off + i];
-        const float rho = w.z + (w.x * uc.x + w.y * uc.y);
+        const float2 w = Wxy[off + i];
+        const float rho = Rc[off + i] + (w.x * uc.x + w.y * uc.y);
         data += fabs((double)rho);
     }
     __shared__ double sred[kEnNT / 32];
@@ -836,7 +854,46 @@ void launch_resample(const float *src, size_t sstride, int nx, int ny, float *ds
 }
 
 // ================================================================ host plan
-TvPlan::TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, bool trace)
+template <int TW, int TH, int NT>
+static void tb_launch(dim3 g, cudaStream_t st, const TbArgs &ta) {
+    k_tvl1_tb<TW, TH, kTbK, NT><<<g, NT, tb_smem_bytes(TW, TH), st>>>(ta);
+}
+
+static void tb_launch_cfg(int cfg, dim3 g, cudaStream_t st, const TbArgs &ta) {
+    switch (cfg) {
+        case 0: tb_launch<64, 32, 512>(g, st, ta); break;
+        case 1: tb_launch<64, 16, 256>(g, st, ta); break;
+        case 2: tb_launch<32, 16, 256>(g, st, ta); break;
+        default: tb_launch<16, 8, 128>(g, st, ta); break;
+    }
+}
+
+static void tb_set_smem_attrs() {
+    OF_CUDA(cudaFuncSetAttribute(k_tvl1_tb<64, 32, kTbK, 512>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tb_smem_bytes(64, 32)));
+    OF_CUDA(cudaFuncSetAttribute(k_tvl1_tb<64, 16, kTbK, 256>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tb_smem_bytes(64, 16)));
+}
+
+static int tb_tiles(int cfg, int nx, int ny) {
+    return div_up(nx, kTbCfgs[cfg].tw) * div_up(ny, kTbCfgs[cfg].th);
+}
+
+// Largest tile whose grid still gives every SM two blocks; small scales get
+// small tiles (more blocks, shorter per-launch latency).  OFLOW_TB_CFG forces
+// one configuration (used to time them against each other).
+static int tb_pick(int nx, int ny, int B) {
+    if (const char *e = getenv("OFLOW_TB_CFG")) {
+        const int c = atoi(e);
+        if (c >= 0 && c < kTbNumCfgs) return c;
+    }
+    for (int c = 0; c < kTbNumCfgs; c++)
+        if (tb_tiles(c, nx, ny) * B >= 2 * kNumSMs) return c;
+    return kTbNumCfgs - 1;
+}
+
+TvPlan::TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, bool trace,
+               const TuneTable *tuned)
     : w_(w), h_(h), B_(B), dtype_(dtype), prm_(prm), trace_(trace) {
     OF_CHECK(w >= 8 && h >= 8, "tvl1: frames must be at least 8x8");
     OF_CHECK(B >= 1, "tvl1: empty batch");
@@ -860,8 +917,13 @@ TvPlan::TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, boo
 
     const size_t N0 = (size_t)w * h;
     N0_ = N0;
-    iter_blocks_ = imax(div_up(w, kIterTW) * div_up(h, kIterTH),
-                        div_up(w, kTbTW) * div_up(h, kTbTH) * kTbK);
+    iter_blocks_ = div_up(w, kIterTW) * div_up(h, kIterTH);
+    for (int s = 0; s < ns_; s++) {
+        const auto it = tuned ? tuned->find(tune_key(nx_[s], ny_[s], B)) : TuneTable::const_iterator();
+        tb_cfg_[s] = (tuned && it != tuned->end()) ? it->second : tb_pick(nx_[s], ny_[s], B);
+        for (int c = 0; c < kTbNumCfgs; c++)  // any configuration may run while tuning
+            iter_blocks_ = imax(iter_blocks_, tb_tiles(c, nx_[s], ny_[s]) * kTbK);
+    }
     ingest_blocks_ = imin(div_up((int)N0, kIngestNT * kIngestPPT), 1024);
     energy_blocks_ = imin(div_up((int)N0, kEnNT * 4), 512);
     max_blocks_ = imax(iter_blocks_, energy_blocks_);
@@ -874,7 +936,8 @@ TvPlan::TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, boo
     o_T_ = ar_.reserve(2 * B * N0 * 4);
     o_pyr_ = ar_.reserve(pyr_total * 4);
     o_I1g_ = ar_.reserve(B * N0 * 16);
-    o_W_ = ar_.reserve(B * N0 * 16);
+    o_Wxy_ = ar_.reserve(B * N0 * 8);
+    o_Rc_ = ar_.reserve(B * N0 * 4);
     o_U0_ = ar_.reserve(B * N0 * 8);
     o_U1_ = ar_.reserve(B * N0 * 8);
     o_Uz_ = ar_.reserve(B * N0 * 8);
@@ -890,8 +953,7 @@ TvPlan::TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, boo
     o_energy_ = ar_.reserve((size_t)B * energy_slots_ * 8);
     ar_.commit();
     OF_CUDA(cudaMemset(ar_.at<char>(o_ctrl_), 0, B * sizeof(TvCtrl)));
-    OF_CUDA(cudaFuncSetAttribute(k_tvl1_tb<kTbTW, kTbTH, kTbK, kTbNT>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTbSmem));
+    tb_set_smem_attrs();
 }
 
 void *TvPlan::raw_input(int b, int k) const {
@@ -902,6 +964,11 @@ const float *TvPlan::out_u(int b) const { return ar_.at<float>(o_out_) + (size_t
 const float *TvPlan::out_v(int b) const { return ar_.at<float>(o_out_) + (size_t)(B_ + b) * N0_; }
 const int *TvPlan::iters_dev() const { return ar_.at<int>(o_iters_); }
 
+int TvPlan::iter_launches_per_stage() const {
+    if (trace_) return prm_.max_iterations;
+    return prm_.max_iterations > 0 ? div_up(prm_.max_iterations, kTbK) + 1 : 0;
+}
+
 void TvPlan::record(cudaStream_t st) {
     launches_ = 0;
     const int B = B_;
@@ -909,7 +976,8 @@ void TvPlan::record(cudaStream_t st) {
     float *T = ar_.at<float>(o_T_);
     float *pyr = ar_.at<float>(o_pyr_);
     float4 *I1g = ar_.at<float4>(o_I1g_);
-    float4 *W = ar_.at<float4>(o_W_);
+    float2 *Wxy = ar_.at<float2>(o_Wxy_);
+    float *Rc = ar_.at<float>(o_Rc_);
     float2 *U0 = ar_.at<float2>(o_U0_), *U1 = ar_.at<float2>(o_U1_), *Uz = ar_.at<float2>(o_Uz_);
     float4 *P0 = ar_.at<float4>(o_P0_), *P1 = ar_.at<float4>(o_P1_);
     TvCtrl *ctrl = ar_.at<TvCtrl>(o_ctrl_);
@@ -917,6 +985,11 @@ void TvPlan::record(cudaStream_t st) {
     NormRec *recs = ar_.at<NormRec>(o_recs_);
     int *iters = ar_.at<int>(o_iters_);
     double *energy = ar_.at<double>(o_energy_);
+    // profile replays are captured: external event nodes keep timestamps
+    auto mark = [&]() {
+        if (prof_)
+            OF_CUDA(cudaEventRecordWithFlags(prof_->ev[prof_->n_ev++], st, cudaEventRecordExternal));
+    };
 
     OF_CUDA(cudaMemsetAsync(iters, 0, sizeof(int) * (size_t)B * iter_stride_, st));
     // ingest + normalisation range
@@ -964,51 +1037,50 @@ void TvPlan::record(cudaStream_t st) {
         }
         k_grad_pack<<<gr, blk, 0, st>>>(pyr + pyr_off_[s], lp, nx, ny, I1g, N0);
         launches_ += 1;
-        IterArgs ia{W, U0, U1, P0, P1, N0, nx, ny, l_t, prm_.theta, taut, eps2, ctrl, part,
+        IterArgs ia{Wxy, Rc, U0, U1, P0, P1, N0, nx, ny, l_t, prm_.theta, taut, eps2, ctrl, part,
                     max_blocks_, iters, iter_stride_, 0};
         dim3 ig(div_up(nx, kIterTW), div_up(ny, kIterTH), B);
+        const int cfg = tb_cfg_[s];
         for (int wi = 0; wi < prm_.warps; wi++) {
             const int mode = wi > 0 ? kWarpFromU : (s == ns_ - 1 ? kWarpZero : kWarpFromUz);
-            if (prof_) OF_CUDA(cudaEventRecord(prof_->ev[prof_->n_ev++], st));
-            k_warp<<<gr, blk, 0, st>>>(pyr + pyr_off_[s], lp, I1g, W, U0, U1, Uz, P0, P1, N0, nx,
-                                       ny, mode, wi == 0, ctrl);
-            if (prof_) OF_CUDA(cudaEventRecord(prof_->ev[prof_->n_ev++], st));
+            mark();
+            k_warp<<<gr, blk, 0, st>>>(pyr + pyr_off_[s], lp, I1g, Wxy, Rc, U0, U1, Uz, P0, P1,
+                                       N0, nx, ny, mode, wi == 0, ctrl);
+            mark();
             launches_ += 1;
             ia.stage = s * prm_.warps + wi;
             if (!trace_) {
                 // blocked schedule: ceil(max/K) launches plus one for a
                 // possible re-run after a mid-block stop
-                TbArgs ta{W, U0, U1, P0, P1, N0, nx, ny, prm_.max_iterations, l_t, prm_.theta,
-                          taut, eps2, ctrl, part, max_blocks_ / kTbK, iters, iter_stride_,
-                          ia.stage};
-                dim3 tg(div_up(nx, kTbTW), div_up(ny, kTbTH), B);
-                const int nl = prm_.max_iterations > 0 ? div_up(prm_.max_iterations, kTbK) + 1 : 0;
+                TbArgs ta{Wxy, Rc, U0, U1, P0, P1, N0, nx, ny, prm_.max_iterations, l_t,
+                          prm_.theta, taut, eps2, ctrl, part, max_blocks_ / kTbK, iters,
+                          iter_stride_, ia.stage};
+                dim3 tg(div_up(nx, kTbCfgs[cfg].tw), div_up(ny, kTbCfgs[cfg].th), B);
+                const int nl = iter_launches_per_stage();
                 for (int it = 0; it < nl; it++) {
-                    if (prof_) OF_CUDA(cudaEventRecord(prof_->ev[prof_->n_ev++], st));
-                    k_tvl1_tb<kTbTW, kTbTH, kTbK, kTbNT><<<tg, kTbNT, kTbSmem, st>>>(ta);
-                    if (prof_) OF_CUDA(cudaEventRecord(prof_->ev[prof_->n_ev++], st));
+                    mark();
+                    tb_launch_cfg(cfg, tg, st, ta);
+                    mark();
                     launches_ += 1;
                 }
                 continue;
             }
             for (int it = 0; it < prm_.max_iterations; it++) {
-                if (prof_) OF_CUDA(cudaEventRecord(prof_->ev[prof_->n_ev++], st));
+                mark();
                 k_tvl1_iter<kIterTW, kIterTH, kIterNT><<<ig, kIterNT, 0, st>>>(ia);
-                if (prof_) OF_CUDA(cudaEventRecord(prof_->ev[prof_->n_ev++], st));
+                mark();
                 launches_ += 1;
-                if (trace_) {
-                    const int slot = (s * prm_.warps + wi) * prm_.max_iterations + it;
-                    k_energy<<<dim3(imin(energy_blocks_, div_up(nx * ny, kEnNT * 4)), B), kEnNT, 0,
-                               st>>>(W, U0, U1, N0, nx, ny, prm_.lambda, ctrl, part, max_blocks_,
-                                     energy, energy_slots_, slot, it + 1);
-                    launches_ += 1;
-                }
+                const int slot = (s * prm_.warps + wi) * prm_.max_iterations + it;
+                k_energy<<<dim3(imin(energy_blocks_, div_up(nx * ny, kEnNT * 4)), B), kEnNT, 0,
+                           st>>>(Wxy, Rc, U0, U1, N0, nx, ny, prm_.lambda, ctrl, part, max_blocks_,
+                                 energy, energy_slots_, slot, it + 1);
+                launches_ += 1;
             }
         }
     }
     // final energy at the finest scale, last warp
-    k_energy<<<dim3(energy_blocks_, B), kEnNT, 0, st>>>(W, U0, U1, N0, w_, h_, prm_.lambda, ctrl,
-                                                        part, max_blocks_, energy,
+    k_energy<<<dim3(energy_blocks_, B), kEnNT, 0, st>>>(Wxy, Rc, U0, U1, N0, w_, h_, prm_.lambda,
+                                                        ctrl, part, max_blocks_, energy,
                                                         energy_slots_, trace_ ? -1 : 0, -1);
     k_split<<<dim3(imin(div_up((int)N0, 256 * 4), 1024), B), 256, 0, st>>>(
         U0, U1, N0, (int)N0, ar_.at<float>(o_out_), ar_.at<float>(o_out_) + (size_t)B * N0, ctrl);
@@ -1016,56 +1088,123 @@ void TvPlan::record(cudaStream_t st) {
     OF_CUDA(cudaGetLastError());
 }
 
-// Eager run with CUDA events around every warp and inner-iteration launch on
-// `st`; returns per-kind totals (ms) and launch counts.
+// The schedule replayed as a CUDA graph with event nodes around every warp and
+// inner-iteration launch (timings on the GPU timeline, no host gaps); returns
+// per-kind totals (ms) and launch counts.
 void TvPlan::profile(cudaStream_t st, oflow_tvl1_profile *out) {
     Prof p;
     const int stages = ns_ * prm_.warps;
-    p.ev.resize((size_t)2 * stages * (1 + prm_.max_iterations) + 2);
+    const int nl = iter_launches_per_stage();
+    p.ev.resize((size_t)2 * stages * (1 + nl) + 2);
     for (auto &e : p.ev) OF_CUDA(cudaEventCreate(&e));
     cudaEvent_t t0, t1;
     OF_CUDA(cudaEventCreate(&t0));
     OF_CUDA(cudaEventCreate(&t1));
-    prof_ = &p;
-    try {
-        OF_CUDA(cudaEventRecord(t0, st));
-        record(st);
-        OF_CUDA(cudaEventRecord(t1, st));
-        OF_CUDA(cudaStreamSynchronize(st));
-    } catch (...) {
+    auto cleanup = [&]() {
         prof_ = nullptr;
         for (auto &e : p.ev) cudaEventDestroy(e);
         cudaEventDestroy(t0);
         cudaEventDestroy(t1);
+    };
+    try {
+        Graph g;
+        prof_ = &p;
+        g.capture(st, [&](cudaStream_t s) {
+            OF_CUDA(cudaEventRecordWithFlags(t0, s, cudaEventRecordExternal));
+            record(s);
+            OF_CUDA(cudaEventRecordWithFlags(t1, s, cudaEventRecordExternal));
+        });
+        prof_ = nullptr;
+        g.launch(st);
+        OF_CUDA(cudaStreamSynchronize(st));
+        std::memset(out, 0, sizeof(*out));
+        float ms = 0.0f;
+        OF_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+        out->total_ms = ms;
+        int k = 0;
+        for (int st_i = 0; st_i < stages; st_i++) {
+            // stages are recorded coarse to fine: stage index -> scale
+            const int scale = ns_ - 1 - st_i / prm_.warps;
+            OF_CUDA(cudaEventElapsedTime(&ms, p.ev[k], p.ev[k + 1]));
+            out->warp_ms += ms;
+            out->warp_launches += 1;
+            k += 2;
+            for (int it = 0; it < nl; it++) {
+                OF_CUDA(cudaEventElapsedTime(&ms, p.ev[k], p.ev[k + 1]));
+                out->iter_ms += ms;
+                out->iter_ms_scale[scale] += ms;
+                out->iter_launches += 1;
+                k += 2;
+            }
+        }
+        out->launches = launches_;
+    } catch (...) {
+        cleanup();
         throw;
     }
-    prof_ = nullptr;
-    std::memset(out, 0, sizeof(*out));
-    float ms = 0.0f;
-    OF_CUDA(cudaEventElapsedTime(&ms, t0, t1));
-    out->total_ms = ms;
-    int k = 0;
-    for (int st_i = 0; st_i < stages; st_i++) {
-        // stages are recorded coarse to fine: stage index -> scale
-        const int scale = ns_ - 1 - st_i / prm_.warps;
-        OF_CUDA(cudaEventElapsedTime(&ms, p.ev[k], p.ev[k + 1]));
-        out->warp_ms += ms;
-        out->warp_launches += 1;
-        k += 2;
-        const int nl = trace_ ? prm_.max_iterations
-                              : (prm_.max_iterations > 0 ? div_up(prm_.max_iterations, kTbK) + 1 : 0);
-        for (int it = 0; it < nl; it++) {
-            OF_CUDA(cudaEventElapsedTime(&ms, p.ev[k], p.ev[k + 1]));
-            out->iter_ms += ms;
-            out->iter_ms_scale[scale] += ms;
-            out->iter_launches += 1;
-            k += 2;
+    cleanup();
+}
+
+// Re-arms every pair for a timing launch: iteration count 0, not stopped.
+__global__ void k_ctrl_rearm(TvCtrl *ctrl, int B) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B) return;
+    ctrl[b].n = 0;
+    ctrl[b].stop = 0;
+    ctrl[b].redo = 0;
+    ctrl[b].arrive = 0;
+}
+
+// Times every blocked-iteration configuration at every scale on the plan's
+// current buffers (run a solve first so they hold real data) and keeps the
+// fastest; best of `reps` single launches with all pairs active.
+void TvPlan::autotune(cudaStream_t st, TuneTable *table, int reps) {
+    const size_t N0 = N0_;
+    TvCtrl *ctrl = ar_.at<TvCtrl>(o_ctrl_);
+    cudaEvent_t e0, e1;
+    OF_CUDA(cudaEventCreate(&e0));
+    OF_CUDA(cudaEventCreate(&e1));
+    const float l_t = prm_.lambda * prm_.theta, taut = prm_.tau / prm_.theta;
+    const float eps2 = prm_.epsilon * prm_.epsilon;
+    try {
+        for (int s = 0; s < ns_; s++) {
+            const int nx = nx_[s], ny = ny_[s];
+            float best = 1e30f;
+            int best_c = tb_cfg_[s];
+            for (int c = 0; c < kTbNumCfgs; c++) {
+                TbArgs ta{ar_.at<float2>(o_Wxy_), ar_.at<float>(o_Rc_), ar_.at<float2>(o_U0_),
+                          ar_.at<float2>(o_U1_), ar_.at<float4>(o_P0_), ar_.at<float4>(o_P1_), N0,
+                          nx, ny, 1 << 30, l_t, prm_.theta, taut, -1.0f, ctrl,
+                          ar_.at<double>(o_part_), max_blocks_ / kTbK, ar_.at<int>(o_iters_),
+                          iter_stride_, 0};
+                dim3 tg(div_up(nx, kTbCfgs[c].tw), div_up(ny, kTbCfgs[c].th), B_);
+                float ms_min = 1e30f;
+                for (int r = 0; r <= reps; r++) {  // first launch warms up
+                    k_ctrl_rearm<<<div_up(B_, 128), 128, 0, st>>>(ctrl, B_);
+                    OF_CUDA(cudaEventRecord(e0, st));
+                    tb_launch_cfg(c, tg, st, ta);
+                    OF_CUDA(cudaEventRecord(e1, st));
+                    OF_CUDA(cudaEventSynchronize(e1));
+                    float ms = 0.0f;
+                    OF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                    if (r > 0) ms_min = ms < ms_min ? ms : ms_min;
+                }
+                if (ms_min < best) {
+                    best = ms_min;
+                    best_c = c;
+                }
+            }
+            tb_cfg_[s] = best_c;
+            if (table) (*table)[tune_key(nx, ny, B_)] = best_c;
         }
+    } catch (...) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw;
     }
-    out->launches = launches_;
-    for (auto &e : p.ev) cudaEventDestroy(e);
-    cudaEventDestroy(t0);
-    cudaEventDestroy(t1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    graph_.reset();  // the next run captures the new configurations
 }
 
 void TvPlan::run(cudaStream_t st) {

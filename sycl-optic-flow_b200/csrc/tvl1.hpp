@@ -3,6 +3,9 @@
 // iterations, output split).
 #pragma once
 
+#include <map>
+#include <tuple>
+
 #include "internal.hpp"
 
 namespace oflow {
@@ -14,6 +17,14 @@ struct GaussTaps {
 };
 
 int tvl1_nscales(int w, int h, int nscales, float zfactor);
+
+// Tuned kernel configurations: key (solver, level w, level h, batch) -> config index.
+using TuneKey = std::tuple<int, int, int, int>;
+using TuneTable = std::map<TuneKey, int>;
+enum { kTuneTvl1 = 1, kTuneHs = 2 };
+inline TuneKey tune_key(int w, int h, int B, int solver = kTuneTvl1) {
+    return TuneKey(solver, w, h, B);
+}
 void tvl1_zoom_size(int nx, int ny, int *nxx, int *nyy, float f);
 // Taps of the pre-decimation blur, sigma = 0.6*sqrt(1/f^2 - 1) (zoom.cpp:39).
 GaussTaps make_zoom_taps(float zfactor);
@@ -27,7 +38,12 @@ void launch_resample(const float *src, size_t sstride, int nx, int ny, float *ds
 
 class TvPlan {
   public:
-    TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, bool trace = false);
+    TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, bool trace = false,
+           const TuneTable *tuned = nullptr);
+    // Times each blocked-iteration configuration per scale on the current
+    // buffers, keeps the fastest and records it in `table`.
+    void autotune(cudaStream_t st, TuneTable *table, int reps = 3);
+    int tb_config(int s) const { return tb_cfg_[s]; }
     // Device destination of input frame k (0: I0, 1: I1) of pair b: a dense
     // w*h plane of the plan's dtype.
     void *raw_input(int b, int k) const;
@@ -74,7 +90,10 @@ class TvPlan {
     Prof *prof_ = nullptr;
     int launches_ = 0;
     Arena ar_;
-    size_t o_raw_ = 0, o_T_ = 0, o_pyr_ = 0, o_I1g_ = 0, o_W_ = 0, o_U0_ = 0, o_U1_ = 0,
+    int tb_cfg_[OFLOW_MAX_SCALES] = {};
+    int iter_launches_per_stage() const;
+    size_t o_Wxy_ = 0, o_Rc_ = 0;
+    size_t o_raw_ = 0, o_T_ = 0, o_pyr_ = 0, o_I1g_ = 0, o_U0_ = 0, o_U1_ = 0,
            o_Uz_ = 0, o_P0_ = 0, o_P1_ = 0, o_out_ = 0, o_ctrl_ = 0, o_part_ = 0, o_recs_ = 0,
            o_iters_ = 0, o_energy_ = 0;
     Graph graph_;

@@ -103,6 +103,12 @@ class Context:
     def trim(self):
         _check(lib().oflow_ctx_trim(self._h), self._h)
 
+    def save_tuning(self, path: str):
+        _check(lib().oflow_ctx_save_tuning(self._h, os.fsencode(path)), self._h)
+
+    def load_tuning(self, path: str):
+        _check(lib().oflow_ctx_load_tuning(self._h, os.fsencode(path)), self._h)
+
     def close(self):
         if self._h:
             lib().oflow_ctx_destroy(self._h)
@@ -243,6 +249,24 @@ def tvl1_batch_profile(pairs, params: TVL1Params | None = None, ctx: Context | N
     prof = {k: getattr(pr, k) for k, _ in Tvl1Profile._fields_}
     prof["iter_ms_scale"] = list(pr.iter_ms_scale)
     return res, [_stats_dict(s) for s in st], prof
+
+
+def tvl1_autotune(pairs, params: TVL1Params | None = None, ctx: Context | None = None):
+    """Tune the blocked-iteration configuration per scale for this size and
+    batch (see oflow_tvl1_autotune).  Returns the chosen config per scale."""
+    p = (params or TVL1Params()).c()
+    n = len(pairs)
+    I0 = (Image * n)()
+    I1 = (Image * n)()
+    keep = []
+    for i, (a, b) in enumerate(pairs):
+        I0[i], ka = _image(a)
+        I1[i], kb = _image(b)
+        keep += [ka, kb]
+    cfg = (C.c_int * 16)()
+    h = _ctx(ctx)
+    _check(lib().oflow_tvl1_autotune(h, n, I0, I1, C.byref(p), cfg), h)
+    return [c for c in cfg if c >= 0]
 
 
 def tvl1(I0, I1, params: TVL1Params | None = None, ctx: Context | None = None,

@@ -80,6 +80,10 @@ SIGNATURES = {
     "oflow_tvl1_batch_profile": (_I, [_VP, _I, C.POINTER(Image), C.POINTER(Image),
                                       C.POINTER(Tvl1Params), C.POINTER(Flow),
                                       C.POINTER(Tvl1Stats), C.POINTER(Tvl1Profile)]),
+    "oflow_tvl1_autotune": (_I, [_VP, _I, C.POINTER(Image), C.POINTER(Image),
+                                 C.POINTER(Tvl1Params), C.POINTER(C.c_int)]),
+    "oflow_ctx_save_tuning": (_I, [_VP, C.c_char_p]),
+    "oflow_ctx_load_tuning": (_I, [_VP, C.c_char_p]),
     "oflow_hs_default_params": (None, [C.POINTER(HsParams)]),
     "oflow_hs": (_I, [_VP, C.POINTER(Image), C.POINTER(Image), C.POINTER(HsParams),
                       C.POINTER(Flow)]),

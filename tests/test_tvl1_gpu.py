@@ -182,3 +182,33 @@ def test_reference_class_mirror(of, orc):
     s.runDualTVL1Multiscale(a.astype(np.float32).ravel())
     s.runDualTVL1Multiscale(b.astype(np.float32).ravel())
     assert np.array_equal(s.getU(), U)
+
+
+def test_autotune_keeps_results_and_roundtrips(of, tmp_path):
+    """The autotuner picks a configuration per scale; every configuration is
+    exact, so the flow after tuning is identical; the table survives a
+    save/load round trip into a fresh context."""
+    ctx = of.Context(0)
+    pairs = [_pair(s, 160, 120)[1:] for s in (61, 62)]
+    prm = of.TVL1Params(nscales=3, max_iterations=12)
+    before = of.tvl1_batch(pairs, prm, ctx)
+    cfg = of.tvl1_autotune(pairs, prm, ctx)
+    assert len(cfg) == 3 and all(0 <= c < 4 for c in cfg)
+    after = of.tvl1_batch(pairs, prm, ctx)
+    for (u0, v0), (u1, v1) in zip(before, after):
+        assert np.array_equal(u0, u1) and np.array_equal(v0, v1)
+    path = str(tmp_path / "tune.txt")
+    ctx.save_tuning(path)
+    lines = [l for l in open(path) if not l.startswith("#")]
+    assert len(lines) == 3 and all(l.startswith("tvl1 ") for l in lines)
+    ctx2 = of.Context(0)
+    ctx2.load_tuning(path)
+    again = of.tvl1_batch(pairs, prm, ctx2)
+    for (u0, v0), (u1, v1) in zip(before, again):
+        assert np.array_equal(u0, u1) and np.array_equal(v0, v1)
+    bad = tmp_path / "bad.txt"
+    bad.write_text("tvl1 1 2\n")
+    with pytest.raises(of.OflowError):
+        ctx2.load_tuning(str(bad))
+    ctx.close()
+    ctx2.close()
