@@ -386,6 +386,87 @@ def once(args):
     return 0
 
 
+METRIC_BATCH = "mixed batch pairs/s: 256 pairs, half HS half TV-L1, 5 sizes up to 1920x1080"
+
+
+def batch_arm(args, rank, world, local_rank):
+    """The batched uneven workload: 256 pairs with sizes uniform over
+    {320x240, 640x480, 1024x436, 1280x720, 1920x1080}, half Horn-Schunck
+    (alpha 15, 200 sweeps) and half TV-L1 (5 scales x 5 warps x <= 50),
+    solved as one oflow_batch schedule (one graph, a branch per group)."""
+    import torch
+    import oflow
+    from oflow import multigpu, synth, synth_gpu
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    specs = multigpu.shard(synth.batch_specs(args.batch_pairs, seed=rank), 0, 1)
+    tp = oflow.TVL1Params(nscales=5, max_iterations=50)
+    hp = oflow.HSParams(15.0, 1, 1, 200)
+    groups = {}
+    for i, (solver, w, h, seed) in enumerate(specs):
+        groups.setdefault((solver, w, h), []).append(i)
+    frames = [None] * len(specs)
+    for (solver, w, h), idx in groups.items():
+        if solver == "tvl1":
+            a, b, *_ = synth_gpu.tvl1_pairs(len(idx), w, h, seed=hash((w, h)) & 0xffff, device=dev)
+        else:
+            a, b, *_ = synth_gpu.hs_pairs(len(idx), w, h, seed=hash((w, h)) & 0xffff, device=dev)
+        for k, i in enumerate(idx):
+            frames[i] = (a[k].contiguous(), b[k].contiguous())
+    jobs = [(solver, frames[i][0], frames[i][1], tp if solver == "tvl1" else hp)
+            for i, (solver, w, h, seed) in enumerate(specs)]
+    outs = [(torch.empty((h, w), dtype=torch.float32, device=dev),
+             torch.empty((h, w), dtype=torch.float32, device=dev)) for (_, w, h, _) in specs]
+    ctx = oflow.Context(local_rank)
+    stream = torch.cuda.current_stream(dev)
+    ctx.set_stream(stream.cuda_stream)
+    for (solver, w, h), idx in groups.items():  # tile shapes per TV-L1 group (untimed)
+        if solver == "tvl1":
+            oflow.tvl1_autotune([frames[i] for i in idx], tp, ctx)
+    for _ in range(args.warmup):
+        oflow.batch(jobs, ctx, out=outs)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local_rank) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            oflow.batch(jobs, ctx, out=outs)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3
+    # end to end: pinned host frames in, host flows out
+    h_jobs = [(s_, f0.cpu().pin_memory().numpy(), f1.cpu().pin_memory().numpy(), p_)
+              for (s_, f0, f1, p_) in jobs]
+    h_outs = [(torch.empty(o[0].shape).pin_memory().numpy(),
+               torch.empty(o[0].shape).pin_memory().numpy()) for o in outs]
+    oflow.batch(h_jobs, ctx, out=h_outs)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    e2e_steps = max(2, args.steps // 2)
+    for _ in range(e2e_steps):
+        oflow.batch(h_jobs, ctx, out=h_outs)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_e2e = e0.elapsed_time(e1) / 1e3
+    n = len(specs)
+    px = sum(w * h for (_, w, h, _) in specs)
+    line = {"metric": METRIC_BATCH, "value": n * args.steps / t, "unit": "pairs/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "mixed batch (HS alpha 15, 200 sweeps; TV-L1 5x5x<=50)",
+                       "pairs": n, "groups": len(groups), "megapixels_per_step": px / 1e6,
+                       "l2": "inputs larger than L2"},
+            "e2e": {"value": n * e2e_steps / t_e2e, "unit": "pairs/s",
+                    "h2d_bytes_per_step": sum(f[0].nbytes + f[1].nbytes for (_, f0, f1, _) in h_jobs
+                                              for f in [(f0, f1)]),
+                    "d2h_bytes_per_step": 2 * 4 * px},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -395,6 +476,10 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--workload", choices=["tvl1", "batch"], default="tvl1",
+                    help="tvl1: the 1024x436 TV-L1 workload (default); batch: the 256-pair "
+                         "mixed HS/TV-L1 workload")
+    ap.add_argument("--batch-pairs", type=int, default=256)
     ap.add_argument("--cpu-pairs", type=int, default=30)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--cpu-worker", action="store_true", help=argparse.SUPPRESS)
@@ -415,6 +500,8 @@ def main():
         return reference_arm(args, rank)
     if args.once:
         return once(args)
+    if args.workload == "batch":
+        return batch_arm(args, rank, world, local_rank)
     return our_arm(args, rank, world, local_rank)
 
 

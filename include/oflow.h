@@ -202,6 +202,26 @@ oflow_status oflow_hs_noalloc(const float *I0, const float *I1, int width, int h
                               int pitch, const oflow_hs_params *p, float *u, float *v,
                               int out_pitch, void *stream);
 
+/* ------------------------------------------------------------ mixed batches */
+typedef enum { OFLOW_SOLVER_TVL1 = 0, OFLOW_SOLVER_HS = 1 } oflow_solver;
+
+/* One frame pair of a mixed batch. */
+typedef struct {
+    int solver;                     /* oflow_solver */
+    oflow_image I0, I1;
+    const oflow_tvl1_params *tvl1;  /* used when solver == OFLOW_SOLVER_TVL1 */
+    const oflow_hs_params *hs;      /* used when solver == OFLOW_SOLVER_HS */
+    oflow_flow out;
+} oflow_job;
+
+/* Solves n pairs of mixed solvers and sizes as one schedule: the pairs are
+ * grouped by (solver, size, dtype, parameters), each group is a batched plan,
+ * and all groups' launch sequences are captured into one CUDA graph as
+ * parallel branches, so groups run concurrently on the device.  The graph is
+ * kept for the batch composition and replayed when the same composition
+ * comes again. */
+oflow_status oflow_batch(oflow_ctx *ctx, int n, const oflow_job *jobs);
+
 /* ------------------------------------------------------------ Lucas-Kanade */
 /* spac: spatial derivative taps (1,3,5,7,9); temp: temporal taps
  * (1,2,3,5,7,9); window: odd window side (src/lk/cuda/lucaskanade.cuh:8).

@@ -60,6 +60,25 @@ void unstage_plane(const float *src, int w, int h, float *dst, int pitch, int lo
 
 }  // namespace oflow
 
+namespace {
+// A mixed batch: one plan per (solver, size, dtype, parameters) group and one
+// graph with a parallel branch per group.
+struct MixedBatch {
+    std::vector<std::string> key;
+    std::vector<std::vector<int>> members;  // job indices per group
+    std::vector<std::unique_ptr<TvPlan>> tv;
+    std::vector<std::unique_ptr<HsPlan>> hs;
+    std::vector<int> kind, slot;            // per group: solver and index into tv/hs
+    std::vector<cudaStream_t> streams;
+    std::vector<cudaEvent_t> events;
+    Graph graph;
+    ~MixedBatch() {
+        for (auto s : streams) cudaStreamDestroy(s);
+        for (auto e : events) cudaEventDestroy(e);
+    }
+};
+}  // namespace
+
 struct oflow_ctx {
     int device = 0;
     cudaStream_t own = nullptr;
@@ -70,6 +89,7 @@ struct oflow_ctx {
     std::vector<std::unique_ptr<PyrLkPlan>> pyrlk;
     std::vector<std::unique_ptr<LkPlan>> lk;
     TuneTable tune;  // autotuned kernel configurations, consulted by new plans
+    std::vector<std::unique_ptr<MixedBatch>> mixed;
     cudaStream_t stream() const { return user ? user : own; }
 };
 
@@ -247,6 +267,7 @@ oflow_status oflow_ctx_destroy(oflow_ctx *ctx) {
     ctx->hs.clear();
     ctx->pyrlk.clear();
     ctx->lk.clear();
+    ctx->mixed.clear();
     if (ctx->own) cudaStreamDestroy(ctx->own);
     delete ctx;
     return OFLOW_OK;
@@ -266,6 +287,7 @@ oflow_status oflow_ctx_trim(oflow_ctx *ctx) {
         ctx->hs.clear();
         ctx->pyrlk.clear();
         ctx->lk.clear();
+        ctx->mixed.clear();
     });
 }
 
@@ -342,6 +364,121 @@ oflow_status oflow_tvl1_autotune(oflow_ctx *ctx, int n, const oflow_image *I0,
         if (cfg_per_scale)
             for (int s = 0; s < OFLOW_MAX_SCALES; s++)
                 cfg_per_scale[s] = s < pl.nscales() ? pl.tb_config(s) : -1;
+    });
+}
+
+oflow_status oflow_batch(oflow_ctx *ctx, int n, const oflow_job *jobs) {
+    return guard(ctx, [&] {
+        OF_CHECK(ctx != nullptr && jobs != nullptr && n >= 1, "batch: empty or null");
+        // group key per job
+        std::vector<std::string> gkeys;
+        std::vector<std::vector<int>> members;
+        for (int i = 0; i < n; i++) {
+            const oflow_job &j = jobs[i];
+            check_image(&j.I0, "I0");
+            check_image(&j.I1, "I1");
+            check_flow(&j.out, j.I0.width);
+            OF_CHECK(j.I0.width == j.I1.width && j.I0.height == j.I1.height && j.I0.dtype == j.I1.dtype,
+                     "batch: frames of a pair differ");
+            std::string k;
+            char hdr[64];
+            snprintf(hdr, sizeof hdr, "%d:%d:%d:%d:", j.solver, j.I0.width, j.I0.height, j.I0.dtype);
+            k = hdr;
+            if (j.solver == OFLOW_SOLVER_TVL1) {
+                check_tvl1_params(j.tvl1);
+                k.append(reinterpret_cast<const char *>(j.tvl1), sizeof(oflow_tvl1_params));
+            } else if (j.solver == OFLOW_SOLVER_HS) {
+                OF_CHECK(j.hs != nullptr, "batch: null hs params");
+                k.append(reinterpret_cast<const char *>(j.hs), sizeof(oflow_hs_params));
+            } else {
+                throw Error(OFLOW_ERR_BAD_ARG, "batch: unknown solver");
+            }
+            auto it = std::find(gkeys.begin(), gkeys.end(), k);
+            if (it == gkeys.end()) {
+                gkeys.push_back(k);
+                members.emplace_back();
+                it = gkeys.end() - 1;
+            }
+            members[it - gkeys.begin()].push_back(i);
+        }
+        std::vector<std::string> comp;
+        for (size_t g = 0; g < gkeys.size(); g++)
+            comp.push_back(gkeys[g] + "#" + std::to_string(members[g].size()));
+        MixedBatch *mb = nullptr;
+        for (auto &m : ctx->mixed)
+            if (m->key == comp) mb = m.get();
+        if (!mb) {
+            std::unique_ptr<MixedBatch> m(new MixedBatch());
+            m->key = comp;
+            m->members = members;
+            for (size_t g = 0; g < gkeys.size(); g++) {
+                const oflow_job &j = jobs[members[g][0]];
+                const int B = (int)members[g].size();
+                m->kind.push_back(j.solver);
+                if (j.solver == OFLOW_SOLVER_TVL1) {
+                    m->slot.push_back((int)m->tv.size());
+                    m->tv.emplace_back(new TvPlan(j.I0.width, j.I0.height, B, j.I0.dtype, *j.tvl1,
+                                                  false, &ctx->tune));
+                } else {
+                    m->slot.push_back((int)m->hs.size());
+                    m->hs.emplace_back(new HsPlan(j.I0.width, j.I0.height, B, j.I0.dtype, *j.hs));
+                }
+                cudaStream_t s;
+                OF_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+                m->streams.push_back(s);
+                cudaEvent_t e;
+                OF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+                m->events.push_back(e);
+            }
+            cudaEvent_t fork;
+            OF_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+            m->events.push_back(fork);
+            ctx->mixed.emplace_back(std::move(m));
+            while (ctx->mixed.size() > 4) ctx->mixed.erase(ctx->mixed.begin());
+            mb = ctx->mixed.back().get();
+        }
+        const cudaStream_t st = ctx->stream();
+        const size_t G = mb->kind.size();
+        // stage inputs (outside the graph: host copies from pageable memory)
+        for (size_t g = 0; g < G; g++)
+            for (size_t b = 0; b < mb->members[g].size(); b++) {
+                const oflow_job &j = jobs[mb->members[g][b]];
+                void *d0 = mb->kind[g] == OFLOW_SOLVER_TVL1 ? mb->tv[mb->slot[g]]->raw_input((int)b, 0)
+                                                            : mb->hs[mb->slot[g]]->raw_input((int)b, 0);
+                void *d1 = mb->kind[g] == OFLOW_SOLVER_TVL1 ? mb->tv[mb->slot[g]]->raw_input((int)b, 1)
+                                                            : mb->hs[mb->slot[g]]->raw_input((int)b, 1);
+                stage_image(j.I0, d0, dtype_size(j.I0.dtype), st);
+                stage_image(j.I1, d1, dtype_size(j.I1.dtype), st);
+            }
+        if (!mb->graph.ready()) {
+            mb->graph.capture(st, [&](cudaStream_t s) {
+                cudaEvent_t fork = mb->events.back();
+                OF_CUDA(cudaEventRecord(fork, s));
+                for (size_t g = 0; g < G; g++) {
+                    OF_CUDA(cudaStreamWaitEvent(mb->streams[g], fork, 0));
+                    if (mb->kind[g] == OFLOW_SOLVER_TVL1)
+                        mb->tv[mb->slot[g]]->record(mb->streams[g]);
+                    else
+                        mb->hs[mb->slot[g]]->record(mb->streams[g]);
+                    OF_CUDA(cudaEventRecord(mb->events[g], mb->streams[g]));
+                    OF_CUDA(cudaStreamWaitEvent(s, mb->events[g], 0));
+                }
+            });
+        }
+        mb->graph.launch(st);
+        bool device_only = true;
+        for (size_t g = 0; g < G; g++)
+            for (size_t b = 0; b < mb->members[g].size(); b++) {
+                const oflow_job &j = jobs[mb->members[g][b]];
+                const float *ou = mb->kind[g] == OFLOW_SOLVER_TVL1 ? mb->tv[mb->slot[g]]->out_u((int)b)
+                                                                   : mb->hs[mb->slot[g]]->out_u((int)b);
+                const float *ov = mb->kind[g] == OFLOW_SOLVER_TVL1 ? mb->tv[mb->slot[g]]->out_v((int)b)
+                                                                   : mb->hs[mb->slot[g]]->out_v((int)b);
+                unstage_plane(ou, j.I0.width, j.I0.height, j.out.u, j.out.pitch, j.out.location, st);
+                unstage_plane(ov, j.I0.width, j.I0.height, j.out.v, j.out.pitch, j.out.location, st);
+                if (j.out.location == OFLOW_HOST) device_only = false;
+            }
+        finish(ctx, device_only);
     });
 }
 

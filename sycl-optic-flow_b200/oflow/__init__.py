@@ -22,8 +22,8 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .capi import (LIB_PATH, OflowError, Flow, Image, HsParams, LkParams, Tvl1Params,
-                   Tvl1Profile, Tvl1Stats, lib, status_string)
+from .capi import (LIB_PATH, SOLVER_HS, SOLVER_TVL1, Flow, HsParams, Image, Job, LkParams,
+                   OflowError, Tvl1Params, Tvl1Profile, Tvl1Stats, lib, status_string)
 
 __all__ = [
     "Context", "OflowError", "TVL1Params", "HSParams", "LKParams", "tvl1", "tvl1_batch",
@@ -315,6 +315,31 @@ def hs_batch(pairs, params: HSParams | None = None, ctx: Context | None = None, 
 
 def hs(I0, I1, params: HSParams | None = None, ctx: Context | None = None, out=None):
     return hs_batch([(I0, I1)], params, ctx, None if out is None else [out])[0]
+
+
+# ------------------------------------------------------------------ mixed batches
+def batch(jobs, ctx: Context | None = None, out=None):
+    """Solve a mixed list of jobs ("tvl1" | "hs", I0, I1, params) as one
+    schedule (oflow_batch).  Returns a list of (u, v)."""
+    n = len(jobs)
+    J = (Job * n)()
+    keep, res = [], []
+    for i, (solver, a, b, prm) in enumerate(jobs):
+        ia, ka = _image(a)
+        ib, kb = _image(b)
+        f, uv = _outputs(a, ia.height, ia.width, None if out is None else out[i])
+        cp = prm.c()
+        keep += [ka, kb, cp]
+        if solver == "tvl1":
+            J[i] = Job(SOLVER_TVL1, ia, ib, C.pointer(cp), None, f)
+        elif solver == "hs":
+            J[i] = Job(SOLVER_HS, ia, ib, None, C.pointer(cp), f)
+        else:
+            raise ValueError("solver must be 'tvl1' or 'hs'")
+        res.append(uv)
+    h = _ctx(ctx)
+    _check(lib().oflow_batch(h, n, J), h)
+    return res
 
 
 # ------------------------------------------------------------------ Lucas-Kanade

@@ -58,6 +58,13 @@ class LkParams(C.Structure):
                 ("iters", C.c_int)]
 
 
+class Job(C.Structure):
+    _fields_ = [("solver", C.c_int), ("I0", Image), ("I1", Image),
+                ("tvl1", C.POINTER(Tvl1Params)), ("hs", C.POINTER(HsParams)), ("out", Flow)]
+
+
+SOLVER_TVL1, SOLVER_HS = 0, 1
+
 # every entry point of include/oflow.h: name -> (restype, argtypes)
 _VP, _I = C.c_void_p, C.c_int
 SIGNATURES = {
@@ -90,6 +97,7 @@ SIGNATURES = {
     "oflow_hs_batch": (_I, [_VP, _I, C.POINTER(Image), C.POINTER(Image), C.POINTER(HsParams),
                             C.POINTER(Flow)]),
     "oflow_hs_noalloc": (_I, [_VP, _VP, _I, _I, _I, C.POINTER(HsParams), _VP, _VP, _I, _VP]),
+    "oflow_batch": (_I, [_VP, _I, C.POINTER(Job)]),
     "oflow_lk_default_params": (None, [C.POINTER(LkParams)]),
     "oflow_lk": (_I, [_VP, C.POINTER(Image), _I, C.POINTER(LkParams), C.POINTER(Flow)]),
     "oflow_pyrlk": (_I, [_VP, C.POINTER(Image), C.POINTER(Image), C.POINTER(LkParams),

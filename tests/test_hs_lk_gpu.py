@@ -97,3 +97,23 @@ def test_pyrlk_golden_and_accuracy(of, ctx):
     l = synth.lk_pair(seed=0)
     u, v = of.pyrlk(l.I0, l.I1, of.LKParams(), ctx)
     assert synth.epe(u, v, l.u, l.v, l.valid, 8) < 1.0
+
+
+def test_mixed_batch_matches_single_solves(of, ctx):
+    """oflow_batch: HS and TV-L1 pairs of several sizes in one multi-branch
+    graph give the same flows as solving each pair alone; the replayed graph
+    (same composition) gives them again."""
+    from oflow import synth
+    tp = of.TVL1Params(nscales=3, max_iterations=10)
+    hp = of.HSParams(15.0, 1, 1, 30)
+    jobs = []
+    for k, (w, h) in enumerate([(96, 64), (128, 96), (96, 64), (160, 120)]):
+        p = synth.tvl1_pair(seed=80 + k, w=w, h=h, radius=12.0)
+        jobs.append(("tvl1", synth.quantize(p.I0), synth.quantize(p.I1), tp))
+        q = synth.hs_pair(seed=90 + k, w=w, h=h)
+        jobs.append(("hs", q.I0, q.I1, hp))
+    for _ in range(2):
+        res = of.batch(jobs, ctx)
+        for (solver, a, b, prm), (u, v) in zip(jobs, res):
+            su, sv = (of.tvl1 if solver == "tvl1" else of.hs)(a, b, prm, ctx)
+            assert _same(u, su) and _same(v, sv)
