@@ -222,6 +222,50 @@ typedef struct {
  * comes again. */
 oflow_status oflow_batch(oflow_ctx *ctx, int n, const oflow_job *jobs);
 
+/* --------------------------------------------------- learned warm start (TV-L1) */
+/* A small encoder-decoder network (4 stages, 32/64/96/128 channels, 3x3
+ * convolutions, BF16 weights and activations, FP32 accumulation on tensor
+ * cores) that predicts flow at 1/8 resolution -- the size of TV-L1 scale 3 --
+ * from a frame pair.  No counterpart in the reference.  One network object
+ * serves `batch` pairs of width x height per call. */
+typedef struct oflow_net oflow_net;
+int oflow_net_num_params(void);
+oflow_status oflow_net_create(oflow_ctx *ctx, int width, int height, int batch, oflow_net **out);
+oflow_status oflow_net_destroy(oflow_net *net);
+oflow_status oflow_net_out_size(const oflow_net *net, int *width, int *height);
+/* fp32 parameters (per layer: weights [K][3][3][C], then bias), host memory */
+oflow_status oflow_net_set_params(oflow_net *net, const float *params);
+oflow_status oflow_net_get_params(oflow_net *net, float *params);
+/* frames: device buffer [batch][2][height][width] (dtype OFLOW_U8 / OFLOW_F32);
+ * target: device f32 [batch][out_h][out_w][2].  One Adam step on the
+ * Charbonnier loss; *loss receives the mean loss before the step. */
+oflow_status oflow_net_train_step(oflow_net *net, const void *frames, int dtype,
+                                  const float *target, float lr, double *loss);
+/* flow: device f32 [batch][out_h][out_w][2] */
+oflow_status oflow_net_predict(oflow_net *net, const void *frames, int dtype, float *flow);
+
+/* TV-L1 warm-started by the network: the network's flow initialises scale 3
+ * and the solve runs scales 3..0 with `warm` (e.g. 2 warps x 20 iterations).
+ * With `plain` non-NULL the plain solve also runs and is the judge: a pair's
+ * warm result is kept only if its TV-L1 energy (non-linearised: sum |grad u|
+ * + lambda * sum |I1(x+u) - I0(x)|, bicubic warp with border zeroing) is at
+ * most 1.01 times the plain solve's; otherwise the plain result is returned.
+ * n must equal the network's batch and all frames its size.  energy_warm,
+ * energy_plain and accepted (arrays of n) may be NULL. */
+oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_image *I0,
+                             const oflow_image *I1, const oflow_tvl1_params *warm,
+                             const oflow_tvl1_params *plain, const oflow_flow *out,
+                             double *energy_warm, double *energy_plain, int *accepted);
+
+/* One product of a 3x3 convolution (pad 1, stride 1 or 2) on device buffers,
+ * for validating the network's kernels.  mode 0: y = conv(x, w) + bias (ReLU if
+ * relu; y f32 if out_f32 else bf16); mode 1: gin = conv^T(g) (f32; g masked by
+ * y_act > 0 when y_act is non-NULL); mode 2: gw = dL/dw, gbias = dL/db (f32).
+ * x, w, y_act: bf16; g: f32.  Shapes: x [N,H,W,C], w [K,3,3,C], y [N,P,Q,K]. */
+oflow_status oflow_conv3x3(int mode, int N, int H, int W, int C, int K, int stride, int relu,
+                           int out_f32, const void *x_or_g, const void *y_act, const void *w_or_x,
+                           void *out, const float *bias, float *gbias, void *stream);
+
 /* ------------------------------------------------------------ Lucas-Kanade */
 /* spac: spatial derivative taps (1,3,5,7,9); temp: temporal taps
  * (1,2,3,5,7,9); window: odd window side (src/lk/cuda/lucaskanade.cuh:8).

@@ -18,6 +18,7 @@
 #include "internal.hpp"
 #include "lk.hpp"
 #include "tvl1.hpp"
+#include "warmnet.hpp"
 
 using namespace oflow;
 
@@ -89,6 +90,7 @@ struct oflow_ctx {
     std::vector<std::unique_ptr<PyrLkPlan>> pyrlk;
     std::vector<std::unique_ptr<LkPlan>> lk;
     TuneTable tune;  // autotuned kernel configurations, consulted by new plans
+    std::vector<std::unique_ptr<TvPlan>> tv_warm;  // plans that start at scale 3
     std::vector<std::unique_ptr<MixedBatch>> mixed;
     cudaStream_t stream() const { return user ? user : own; }
 };
@@ -268,6 +270,7 @@ oflow_status oflow_ctx_destroy(oflow_ctx *ctx) {
     ctx->pyrlk.clear();
     ctx->lk.clear();
     ctx->mixed.clear();
+    ctx->tv_warm.clear();
     if (ctx->own) cudaStreamDestroy(ctx->own);
     delete ctx;
     return OFLOW_OK;
@@ -288,6 +291,7 @@ oflow_status oflow_ctx_trim(oflow_ctx *ctx) {
         ctx->pyrlk.clear();
         ctx->lk.clear();
         ctx->mixed.clear();
+        ctx->tv_warm.clear();
     });
 }
 
@@ -634,6 +638,166 @@ oflow_status oflow_pyrlk(oflow_ctx *ctx, const oflow_image *I0, const oflow_imag
             unstage_plane(pl->out_v(0), g.w, g.h, out->v, out->pitch, out->location, st);
         }
         finish(ctx, out->location == OFLOW_DEVICE);
+    });
+}
+
+}  // extern "C"
+
+struct oflow_net {
+    oflow_ctx *ctx;
+    std::unique_ptr<WarmNet> net;
+};
+
+extern "C" {
+
+int oflow_net_num_params(void) { return warmnet_num_params(); }
+
+oflow_status oflow_net_create(oflow_ctx *ctx, int width, int height, int batch, oflow_net **out) {
+    if (!out) return OFLOW_ERR_BAD_ARG;
+    *out = nullptr;
+    return guard(ctx, [&] {
+        OF_CHECK(ctx != nullptr, "null context");
+        std::unique_ptr<oflow_net> n(new oflow_net());
+        n->ctx = ctx;
+        n->net.reset(new WarmNet(width, height, batch));
+        *out = n.release();
+    });
+}
+
+oflow_status oflow_net_destroy(oflow_net *net) {
+    if (!net) return OFLOW_ERR_BAD_ARG;
+    cudaStreamSynchronize(net->ctx->stream());
+    delete net;
+    return OFLOW_OK;
+}
+
+oflow_status oflow_net_out_size(const oflow_net *net, int *w, int *h) {
+    if (!net || !w || !h) return OFLOW_ERR_BAD_ARG;
+    *w = net->net->out_w();
+    *h = net->net->out_h();
+    return OFLOW_OK;
+}
+
+oflow_status oflow_net_set_params(oflow_net *net, const float *params) {
+    if (!net || !params) return OFLOW_ERR_BAD_ARG;
+    return guard(net->ctx, [&] { net->net->set_params(params, net->ctx->stream()); });
+}
+
+oflow_status oflow_net_get_params(oflow_net *net, float *params) {
+    if (!net || !params) return OFLOW_ERR_BAD_ARG;
+    return guard(net->ctx, [&] { net->net->get_params(params, net->ctx->stream()); });
+}
+
+oflow_status oflow_net_train_step(oflow_net *net, const void *frames, int dtype,
+                                  const float *target, float lr, double *loss) {
+    if (!net || !frames || !target) return OFLOW_ERR_BAD_ARG;
+    return guard(net->ctx, [&] {
+        OF_CHECK(dtype == OFLOW_U8 || dtype == OFLOW_F32, "net: bad dtype");
+        const size_t ps = (size_t)net->net->width() * net->net->height();
+        const double l = net->net->train_step(frames, dtype, ps, target, lr, net->ctx->stream());
+        if (loss) *loss = l;
+    });
+}
+
+oflow_status oflow_net_predict(oflow_net *net, const void *frames, int dtype, float *flow) {
+    if (!net || !frames || !flow) return OFLOW_ERR_BAD_ARG;
+    return guard(net->ctx, [&] {
+        OF_CHECK(dtype == OFLOW_U8 || dtype == OFLOW_F32, "net: bad dtype");
+        const cudaStream_t st = net->ctx->stream();
+        const size_t ps = (size_t)net->net->width() * net->net->height();
+        net->net->forward(frames, dtype, ps, st);
+        net->net->flow_to(nullptr, 0, flow, st);
+        OF_CUDA(cudaGetLastError());
+        OF_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_image *I0,
+                             const oflow_image *I1, const oflow_tvl1_params *warm,
+                             const oflow_tvl1_params *plain, const oflow_flow *out,
+                             double *energy_warm, double *energy_plain, int *accepted) {
+    return guard(ctx, [&] {
+        OF_CHECK(ctx != nullptr && net != nullptr && I0 && I1 && out, "tvl1 warm: null argument");
+        OF_CHECK(n == net->net->batch(), "tvl1 warm: n must equal the network batch");
+        check_tvl1_params(warm);
+        if (plain) check_tvl1_params(plain);
+        const std::vector<Group> groups = group_pairs(n, I0, I1);
+        OF_CHECK(groups.size() == 1, "tvl1 warm: pairs must share one size and dtype");
+        const Group &g = groups[0];
+        OF_CHECK(g.w == net->net->width() && g.h == net->net->height(),
+                 "tvl1 warm: frame size differs from the network's");
+        for (int i = 0; i < n; i++) check_flow(&out[i], g.w);
+        const cudaStream_t st = ctx->stream();
+        TvPlan *wp = nullptr;
+        for (auto &q : ctx->tv_warm)
+            if (q->width() == g.w && q->height() == g.h && q->batch() == n && q->dtype() == g.dtype &&
+                same(q->params(), *warm))
+                wp = q.get();
+        if (!wp) {
+            ctx->tv_warm.emplace_back(new TvPlan(g.w, g.h, n, g.dtype, *warm, false, &ctx->tune, 3));
+            keep_recent(ctx->tv_warm);
+            wp = ctx->tv_warm.back().get();
+        }
+        OF_CHECK(wp->level_w(3) == net->net->out_w() && wp->level_h(3) == net->net->out_h(),
+                 "tvl1 warm: scale 3 does not match the network output");
+        for (int b = 0; b < n; b++) {
+            stage_image(I0[b], wp->raw_input(b, 0), dtype_size(g.dtype), st);
+            stage_image(I1[b], wp->raw_input(b, 1), dtype_size(g.dtype), st);
+        }
+        net->net->forward(wp->raw_input(0, 0), g.dtype, wp->plane_stride(), st);
+        net->net->flow_to(wp->uz(), wp->plane_stride(), nullptr, st);
+        wp->run(st);
+        std::vector<double> ew(n), ep(n, 0.0);
+        std::vector<int> acc(n, 1);
+        wp->true_energy(ew.data(), st);
+        TvPlan *pp = nullptr;
+        if (plain) {
+            pp = &tv_plan(ctx, g.w, g.h, n, g.dtype, *plain, false);
+            for (int b = 0; b < n; b++) {
+                stage_image(I0[b], pp->raw_input(b, 0), dtype_size(g.dtype), st);
+                stage_image(I1[b], pp->raw_input(b, 1), dtype_size(g.dtype), st);
+            }
+            pp->run(st);
+            pp->true_energy(ep.data(), st);
+            for (int b = 0; b < n; b++) acc[b] = ew[b] <= 1.01 * ep[b] ? 1 : 0;
+        }
+        for (int b = 0; b < n; b++) {
+            const TvPlan *src = acc[b] ? wp : pp;
+            unstage_plane(src->out_u(b), g.w, g.h, out[b].u, out[b].pitch, out[b].location, st);
+            unstage_plane(src->out_v(b), g.w, g.h, out[b].v, out[b].pitch, out[b].location, st);
+            if (energy_warm) energy_warm[b] = ew[b];
+            if (energy_plain) energy_plain[b] = ep[b];
+            if (accepted) accepted[b] = acc[b];
+        }
+        OF_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+oflow_status oflow_conv3x3(int mode, int N, int H, int W, int C, int K, int stride, int relu,
+                           int out_f32, const void *a, const void *y_act, const void *b, void *out,
+                           const float *bias, float *gbias, void *stream) {
+    return guard(nullptr, [&] {
+        OF_CHECK(N >= 1 && H >= 1 && W >= 1 && C >= 1 && K >= 1 && (stride == 1 || stride == 2),
+                 "conv3x3: bad shape");
+        OF_CHECK(a && b && out, "conv3x3: null buffer");
+        const ConvDims d{N, H, W, C, conv_out(H, stride), conv_out(W, stride), K, stride};
+        const cudaStream_t st = static_cast<cudaStream_t>(stream);
+        if (mode == 0) {
+            OF_CHECK(bias != nullptr, "conv3x3: null bias");
+            conv_forward(d, static_cast<const __nv_bfloat16 *>(a), static_cast<const __nv_bfloat16 *>(b),
+                         bias, out, out_f32 != 0, relu != 0, st);
+        } else if (mode == 1) {
+            conv_backward_data(d, static_cast<const float *>(a), static_cast<const __nv_bfloat16 *>(y_act),
+                               static_cast<const __nv_bfloat16 *>(b), static_cast<float *>(out), false, st);
+        } else if (mode == 2) {
+            OF_CHECK(gbias != nullptr, "conv3x3: null bias gradient");
+            conv_backward_weight(d, static_cast<const float *>(a),
+                                 static_cast<const __nv_bfloat16 *>(y_act),
+                                 static_cast<const __nv_bfloat16 *>(b), static_cast<float *>(out), gbias, st);
+        } else {
+            throw Error(OFLOW_ERR_BAD_ARG, "conv3x3: bad mode");
+        }
+        OF_CUDA(cudaGetLastError());
     });
 }
 

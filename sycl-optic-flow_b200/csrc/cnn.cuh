@@ -1,0 +1,66 @@
+// BF16 tensor-core convolution kernels (3x3, pad 1, stride 1 or 2) written as
+// implicit GEMMs with FP32 accumulation, and the small element-wise kernels
+// the warm-start network needs.  Layout: activations NHWC, weights [K][3][3][C]
+// (output channel, tap row, tap column, input channel).
+//
+// One generic kernel covers the three products of a convolution layer:
+//   forward      out[m=(n,p,q)][k]      = sum_{r,s,c} x[n][p*st+r-1][q*st+s-1][c] w[k][r][s][c]
+//   backward-in  gin[m=(n,y,x)][c]      = sum_{r,s,k} g[n][(y+1-r)/st][(x+1-s)/st][k] w[k][r][s][c]
+//                                         (taps whose division is inexact or out of range are 0)
+//   backward-w   gw[k][(r,s,c)]        += sum_{n,p,q} g[n][p][q][k] x[n][p*st+r-1][q*st+s-1][c]
+// Operands are gathered into shared memory tile by tile (BM x 16 and 16 x BN
+// bf16), multiplied with mma.sync.m16n8k16 (bf16 in, f32 accumulate).  With a
+// ReLU after the layer, the output gradient is masked by (out > 0) while it is
+// gathered.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace oflow {
+
+enum ConvMode { kConvFwd = 0, kConvBwdData = 1, kConvBwdWeight = 2 };
+
+struct ConvDims {
+    int N, H, W, C;   // input activations
+    int P, Q, K;      // output activations
+    int stride;
+};
+
+inline int conv_out(int n, int stride) { return stride == 1 ? n : (n + 1) / 2; }
+
+// forward: x bf16 [N,H,W,C], w bf16 [K,3,3,C], bias f32 [K] -> y [N,P,Q,K]
+// (bf16, or f32 when y_f32); relu applies max(0, .).
+void conv_forward(const ConvDims &d, const __nv_bfloat16 *x, const __nv_bfloat16 *w,
+                  const float *bias, void *y, bool y_f32, bool relu, cudaStream_t st);
+// backward-data: g f32 [N,P,Q,K] (masked by y_act > 0 when y_act != null,
+// y_act bf16 [N,P,Q,K]) -> gin f32 [N,H,W,C]; accumulate adds to gin.
+void conv_backward_data(const ConvDims &d, const float *g, const __nv_bfloat16 *y_act,
+                        const __nv_bfloat16 *w, float *gin, bool accumulate, cudaStream_t st);
+// backward-weight: gw f32 [K,3,3,C] and gb f32 [K] are overwritten.
+void conv_backward_weight(const ConvDims &d, const float *g, const __nv_bfloat16 *y_act,
+                          const __nv_bfloat16 *x, float *gw, float *gb, cudaStream_t st);
+
+// element-wise helpers
+void cnn_f32_to_bf16(const float *src, __nv_bfloat16 *dst, size_t n, cudaStream_t st);
+// out[n][y][x][0..Ca) = lo[n][y/2][x/2][:], out[...][Ca..Ca+Cb) = skip[n][y][x][:]
+void upcat_forward(const __nv_bfloat16 *lo, int Hl, int Wl, int Ca, const __nv_bfloat16 *skip,
+                   int H, int W, int Cb, int N, __nv_bfloat16 *out, cudaStream_t st);
+// gradient of upcat: glo (overwritten) and gskip (added to)
+void upcat_backward(const float *g, int H, int W, int Ca, int Cb, int N, float *glo, int Hl,
+                    int Wl, float *gskip, cudaStream_t st);
+// network input: 2x2 box of two frames (u8 or f32, dense w x h, pair stride),
+// /255, into channels 0 and 1 of a [N, ceil(h/2), ceil(w/2), 16] bf16 tensor
+void cnn_input(const void *frames, int dtype, int w, int h, int N, size_t pair_stride,
+               __nv_bfloat16 *x0, cudaStream_t st);
+// Charbonnier loss between flow channels (0,1) of pred f32 [M,Kp] and target
+// f32 [M,2]; writes the gradient into g f32 [M,Kp] (other channels 0) and the
+// loss sum into loss (one double).
+void flow_loss(const float *pred, int Kp, const float *target, int M, float *g, double *loss,
+               cudaStream_t st);
+// Adam on fp32 parameters, then bf16 copies of the weights.
+void adam_step(float *p, const float *gp, float *m, float *v, size_t n, float lr, float b1,
+               float b2, float eps, int t, cudaStream_t st);
+
+}  // namespace oflow

@@ -825,6 +825,54 @@ __global__ void __launch_bounds__(kEnNT) k_energy(const float2 *Wxy, const float
     }
 }
 
+// Non-linearised TV-L1 energy of (u1, u2) at the finest scale: sum of
+// |grad u1| + |grad u2| (forward differences, double) + lambda * sum
+// |I1(x+u) - I0(x)| with the bicubic sample and border zeroing of the warp
+// (bicubic_interpolation.cpp:141-163).  Used to compare two solutions of the
+// same pair at the same linearisation-free cost.
+__global__ void __launch_bounds__(kEnNT) k_energy_true(const float *__restrict__ pyr, size_t lp,
+                                                       const float2 *U0, const float2 *U1,
+                                                       size_t stride, int nx, int ny,
+                                                       float lambda, const TvCtrl *ctrl,
+                                                       double *partials, int max_blocks,
+                                                       unsigned *arrive, double *out) {
+    const int b = blockIdx.y;
+    const float2 *U = (ctrl[b].cur ? U1 : U0) + (size_t)b * stride;
+    const float *I0 = pyr + (size_t)(2 * b) * lp;
+    const float *I1 = pyr + (size_t)(2 * b + 1) * lp;
+    const int N = nx * ny;
+    double acc = 0.0;
+    for (int i = blockIdx.x * kEnNT + threadIdx.x; i < N; i += gridDim.x * kEnNT) {
+        const int x = i % nx, y = i / nx;
+        const float2 uc = U[i];
+        double f1x = 0, f1y = 0, f2x = 0, f2y = 0;
+        if (x < nx - 1) { const float2 r = U[i + 1]; f1x = (double)(r.x - uc.x); f2x = (double)(r.y - uc.y); }
+        if (y < ny - 1) { const float2 d = U[i + nx]; f1y = (double)(d.x - uc.x); f2y = (double)(d.y - uc.y); }
+        const float w = bicubic_at(I1, (float)x + uc.x, (float)y + uc.y, nx, ny, true);
+        acc += sqrt(f1x * f1x + f1y * f1y) + sqrt(f2x * f2x + f2y * f2y) +
+               (double)lambda * fabs((double)(w - __ldg(I0 + i)));
+    }
+    __shared__ double sred[kEnNT / 32];
+    __shared__ int s_last;
+    const double s = block_sum_double<kEnNT>(acc, sred);
+    double *part = partials + (size_t)b * max_blocks;
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = s;
+        __threadfence();
+        s_last = (atomicAdd(arrive + b, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    double a2 = 0.0;
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += kEnNT) a2 += __ldcg(part + k);
+    const double tot = block_sum_double<kEnNT>(a2, sred);
+    if (threadIdx.x == 0) {
+        out[b] = tot;
+        arrive[b] = 0;
+    }
+}
+
 // ---------------------------------------------------------------- output
 __global__ void k_split(const float2 *U0, const float2 *U1, size_t stride, int N, float *ou,
                         float *ov, const TvCtrl *ctrl) {
@@ -893,7 +941,7 @@ static int tb_pick(int nx, int ny, int B) {
 }
 
 TvPlan::TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, bool trace,
-               const TuneTable *tuned)
+               const TuneTable *tuned, int start_scale)
     : w_(w), h_(h), B_(B), dtype_(dtype), prm_(prm), trace_(trace) {
     OF_CHECK(w >= 8 && h >= 8, "tvl1: frames must be at least 8x8");
     OF_CHECK(B >= 1, "tvl1: empty batch");
@@ -914,6 +962,9 @@ TvPlan::TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, boo
         OF_CHECK(tapsz_.size <= nx_[s] && tapsz_.size <= ny_[s],
                  "tvl1: pyramid level smaller than the Gaussian window");
     for (int s = 0; s < ns_; s++) OF_CHECK(nx_[s] >= 2 && ny_[s] >= 2, "tvl1: level below 2x2");
+    OF_CHECK(start_scale < ns_, "tvl1: warm-start scale beyond the pyramid");
+    s0_ = start_scale >= 0 ? start_scale : ns_ - 1;
+    warm_ = start_scale >= 0;
 
     const size_t N0 = (size_t)w * h;
     N0_ = N0;
@@ -951,6 +1002,8 @@ TvPlan::TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, boo
     o_iters_ = ar_.reserve((size_t)B * iter_stride_ * 4);
     energy_slots_ = trace ? ns_ * prm.warps * prm.max_iterations : 1;
     o_energy_ = ar_.reserve((size_t)B * energy_slots_ * 8);
+    o_tarr_ = ar_.reserve(sizeof(unsigned) * B);
+    o_tout_ = ar_.reserve(sizeof(double) * B);
     ar_.commit();
     OF_CUDA(cudaMemset(ar_.at<char>(o_ctrl_), 0, B * sizeof(TvCtrl)));
     tb_set_smem_attrs();
@@ -963,6 +1016,7 @@ void *TvPlan::raw_input(int b, int k) const {
 const float *TvPlan::out_u(int b) const { return ar_.at<float>(o_out_) + (size_t)b * N0_; }
 const float *TvPlan::out_v(int b) const { return ar_.at<float>(o_out_) + (size_t)(B_ + b) * N0_; }
 const int *TvPlan::iters_dev() const { return ar_.at<int>(o_iters_); }
+float2 *TvPlan::uz() const { return ar_.at<float2>(o_Uz_); }
 
 int TvPlan::iter_launches_per_stage() const {
     if (trace_) return prm_.max_iterations;
@@ -1025,11 +1079,11 @@ void TvPlan::record(cudaStream_t st) {
     const float taut = prm_.tau / prm_.theta;
     const float eps2 = prm_.epsilon * prm_.epsilon;
     const float inv = 1 / prm_.zfactor;
-    for (int s = ns_ - 1; s >= 0; s--) {
+    for (int s = s0_; s >= 0; s--) {
         const int nx = nx_[s], ny = ny_[s];
         const size_t lp = (size_t)nx * ny;
         dim3 blk(32, 8), gr(div_up(nx, 32), div_up(ny, 8), B);
-        if (s < ns_ - 1) {
+        if (s < s0_) {
             const int cx = nx_[s + 1], cy = ny_[s + 1];
             k_zoom_flow<<<gr, blk, 0, st>>>(U0, U1, N0, cx, cy, Uz, nx, ny, (float)nx / cx,
                                             (float)ny / cy, inv, ctrl);
@@ -1042,7 +1096,8 @@ void TvPlan::record(cudaStream_t st) {
         dim3 ig(div_up(nx, kIterTW), div_up(ny, kIterTH), B);
         const int cfg = tb_cfg_[s];
         for (int wi = 0; wi < prm_.warps; wi++) {
-            const int mode = wi > 0 ? kWarpFromU : (s == ns_ - 1 ? kWarpZero : kWarpFromUz);
+            const int mode = wi > 0 ? kWarpFromU
+                                    : (s == s0_ ? (warm_ ? kWarpFromUz : kWarpZero) : kWarpFromUz);
             mark();
             k_warp<<<gr, blk, 0, st>>>(pyr + pyr_off_[s], lp, I1g, Wxy, Rc, U0, U1, Uz, P0, P1,
                                        N0, nx, ny, mode, wi == 0, ctrl);
@@ -1093,7 +1148,7 @@ void TvPlan::record(cudaStream_t st) {
 // per-kind totals (ms) and launch counts.
 void TvPlan::profile(cudaStream_t st, oflow_tvl1_profile *out) {
     Prof p;
-    const int stages = ns_ * prm_.warps;
+    const int stages = (s0_ + 1) * prm_.warps;
     const int nl = iter_launches_per_stage();
     p.ev.resize((size_t)2 * stages * (1 + nl) + 2);
     for (auto &e : p.ev) OF_CUDA(cudaEventCreate(&e));
@@ -1124,7 +1179,7 @@ void TvPlan::profile(cudaStream_t st, oflow_tvl1_profile *out) {
         int k = 0;
         for (int st_i = 0; st_i < stages; st_i++) {
             // stages are recorded coarse to fine: stage index -> scale
-            const int scale = ns_ - 1 - st_i / prm_.warps;
+            const int scale = s0_ - st_i / prm_.warps;
             OF_CUDA(cudaEventElapsedTime(&ms, p.ev[k], p.ev[k + 1]));
             out->warp_ms += ms;
             out->warp_launches += 1;
@@ -1205,6 +1260,19 @@ void TvPlan::autotune(cudaStream_t st, TuneTable *table, int reps) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     graph_.reset();  // the next run captures the new configurations
+}
+
+void TvPlan::true_energy(double *host_out, cudaStream_t st) {
+    unsigned *arrive = ar_.at<unsigned>(o_tarr_);
+    double *out = ar_.at<double>(o_tout_);
+    OF_CUDA(cudaMemsetAsync(arrive, 0, sizeof(unsigned) * B_, st));
+    k_energy_true<<<dim3(energy_blocks_, B_), kEnNT, 0, st>>>(
+        ar_.at<float>(o_pyr_) + pyr_off_[0], N0_, ar_.at<float2>(o_U0_), ar_.at<float2>(o_U1_), N0_,
+        w_, h_, prm_.lambda, ar_.at<TvCtrl>(o_ctrl_), ar_.at<double>(o_part_), max_blocks_,
+        arrive, out);
+    OF_CUDA(cudaGetLastError());
+    OF_CUDA(cudaMemcpyAsync(host_out, out, sizeof(double) * B_, cudaMemcpyDeviceToHost, st));
+    OF_CUDA(cudaStreamSynchronize(st));
 }
 
 void TvPlan::run(cudaStream_t st) {

@@ -38,8 +38,17 @@ void launch_resample(const float *src, size_t sstride, int nx, int ny, float *ds
 
 class TvPlan {
   public:
+    // start_scale >= 0: warm start -- the solve begins at that scale from the
+    // flow written into uz() (in that scale's pixel units) instead of zero at
+    // the coarsest scale.
     TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, bool trace = false,
-           const TuneTable *tuned = nullptr);
+           const TuneTable *tuned = nullptr, int start_scale = -1);
+    float2 *uz() const;
+    size_t plane_stride() const { return N0_; }
+    int start_scale() const { return s0_; }
+    // Non-linearised TV-L1 energy of the last result, per pair (see
+    // k_energy_true): sum |grad u1| + |grad u2| + lambda * sum |I1(x+u) - I0(x)|.
+    void true_energy(double *host_out, cudaStream_t st);
     // Times each blocked-iteration configuration per scale on the current
     // buffers, keeps the fastest and records it in `table`.
     void autotune(cudaStream_t st, TuneTable *table, int reps = 3);
@@ -91,6 +100,9 @@ class TvPlan {
     int launches_ = 0;
     Arena ar_;
     int tb_cfg_[OFLOW_MAX_SCALES] = {};
+    int s0_ = 0;
+    bool warm_ = false;
+    size_t o_tarr_ = 0, o_tout_ = 0;
     int iter_launches_per_stage() const;
     size_t o_Wxy_ = 0, o_Rc_ = 0;
     size_t o_raw_ = 0, o_T_ = 0, o_pyr_ = 0, o_I1g_ = 0, o_U0_ = 0, o_U1_ = 0,

@@ -342,6 +342,107 @@ def batch(jobs, ctx: Context | None = None, out=None):
     return res
 
 
+# ------------------------------------------------------------------ warm start
+def net_num_params() -> int:
+    return lib().oflow_net_num_params()
+
+
+class WarmNet:
+    """The warm-start network (oflow_net_*) for `batch` pairs of width x
+    height.  Frames and targets are CUDA torch tensors."""
+
+    def __init__(self, width: int, height: int, batch: int, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        self._h = C.c_void_p()
+        _check(lib().oflow_net_create(self.ctx.handle, width, height, batch, C.byref(self._h)),
+               self.ctx.handle)
+        ow, oh = C.c_int(), C.c_int()
+        lib().oflow_net_out_size(self._h, C.byref(ow), C.byref(oh))
+        self.width, self.height, self.batch = width, height, batch
+        self.out_w, self.out_h = ow.value, oh.value
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_params(self, params: np.ndarray):
+        p = np.ascontiguousarray(params, np.float32)
+        if p.size != net_num_params():
+            raise ValueError("wrong number of parameters")
+        _check(lib().oflow_net_set_params(self._h, p.ctypes.data_as(C.c_void_p)), self.ctx.handle)
+
+    def get_params(self) -> np.ndarray:
+        p = np.empty(net_num_params(), np.float32)
+        _check(lib().oflow_net_get_params(self._h, p.ctypes.data_as(C.c_void_p)), self.ctx.handle)
+        return p
+
+    def train_step(self, frames, target, lr: float) -> float:
+        """frames: CUDA [batch, 2, h, w] uint8/float32; target: CUDA float32
+        [batch, out_h, out_w, 2]."""
+        import torch
+        dt = 0 if frames.dtype == torch.uint8 else 1
+        loss = C.c_double()
+        _check(lib().oflow_net_train_step(self._h, C.c_void_p(frames.data_ptr()), dt,
+                                          C.c_void_p(target.data_ptr()), lr, C.byref(loss)),
+               self.ctx.handle)
+        return loss.value
+
+    def predict(self, frames):
+        import torch
+        dt = 0 if frames.dtype == torch.uint8 else 1
+        out = torch.empty((self.batch, self.out_h, self.out_w, 2), dtype=torch.float32,
+                          device=frames.device)
+        _check(lib().oflow_net_predict(self._h, C.c_void_p(frames.data_ptr()), dt,
+                                       C.c_void_p(out.data_ptr())), self.ctx.handle)
+        return out
+
+    def close(self):
+        if self._h:
+            lib().oflow_net_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def tvl1_warm(pairs, net: WarmNet, warm: TVL1Params, plain: TVL1Params | None = None,
+              ctx: Context | None = None, out=None):
+    """Warm-started TV-L1 (oflow_tvl1_warm).  Returns (results, info) with
+    info = {energy_warm, energy_plain, accepted} arrays."""
+    n = len(pairs)
+    I0 = (Image * n)()
+    I1 = (Image * n)()
+    O = (Flow * n)()
+    keep, res = [], []
+    for i, (a, b) in enumerate(pairs):
+        I0[i], ka = _image(a)
+        I1[i], kb = _image(b)
+        keep += [ka, kb]
+        O[i], uv = _outputs(a, I0[i].height, I0[i].width, None if out is None else out[i])
+        res.append(uv)
+    ew = np.zeros(n, np.float64)
+    ep = np.zeros(n, np.float64)
+    acc = np.zeros(n, np.int32)
+    wp = warm.c()
+    pp = plain.c() if plain is not None else None
+    h = (ctx or net.ctx).handle
+    _check(lib().oflow_tvl1_warm(h, net.handle, n, I0, I1, C.byref(wp),
+                                 C.byref(pp) if pp is not None else None, O,
+                                 ew.ctypes.data_as(C.c_void_p), ep.ctypes.data_as(C.c_void_p),
+                                 acc.ctypes.data_as(C.c_void_p)), h)
+    return res, {"energy_warm": ew, "energy_plain": ep, "accepted": acc.astype(bool)}
+
+
+def conv3x3(mode, N, H, W, C_, K, stride, relu, out_f32, a, y_act, b, out, bias=None, gbias=None):
+    """oflow_conv3x3 on CUDA torch tensors (validation of the network kernels)."""
+    ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
+    _check(lib().oflow_conv3x3(mode, N, H, W, C_, K, stride, int(relu), int(out_f32), ptr(a),
+                               ptr(y_act), ptr(b), ptr(out), ptr(bias), ptr(gbias), None))
+
+
 # ------------------------------------------------------------------ Lucas-Kanade
 def lk(frames, iframe: int, params: LKParams | None = None, ctx: Context | None = None,
        out=None):

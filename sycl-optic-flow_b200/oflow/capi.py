@@ -98,6 +98,18 @@ SIGNATURES = {
                             C.POINTER(Flow)]),
     "oflow_hs_noalloc": (_I, [_VP, _VP, _I, _I, _I, C.POINTER(HsParams), _VP, _VP, _I, _VP]),
     "oflow_batch": (_I, [_VP, _I, C.POINTER(Job)]),
+    "oflow_net_num_params": (_I, []),
+    "oflow_net_create": (_I, [_VP, _I, _I, _I, C.POINTER(C.c_void_p)]),
+    "oflow_net_destroy": (_I, [_VP]),
+    "oflow_net_out_size": (_I, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "oflow_net_set_params": (_I, [_VP, _VP]),
+    "oflow_net_get_params": (_I, [_VP, _VP]),
+    "oflow_net_train_step": (_I, [_VP, _VP, _I, _VP, C.c_float, C.POINTER(C.c_double)]),
+    "oflow_net_predict": (_I, [_VP, _VP, _I, _VP]),
+    "oflow_tvl1_warm": (_I, [_VP, _VP, _I, C.POINTER(Image), C.POINTER(Image),
+                             C.POINTER(Tvl1Params), C.POINTER(Tvl1Params), C.POINTER(Flow),
+                             _VP, _VP, _VP]),
+    "oflow_conv3x3": (_I, [_I, _I, _I, _I, _I, _I, _I, _I, _I, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "oflow_lk_default_params": (None, [C.POINTER(LkParams)]),
     "oflow_lk": (_I, [_VP, C.POINTER(Image), _I, C.POINTER(LkParams), C.POINTER(Flow)]),
     "oflow_pyrlk": (_I, [_VP, C.POINTER(Image), C.POINTER(Image), C.POINTER(LkParams),

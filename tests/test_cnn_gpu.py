@@ -1,0 +1,111 @@
+"""The warm-start network's BF16 tensor-core convolution kernels against a
+float64 CPU oracle (oracle/cnn_ref.py): forward, backward-data and
+backward-weight (the gradient check), stride 1 and 2, with and without the
+ReLU mask; then the network trains (loss falls) and the warm-started TV-L1
+respects its energy judge."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+REL = 2e-3  # bf16 operands are exact in f32 products; f32 sums over <= 9*224 terms
+
+
+def _bf16(t):
+    import torch
+    return t.to(torch.bfloat16)
+
+
+def _rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-12))
+
+
+@pytest.mark.parametrize("N,H,W,C,K,stride,relu", [(2, 9, 13, 16, 32, 1, True), (1, 12, 10, 32, 8, 2, False),
+                                                   (2, 7, 11, 48, 64, 2, True), (1, 16, 16, 160, 64, 1, True)])
+def test_conv_products_match_cpu_oracle(of, N, H, W, C, K, stride, relu):
+    import torch
+    from oracle import cnn_ref
+    g = torch.Generator().manual_seed(N * 1000 + C + K)
+    P, Q = cnn_ref.conv_out(H, stride), cnn_ref.conv_out(W, stride)
+    x = _bf16(torch.randn((N, H, W, C), generator=g))
+    w = _bf16(torch.randn((K, 3, 3, C), generator=g) * 0.1)
+    b = torch.randn(K, generator=g) * 0.1
+    xd, wd, bd = x.cuda(), w.cuda(), b.cuda()
+    # forward, f32 output
+    y = torch.empty((N, P, Q, K), dtype=torch.float32, device="cuda")
+    of.conv3x3(0, N, H, W, C, K, stride, relu, True, xd, None, wd, y, bias=bd)
+    ref = cnn_ref.forward(x.float().numpy(), w.float().numpy(), b.numpy(), stride, relu)
+    assert _rel(y.cpu().numpy(), ref) < REL
+    # forward, bf16 output (what the network stores)
+    yb = torch.empty((N, P, Q, K), dtype=torch.bfloat16, device="cuda")
+    of.conv3x3(0, N, H, W, C, K, stride, relu, False, xd, None, wd, yb, bias=bd)
+    assert _rel(yb.float().cpu().numpy(), ref) < 1e-2
+    # backward: gradients of sum(gout * y); gout is rounded to bf16 by the
+    # kernels, so the oracle gets the same rounded values
+    gout = torch.randn((N, P, Q, K), generator=g)
+    gout_b = _bf16(gout).float()
+    yact = yb if relu else None
+    gx_ref, gw_ref, gb_ref = cnn_ref.backward(x.float().numpy(), w.float().numpy(), gout_b.numpy(),
+                                              stride, yb.float().cpu().numpy() if relu else None)
+    gx = torch.empty((N, H, W, C), dtype=torch.float32, device="cuda")
+    of.conv3x3(1, N, H, W, C, K, stride, relu, True, gout.cuda(), yact, wd, gx)
+    gw = torch.empty((K, 3, 3, C), dtype=torch.float32, device="cuda")
+    gb = torch.empty(K, dtype=torch.float32, device="cuda")
+    of.conv3x3(2, N, H, W, C, K, stride, relu, True, gout.cuda(), yact, xd, gw, gbias=gb)
+    torch.cuda.synchronize()
+    assert _rel(gx.cpu().numpy(), gx_ref) < REL
+    assert _rel(gw.cpu().numpy(), gw_ref) < REL
+    # the bias gradient sums the unrounded f32 gradient
+    gb_ref_f = (gout.numpy() * ((yb.float().cpu().numpy() > 0) if relu else 1)).sum(axis=(0, 1, 2))
+    assert _rel(gb.cpu().numpy(), gb_ref_f) < 1e-4
+
+
+def _init_params(of, seed=0):
+    """He-normal weights, zero biases; the last layer scaled down."""
+    from oflow import warmstart
+    return warmstart.init_params(seed)
+
+
+def test_network_trains(of):
+    import torch
+    from oflow import synth_gpu
+    net = of.WarmNet(128, 96, 4)
+    assert (net.out_w, net.out_h) == (16, 12)
+    net.set_params(_init_params(of, 1))
+    a, b, u, v, _ = synth_gpu.tvl1_pairs(4, 128, 96, seed=5, radius=20.0)
+    frames = torch.stack([a, b], dim=1).contiguous()
+    # target: ground truth averaged over 8x8 blocks, in 1/8-scale pixels
+    t = torch.stack([u, v], dim=1)
+    tgt = (torch.nn.functional.avg_pool2d(t, 8, ceil_mode=True) / 8).permute(0, 2, 3, 1).contiguous()
+    losses = [net.train_step(frames, tgt, 2e-3) for _ in range(60)]
+    assert np.isfinite(losses).all()
+    assert losses[-1] < 0.5 * losses[0]
+    pred = net.predict(frames)
+    assert pred.shape == (4, 12, 16, 2)
+    p = net.get_params()
+    net2 = of.WarmNet(128, 96, 4)
+    net2.set_params(p)
+    assert torch.equal(net2.predict(frames), pred)
+
+
+def test_warm_start_judge(of):
+    """With the plain solve as judge, every returned flow is either the warm
+    result (energy within 1%) or exactly the plain result."""
+    import torch
+    from oflow import synth
+    pairs = []
+    for s in range(2):
+        p = synth.tvl1_pair(seed=300 + s, w=256, h=128, radius=25.0)
+        pairs.append((synth.quantize(p.I0), synth.quantize(p.I1)))
+    net = of.WarmNet(256, 128, 2)
+    net.set_params(_init_params(of, 2))
+    warm = of.TVL1Params(nscales=5, warps=2, max_iterations=20)
+    plain = of.TVL1Params(nscales=5, max_iterations=50)
+    res, info = of.tvl1_warm(pairs, net, warm, plain)
+    for (a, b), (u, v), acc, ew, ep in zip(pairs, res, info["accepted"], info["energy_warm"],
+                                          info["energy_plain"]):
+        assert np.isfinite(ew) and np.isfinite(ep) and ep > 0
+        assert acc == (ew <= 1.01 * ep)
+        if not acc:
+            pu, pv = of.tvl1(a, b, plain)
+            assert np.array_equal(u, pu) and np.array_equal(v, pv)
