@@ -230,6 +230,51 @@ def reference_arm(args, rank):
 
 
 # ------------------------------------------------------------- our arm
+def warm_measure(oflow, synth, np, torch, pairs, d_in, prm, ctx, stream, args, P, world,
+                 max_over_ranks, barrier):
+    """Warm-started TV-L1 on the same pairs: the network's flow initialises
+    scale 3, then 2 warps x 20 inner iterations per scale.  Timed like the plain
+    form; quality from one judged call (plain solve as judge: energy within
+    1%) and EPE against ground truth for both forms."""
+    from oflow import warmstart
+    if not os.path.exists(warmstart.WEIGHTS):
+        return None
+    params, meta = warmstart.load()
+    net = oflow.WarmNet(W, H, P, ctx)
+    net.set_params(params)
+    wprm = oflow.TVL1Params(nscales=5, warps=args.warm_warps, max_iterations=args.warm_iters)
+    dev = d_in[0][0].device
+    w_out = [(torch.empty((H, W), dtype=torch.float32, device=dev),
+              torch.empty((H, W), dtype=torch.float32, device=dev)) for _ in range(P)]
+    for _ in range(args.warmup):
+        oflow.tvl1_warm(d_in, net, wprm, None, ctx, out=w_out)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        oflow.tvl1_warm(d_in, net, wprm, None, ctx, out=w_out)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    epe_w = [synth.epe(w_out[i][0].cpu().numpy(), w_out[i][1].cpu().numpy(), pairs[i][2].u,
+                       pairs[i][2].v, pairs[i][2].valid, 8) for i in range(P)]
+    # plain flows for the same pairs, and the judged call
+    p_out = oflow.tvl1_batch(d_in, prm, ctx)
+    epe_p = [synth.epe(p_out[i][0].cpu().numpy(), p_out[i][1].cpu().numpy(), pairs[i][2].u,
+                       pairs[i][2].v, pairs[i][2].valid, 8) for i in range(P)]
+    _, info = oflow.tvl1_warm(d_in, net, wprm, prm, ctx)
+    ratio = info["energy_warm"] / info["energy_plain"]
+    return {"value": world * P * args.steps / t, "unit": "pairs/s",
+            "schedule": f"network flow at scale 3, then {args.warm_warps} warps x "
+                        f"{args.warm_iters} iterations per scale",
+            "accepted_fraction": float(np.mean(info["accepted"])),
+            "energy_ratio_median": float(np.median(ratio)), "energy_ratio_max": float(ratio.max()),
+            "epe_warm": float(np.mean(epe_w)), "epe_plain": float(np.mean(epe_p)),
+            "epe_rel_diff": float((np.mean(epe_w) - np.mean(epe_p)) / np.mean(epe_p)),
+            "training": meta}
+
+
 def our_arm(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -324,6 +369,12 @@ def our_arm(args, rank, world, local_rank):
     t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3)
     assert np.array_equal(h_out[0][0], u0), "end-to-end result differs from the device run"
 
+    # --- learned warm start (scale 3 from the network, 2 warps x 20 iterations)
+    warm = None
+    if not args.no_warm:
+        warm = warm_measure(oflow, synth, np, torch, pairs, d_in, prm, ctx, stream, args, P,
+                            world, max_over_ranks, barrier)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.cpu_pairs, args.cpu_seconds)
@@ -367,6 +418,9 @@ def our_arm(args, rank, world, local_rank):
     }
     if cpu:
         line["cpu_baseline"] = cpu
+    if warm:
+        warm["speedup_vs_plain"] = warm["value"] / value
+        line["warm_start"] = warm
     print(json.dumps(line), flush=True)
     return 0
 
@@ -476,6 +530,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-warm", action="store_true", help="skip the warm-start measurement")
+    ap.add_argument("--warm-warps", type=int, default=2)
+    ap.add_argument("--warm-iters", type=int, default=20)
     ap.add_argument("--workload", choices=["tvl1", "batch"], default="tvl1",
                     help="tvl1: the 1024x436 TV-L1 workload (default); batch: the 256-pair "
                          "mixed HS/TV-L1 workload")

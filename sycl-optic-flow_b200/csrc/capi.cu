@@ -251,7 +251,9 @@ oflow_status oflow_ctx_create(int device, oflow_ctx **out) {
     if (!ctx) return OFLOW_ERR_OOM;
     ctx->device = device;
     const oflow_status s = guard(ctx, [&] {
-        OF_CUDA(cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking));
+        // a blocking stream: work a caller queued on the legacy default stream
+        // (e.g. torch's) is ordered before ours without extra events
+        OF_CUDA(cudaStreamCreateWithFlags(&ctx->own, cudaStreamDefault));
     });
     if (s != OFLOW_OK) {
         delete ctx;

@@ -280,13 +280,16 @@ __global__ void k_cnn_input(const T *frames, int w, int h, int N, size_t pair_st
         const int x = (int)(i % w2), y = (int)((i / w2) % h2), n = (int)(i / ((size_t)w2 * h2));
         const int xa = 2 * x, xb = imin(2 * x + 1, w - 1), ya = 2 * y, yb = imin(2 * y + 1, h - 1);
         __nv_bfloat16 *o = x0 + i * 16;
+        float m[2];
         for (int k = 0; k < 2; k++) {
             const T *f = frames + pair_stride * (2 * n + k);
             const float s = (float)f[(size_t)ya * w + xa] + (float)f[(size_t)ya * w + xb] +
                             (float)f[(size_t)yb * w + xa] + (float)f[(size_t)yb * w + xb];
-            o[k] = __float2bfloat16(s * (0.25f / 255.0f));
+            m[k] = s * (0.25f / 255.0f);
+            o[k] = __float2bfloat16(m[k] - 0.5f);
         }
-        for (int k = 2; k < 16; k++) o[k] = __float2bfloat16(0.0f);
+        o[2] = __float2bfloat16(4.0f * (m[1] - m[0]));
+        for (int k = 3; k < 16; k++) o[k] = __float2bfloat16(0.0f);
     }
 }
 

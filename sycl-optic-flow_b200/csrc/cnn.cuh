@@ -51,7 +51,8 @@ void upcat_forward(const __nv_bfloat16 *lo, int Hl, int Wl, int Ca, const __nv_b
 void upcat_backward(const float *g, int H, int W, int Ca, int Cb, int N, float *glo, int Hl,
                     int Wl, float *gskip, cudaStream_t st);
 // network input: 2x2 box of two frames (u8 or f32, dense w x h, pair stride),
-// /255, into channels 0 and 1 of a [N, ceil(h/2), ceil(w/2), 16] bf16 tensor
+// scaled to [0,1]: channel 0 = I0 - 0.5, 1 = I1 - 0.5, 2 = 4*(I1 - I0), the
+// rest 0, of a [N, ceil(h/2), ceil(w/2), 16] bf16 tensor
 void cnn_input(const void *frames, int dtype, int w, int h, int N, size_t pair_stride,
                __nv_bfloat16 *x0, cudaStream_t st);
 // Charbonnier loss between flow channels (0,1) of pred f32 [M,Kp] and target

@@ -4,7 +4,7 @@
 // 2 (so a 1024x436 pair enters at 512x218); output: flow at the size of TV-L1
 // scale 3 (128x55 for 1024x436), in that scale's pixel units.
 //
-//   x0  [h1,w1,16]   (channels 0,1: I0/255, I1/255)
+//   x0  [h1,w1,16]   (channels 0,1: I0/255 - 0.5, I1/255 - 0.5; 2: 4*(I1-I0)/255)
 //   c1  s2 16->32   c2 32->32   c3 s2 32->64   c4 64->64
 //   c5  s2 64->96   c6 96->96   c7 s2 96->128
 //   up(c7) ++ c6 -> c8 224->96;  up(c8) ++ c4 -> c9 160->64;  c10 64->8 (flow in 0,1)

@@ -22,14 +22,14 @@ import numpy as np
 # (input channels, output channels) per convolution, as in csrc/warmnet.cu
 LAYERS = [(16, 32), (32, 32), (32, 64), (64, 64), (64, 96), (96, 96), (96, 128), (224, 96),
           (160, 64), (64, 8)]
-# channels that carry signal in layer 0's input (I0, I1; the rest is padding)
-_FAN_IN0 = 2
+# channels that carry signal in layer 0's input (I0, I1, I1-I0; the rest is padding)
+_FAN_IN0 = 3
 WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "warmstart_weights.npz")
 W, H = 1024, 436
 
 
 def init_params(seed: int = 0) -> np.ndarray:
-    """He-normal weights (fan-in 9*C, layer 0 counts its 2 live channels),
+    """He-normal weights (fan-in 9*C, layer 0 counts its 3 live channels),
     zero biases, last layer scaled by 0.1."""
     rng = np.random.default_rng(seed)
     parts = []
@@ -62,6 +62,7 @@ def make_dataset(n: int, seed: int, ctx, chunk: int = 32, w: int = W, h: int = H
     import oflow
     from oflow import synth_gpu
     plain = oflow.TVL1Params(nscales=5, max_iterations=50)
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)  # order after torch's work
     frames = torch.empty((n, 2, h, w), dtype=torch.uint8, device="cuda")
     oh, ow = -(-h // 8), -(-w // 8)
     targets = torch.empty((n, oh, ow, 2), dtype=torch.float32, device="cuda")
@@ -86,6 +87,7 @@ def train(pairs: int, epochs: int, batch: int, lr: float, seed: int, out: str,
 
     import oflow
     ctx = oflow.Context(0)
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
     t0 = time.time()
     frames, targets = make_dataset(pairs, seed, ctx)
     log(f"dataset: {pairs} pairs labelled in {time.time() - t0:.1f} s")
