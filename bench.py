@@ -64,13 +64,16 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "k_tvl1_tb_1024x436.md")
+
+
 def ncu_traffic():
-    """DRAM bytes per inner-iteration launch from the committed ncu summary
-    (a line 'traffic_bytes_per_launch: N' in profiles/), or None."""
-    path = os.path.join(ROOT, "profiles", "tvl1_iter_1024x436.md")
+    """DRAM bytes per pair of one finest-scale inner-iteration launch, from the
+    committed ncu summary (a line 'traffic_bytes_per_pair_per_launch: N'), or
+    None."""
     try:
-        for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
+        for line in open(TRAFFIC_PROFILE):
+            if line.startswith("traffic_bytes_per_pair_per_launch:"):
                 return float(line.split(":")[1].split()[0])
     except OSError:
         pass
@@ -344,7 +347,7 @@ def our_arm(args, rank, world, local_rank):
     achieved = alg0 / (ms0 / 1e3) / 1e9 if ms0 > 0 else None
     traffic = ncu_traffic()
     if traffic is not None:
-        traffic *= P / 16.0  # the summary is per 16-pair launch; traffic scales with pairs
+        traffic *= P  # DRAM traffic of a launch grows with the pairs it processes
     launches_per_step = prof["launches"]
 
     # --- end to end through the public API: pinned host frames in, flow out
@@ -434,6 +437,14 @@ def once(args):
     d_in = [(torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)) for a, b, _ in pairs]
     prm = oflow.TVL1Params(nscales=args.nscales, max_iterations=args.iters)
     ctx = oflow.Context(0)
+    if args.tuning:
+        # the bench's tile choice without the autotuner's launches: tune and
+        # save when the table is missing, else load it
+        if os.path.exists(args.tuning):
+            ctx.load_tuning(args.tuning)
+        else:
+            oflow.tvl1_autotune(d_in, prm, ctx)
+            ctx.save_tuning(args.tuning)
     res, st = oflow.tvl1_batch(d_in, prm, ctx, stats=True)
     torch.cuda.synchronize()
     log("iterations per pair:", [int(s["iterations"].sum()) for s in st])
@@ -544,6 +555,8 @@ def main():
                     help="one solve of --batch device-resident pairs and exit (profiling case)")
     ap.add_argument("--nscales", type=int, default=PARAMS["nscales"])
     ap.add_argument("--iters", type=int, default=PARAMS["max_iterations"])
+    ap.add_argument("--tuning", default=None,
+                    help="with --once: tuning table to load (autotuned and saved if missing)")
     args = ap.parse_args()
     if args.cpu_worker:
         return cpu_worker(args)

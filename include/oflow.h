@@ -251,11 +251,13 @@ oflow_status oflow_net_predict(oflow_net *net, const void *frames, int dtype, fl
  * + lambda * sum |I1(x+u) - I0(x)|, bicubic warp with border zeroing) is at
  * most 1.01 times the plain solve's; otherwise the plain result is returned.
  * n must equal the network's batch and all frames its size.  energy_warm,
- * energy_plain and accepted (arrays of n) may be NULL. */
+ * energy_plain, accepted and stats (arrays of n; stats = the warm solve's
+ * iterations per (scale, warp), 0 for the scales above 3) may be NULL. */
 oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_image *I0,
                              const oflow_image *I1, const oflow_tvl1_params *warm,
                              const oflow_tvl1_params *plain, const oflow_flow *out,
-                             double *energy_warm, double *energy_plain, int *accepted);
+                             double *energy_warm, double *energy_plain, int *accepted,
+                             oflow_tvl1_stats *stats);
 
 /* One product of a 3x3 convolution (pad 1, stride 1 or 2) on device buffers,
  * for validating the network's kernels.  mode 0: y = conv(x, w) + bias (ReLU if

@@ -717,7 +717,8 @@ oflow_status oflow_net_predict(oflow_net *net, const void *frames, int dtype, fl
 oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_image *I0,
                              const oflow_image *I1, const oflow_tvl1_params *warm,
                              const oflow_tvl1_params *plain, const oflow_flow *out,
-                             double *energy_warm, double *energy_plain, int *accepted) {
+                             double *energy_warm, double *energy_plain, int *accepted,
+                             oflow_tvl1_stats *stats) {
     return guard(ctx, [&] {
         OF_CHECK(ctx != nullptr && net != nullptr && I0 && I1 && out, "tvl1 warm: null argument");
         OF_CHECK(n == net->net->batch(), "tvl1 warm: n must equal the network batch");
@@ -752,6 +753,8 @@ oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_
         std::vector<double> ew(n), ep(n, 0.0);
         std::vector<int> acc(n, 1);
         wp->true_energy(ew.data(), st);
+        if (stats)
+            for (int b = 0; b < n; b++) wp->read_stats(b, &stats[b], st);
         TvPlan *pp = nullptr;
         if (plain) {
             pp = &tv_plan(ctx, g.w, g.h, n, g.dtype, *plain, false);

@@ -1006,6 +1006,8 @@ TvPlan::TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, boo
     o_tout_ = ar_.reserve(sizeof(double) * B);
     ar_.commit();
     OF_CUDA(cudaMemset(ar_.at<char>(o_ctrl_), 0, B * sizeof(TvCtrl)));
+    // scales above a warm start's first scale never record a count
+    OF_CUDA(cudaMemset(ar_.at<char>(o_iters_), 0, (size_t)B * iter_stride_ * 4));
     tb_set_smem_attrs();
 }
 

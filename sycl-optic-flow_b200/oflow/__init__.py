@@ -411,7 +411,8 @@ class WarmNet:
 def tvl1_warm(pairs, net: WarmNet, warm: TVL1Params, plain: TVL1Params | None = None,
               ctx: Context | None = None, out=None):
     """Warm-started TV-L1 (oflow_tvl1_warm).  Returns (results, info) with
-    info = {energy_warm, energy_plain, accepted} arrays."""
+    info = {energy_warm, energy_plain, accepted} arrays and "stats", the warm
+    solve's per-pair iteration dicts."""
     n = len(pairs)
     I0 = (Image * n)()
     I1 = (Image * n)()
@@ -426,14 +427,16 @@ def tvl1_warm(pairs, net: WarmNet, warm: TVL1Params, plain: TVL1Params | None = 
     ew = np.zeros(n, np.float64)
     ep = np.zeros(n, np.float64)
     acc = np.zeros(n, np.int32)
+    st = (Tvl1Stats * n)()
     wp = warm.c()
     pp = plain.c() if plain is not None else None
     h = (ctx or net.ctx).handle
     _check(lib().oflow_tvl1_warm(h, net.handle, n, I0, I1, C.byref(wp),
                                  C.byref(pp) if pp is not None else None, O,
                                  ew.ctypes.data_as(C.c_void_p), ep.ctypes.data_as(C.c_void_p),
-                                 acc.ctypes.data_as(C.c_void_p)), h)
-    return res, {"energy_warm": ew, "energy_plain": ep, "accepted": acc.astype(bool)}
+                                 acc.ctypes.data_as(C.c_void_p), st), h)
+    return res, {"energy_warm": ew, "energy_plain": ep, "accepted": acc.astype(bool),
+                 "stats": [_stats_dict(s) for s in st]}
 
 
 def conv3x3(mode, N, H, W, C_, K, stride, relu, out_f32, a, y_act, b, out, bias=None, gbias=None):

@@ -108,7 +108,7 @@ SIGNATURES = {
     "oflow_net_predict": (_I, [_VP, _VP, _I, _VP]),
     "oflow_tvl1_warm": (_I, [_VP, _VP, _I, C.POINTER(Image), C.POINTER(Image),
                              C.POINTER(Tvl1Params), C.POINTER(Tvl1Params), C.POINTER(Flow),
-                             _VP, _VP, _VP]),
+                             _VP, _VP, _VP, C.POINTER(Tvl1Stats)]),
     "oflow_conv3x3": (_I, [_I, _I, _I, _I, _I, _I, _I, _I, _I, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "oflow_lk_default_params": (None, [C.POINTER(LkParams)]),
     "oflow_lk": (_I, [_VP, C.POINTER(Image), _I, C.POINTER(LkParams), C.POINTER(Flow)]),
