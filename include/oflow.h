@@ -261,9 +261,12 @@ oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_
 
 /* One product of a 3x3 convolution (pad 1, stride 1 or 2) on device buffers,
  * for validating the network's kernels.  mode 0: y = conv(x, w) + bias (ReLU if
- * relu; y f32 if out_f32 else bf16); mode 1: gin = conv^T(g) (f32; g masked by
- * y_act > 0 when y_act is non-NULL); mode 2: gw = dL/dw, gbias = dL/db (f32).
- * x, w, y_act: bf16; g: f32.  Shapes: x [N,H,W,C], w [K,3,3,C], y [N,P,Q,K]. */
+ * relu; y f32 if out_f32 else bf16) on the tcgen05 tensor-core kernel the
+ * network's forward pass uses (C % 16 == 0, K <= 128; OFLOW_ERR_TIMEOUT if one
+ * of its bounded waits gave up); mode 3: the same product on the mma.sync
+ * kernel; mode 1: gin = conv^T(g) (f32; g masked by y_act > 0 when y_act is
+ * non-NULL); mode 2: gw = dL/dw, gbias = dL/db (f32).  x, w, y_act: bf16;
+ * g: f32.  Shapes: x [N,H,W,C], w [K,3,3,C], y [N,P,Q,K]. */
 oflow_status oflow_conv3x3(int mode, int N, int H, int W, int C, int K, int stride, int relu,
                            int out_f32, const void *x_or_g, const void *y_act, const void *w_or_x,
                            void *out, const float *bias, float *gbias, void *stream);

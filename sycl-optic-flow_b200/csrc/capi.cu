@@ -710,7 +710,7 @@ oflow_status oflow_net_predict(oflow_net *net, const void *frames, int dtype, fl
         net->net->forward(frames, dtype, ps, st);
         net->net->flow_to(nullptr, 0, flow, st);
         OF_CUDA(cudaGetLastError());
-        OF_CUDA(cudaStreamSynchronize(st));
+        net->net->check_device_error(st);
     });
 }
 
@@ -774,7 +774,7 @@ oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_
             if (energy_plain) energy_plain[b] = ep[b];
             if (accepted) accepted[b] = acc[b];
         }
-        OF_CUDA(cudaStreamSynchronize(st));
+        net->net->check_device_error(st);
     });
 }
 
@@ -788,6 +788,20 @@ oflow_status oflow_conv3x3(int mode, int N, int H, int W, int C, int K, int stri
         const ConvDims d{N, H, W, C, conv_out(H, stride), conv_out(W, stride), K, stride};
         const cudaStream_t st = static_cast<cudaStream_t>(stream);
         if (mode == 0) {
+            // the tcgen05 kernel; the shape must be one it takes
+            OF_CHECK(bias != nullptr, "conv3x3: null bias");
+            DevBuf err(sizeof(int));
+            OF_CUDA(cudaMemsetAsync(err.as<int>(), 0, sizeof(int), st));
+            OF_CHECK(conv_forward_umma(d, static_cast<const __nv_bfloat16 *>(a),
+                                       static_cast<const __nv_bfloat16 *>(b), bias, out, out_f32 != 0,
+                                       relu != 0, err.as<int>(), st),
+                     "conv3x3: shape outside the tensor-core kernel (C % 16 == 0, K <= 128)");
+            int e = 0;
+            OF_CUDA(cudaMemcpyAsync(&e, err.as<int>(), sizeof(int), cudaMemcpyDeviceToHost, st));
+            OF_CUDA(cudaStreamSynchronize(st));
+            if (e) throw Error(OFLOW_ERR_TIMEOUT, "conv3x3: a bounded wait gave up");
+        } else if (mode == 3) {
+            // the mma.sync forward kernel (used by training's backward products)
             OF_CHECK(bias != nullptr, "conv3x3: null bias");
             conv_forward(d, static_cast<const __nv_bfloat16 *>(a), static_cast<const __nv_bfloat16 *>(b),
                          bias, out, out_f32 != 0, relu != 0, st);

@@ -178,7 +178,8 @@ __global__ void k_bias_grad(const float *g, const __nv_bfloat16 *y_act, int M, i
 }
 
 void conv_forward(const ConvDims &d, const __nv_bfloat16 *x, const __nv_bfloat16 *w,
-                  const float *bias, void *y, bool y_f32, bool relu, cudaStream_t st) {
+                  const float *bias, void *y, bool y_f32, bool relu, cudaStream_t st, int *err) {
+    if (err && conv_forward_umma(d, x, w, bias, y, y_f32, relu, err, st)) return;
     const int M = d.N * d.P * d.Q;
     dim3 g(div_up(M, kCBM), div_up(d.K, kCBN));
     k_conv_gemm<kConvFwd><<<g, kCNT, 0, st>>>(d, x, nullptr, w, y, bias,

@@ -31,9 +31,16 @@ struct ConvDims {
 inline int conv_out(int n, int stride) { return stride == 1 ? n : (n + 1) / 2; }
 
 // forward: x bf16 [N,H,W,C], w bf16 [K,3,3,C], bias f32 [K] -> y [N,P,Q,K]
-// (bf16, or f32 when y_f32); relu applies max(0, .).
+// (bf16, or f32 when y_f32); relu applies max(0, .).  With err (a device int)
+// the tcgen05 kernel runs where the shape allows (C % 16 == 0, K <= 128) and
+// sets *err if one of its bounded waits gave up; otherwise, and without err,
+// the mma.sync kernel runs.
 void conv_forward(const ConvDims &d, const __nv_bfloat16 *x, const __nv_bfloat16 *w,
-                  const float *bias, void *y, bool y_f32, bool relu, cudaStream_t st);
+                  const float *bias, void *y, bool y_f32, bool relu, cudaStream_t st,
+                  int *err = nullptr);
+// the tcgen05 form alone; false (nothing launched) when the shape is outside it
+bool conv_forward_umma(const ConvDims &d, const __nv_bfloat16 *x, const __nv_bfloat16 *w,
+                       const float *bias, void *y, bool y_f32, bool relu, int *err, cudaStream_t st);
 // backward-data: g f32 [N,P,Q,K] (masked by y_act > 0 when y_act != null,
 // y_act bf16 [N,P,Q,K]) -> gin f32 [N,H,W,C]; accumulate adds to gin.
 void conv_backward_data(const ConvDims &d, const float *g, const __nv_bfloat16 *y_act,

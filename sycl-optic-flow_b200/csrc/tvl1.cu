@@ -35,6 +35,7 @@ constexpr int kIterTW = 32, kIterTH = 8, kIterNT = 256;
 // configurations, largest first (tile TW x TH, threads); shared memory is
 // 36 B per region pixel (p 16, u 8, I1wx/I1wy 8, rho_c 4)
 constexpr int kTbK = 4;
+// Inner-iteration configurations of k_tvl1_tb: tile tw x th, nt threads.
 struct TbCfg {
     int tw, th, nt;
 };
@@ -641,6 +642,77 @@ __device__ __forceinline__ void tb_iteration(int j, float4 *sP, const float2 *sW
     __syncthreads();
 }
 
+// Per-iteration error sums of one block into its partial slots, then the
+// stopping decision by the last block of the pair to arrive: it finds the
+// first of the kk iterations meeting the stopping rule (tvl1.cpp:216).  If
+// that is the last one (or none does), the launch's state is accepted;
+// otherwise `redo` makes the next launch re-run exactly that many iterations
+// from the untouched input buffers.  Partials are summed in a fixed order, so
+// the decision does not depend on block scheduling.
+template <int K, int NT>
+__device__ __forceinline__ void tb_decide(const TbArgs &a, TvCtrl *ctrl, int b,
+                                          const double (&err)[K], int kk, int redo, int cur,
+                                          int n0) {
+    __shared__ double sred[NT / 32];
+    __shared__ double sE[K];
+    __shared__ int s_last;
+    const int ntiles = gridDim.x * gridDim.y;
+    const int tile = blockIdx.y * gridDim.x + blockIdx.x;
+    double *part = a.partials + (size_t)b * a.max_tiles * K;
+#pragma unroll
+    for (int j = 0; j < K; j++) {
+        if (j < kk) {  // kk is uniform over the block
+            const double s = block_sum_double<NT>(err[j], sred);
+            if (threadIdx.x == 0) part[(size_t)tile * K + j] = s;
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned prev = atomicAdd(&ctrl->arrive, 1u);
+        s_last = (prev == (unsigned)ntiles - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    for (int j = 0; j < kk; j++) {
+        double acc = 0.0;
+        for (int t = threadIdx.x; t < ntiles; t += NT) acc += __ldcg(part + (size_t)t * K + j);
+        const double tot = block_sum_double<NT>(acc, sred);
+        if (threadIdx.x == 0) sE[j] = tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const float npx = (float)(a.nx * a.ny);
+        if (redo > 0) {
+            ctrl->n = n0 + redo;
+            ctrl->cur = cur ^ 1;
+            ctrl->stop = 1;
+            ctrl->redo = 0;
+        } else {
+            int stopj = 0;
+            for (int j = 0; j < kk; j++) {
+                float e = (float)sE[j];
+                e = e / npx;
+                if (!(e > a.eps2) || n0 + j + 1 >= a.max_it) {
+                    stopj = j + 1;
+                    break;
+                }
+            }
+            if (stopj == 0 || stopj == kk) {
+                ctrl->n = n0 + kk;
+                ctrl->cur = cur ^ 1;
+                if (stopj) ctrl->stop = 1;
+            } else {
+                ctrl->redo = stopj;
+            }
+        }
+        a.iters[(size_t)b * a.iter_stride + a.stage] = ctrl->n;
+        ctrl->arrive = 0;
+        __threadfence();
+    }
+}
+
 template <int TW, int TH, int K, int NT>
 __global__ void __launch_bounds__(NT) k_tvl1_tb(TbArgs a) {
     constexpr int RW = TW + 2 * K, RH = TH + 2 * K, RN = RW * RH;
@@ -649,9 +721,6 @@ __global__ void __launch_bounds__(NT) k_tvl1_tb(TbArgs a) {
     float2 *sU = reinterpret_cast<float2 *>(sP + RN);      // RN
     float2 *sW = sU + RN;                                  // RN
     float *sR = reinterpret_cast<float *>(sW + RN);        // RN
-    __shared__ double sred[NT / 32];
-    __shared__ double sE[K];
-    __shared__ int s_last;
 
     const int b = blockIdx.z;
     TvCtrl *ctrl = a.ctrl + b;
@@ -714,62 +783,7 @@ __global__ void __launch_bounds__(NT) k_tvl1_tb(TbArgs a) {
         Pout[q] = sP[r];
     }
 
-    // ---- per-iteration error sums and the stopping decision
-    const int ntiles = gridDim.x * gridDim.y;
-    const int tile = blockIdx.y * gridDim.x + blockIdx.x;
-    double *part = a.partials + (size_t)b * a.max_tiles * K;
-#pragma unroll
-    for (int j = 0; j < K; j++) {
-        if (j < kk) {  // kk is uniform over the block
-            const double s = block_sum_double<NT>(err[j], sred);
-            if (threadIdx.x == 0) part[(size_t)tile * K + j] = s;
-            __syncthreads();
-        }
-    }
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const unsigned prev = atomicAdd(&ctrl->arrive, 1u);
-        s_last = (prev == (unsigned)ntiles - 1);
-    }
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    for (int j = 0; j < kk; j++) {
-        double acc = 0.0;
-        for (int t = threadIdx.x; t < ntiles; t += NT) acc += __ldcg(part + (size_t)t * K + j);
-        const double tot = block_sum_double<NT>(acc, sred);
-        if (threadIdx.x == 0) sE[j] = tot;
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        const float npx = (float)(nx * ny);
-        if (redo > 0) {
-            ctrl->n = n0 + redo;
-            ctrl->cur = cur ^ 1;
-            ctrl->stop = 1;
-            ctrl->redo = 0;
-        } else {
-            int stopj = 0;
-            for (int j = 0; j < kk; j++) {
-                float e = (float)sE[j];
-                e = e / npx;
-                if (!(e > a.eps2) || n0 + j + 1 >= a.max_it) {
-                    stopj = j + 1;
-                    break;
-                }
-            }
-            if (stopj == 0 || stopj == kk) {
-                ctrl->n = n0 + kk;
-                ctrl->cur = cur ^ 1;
-                if (stopj) ctrl->stop = 1;
-            } else {
-                ctrl->redo = stopj;
-            }
-        }
-        a.iters[(size_t)b * a.iter_stride + a.stage] = ctrl->n;
-        ctrl->arrive = 0;
-        __threadfence();
-    }
+    tb_decide<K, NT>(a, ctrl, b, err, kk, redo, cur, n0);
 }
 
 // ---------------------------------------------------------------- energy

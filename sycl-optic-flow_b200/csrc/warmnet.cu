@@ -74,7 +74,9 @@ WarmNet::WarmNet(int w, int h, int B) : w_(w), h_(h), B_(B) {
     o_m_ = ar_.reserve(np_ * 4);
     o_v_ = ar_.reserve(np_ * 4);
     o_loss_ = ar_.reserve(8);
+    o_err_ = ar_.reserve(sizeof(int));
     ar_.commit();
+    OF_CUDA(cudaMemset(ar_.at<char>(o_err_), 0, sizeof(int)));
     OF_CUDA(cudaMemset(ar_.at<char>(o_m_), 0, np_ * 4));
     OF_CUDA(cudaMemset(ar_.at<char>(o_v_), 0, np_ * 4));
     OF_CUDA(cudaMemset(ar_.at<char>(o_p_), 0, np_ * 4));
@@ -119,9 +121,11 @@ void WarmNet::forward(const void *frames, int dtype, size_t pair_stride, cudaStr
             upcat_forward(A(9), hs_[4], ws_[4], 96, A(4), hs_[3], ws_[3], 64, B_, A(10), st);
         const ConvDims d = dims(l);
         if (l < 9)
-            conv_forward(d, A(src[l]), W + woff_[l], P + boff_[l], A(dst[l]), false, kLayers[l].relu, st);
+            conv_forward(d, A(src[l]), W + woff_[l], P + boff_[l], A(dst[l]), false, kLayers[l].relu, st,
+                         ar_.at<int>(o_err_));
         else
-            conv_forward(d, A(src[l]), W + woff_[l], P + boff_[l], ar_.at<float>(o_out_), true, false, st);
+            conv_forward(d, A(src[l]), W + woff_[l], P + boff_[l], ar_.at<float>(o_out_), true, false,
+                         st, ar_.at<int>(o_err_));
     }
 }
 
@@ -162,7 +166,18 @@ double WarmNet::train_step(const void *frames, int dtype, size_t pair_stride, co
     double loss = 0.0;
     OF_CUDA(cudaMemcpyAsync(&loss, ar_.at<double>(o_loss_), 8, cudaMemcpyDeviceToHost, st));
     OF_CUDA(cudaStreamSynchronize(st));
+    check_device_error(st);
     return loss;
+}
+
+void WarmNet::check_device_error(cudaStream_t st) {
+    int e = 0;
+    OF_CUDA(cudaMemcpyAsync(&e, ar_.at<int>(o_err_), sizeof(int), cudaMemcpyDeviceToHost, st));
+    OF_CUDA(cudaStreamSynchronize(st));
+    if (e) {
+        OF_CUDA(cudaMemsetAsync(ar_.at<int>(o_err_), 0, sizeof(int), st));
+        throw Error(OFLOW_ERR_TIMEOUT, "net: a tensor-core convolution gave up a bounded wait");
+    }
 }
 
 __global__ void k_flow_out(const float *out, int M, float2 *dst2, size_t stride, int pix_per_b,

@@ -31,6 +31,9 @@ class WarmNet {
     // last forward's flow into dst[b*stride + p] (float2) and/or planar
     // [B][out_h][out_w][2] floats
     void flow_to(float2 *dst, size_t stride, float *planar, cudaStream_t st) const;
+    // throws OFLOW_ERR_TIMEOUT if a tensor-core convolution gave up a bounded
+    // wait since the last check (synchronises st), and clears the flag
+    void check_device_error(cudaStream_t st);
 
   private:
     ConvDims dims(int l) const;
@@ -41,7 +44,7 @@ class WarmNet {
     Arena ar_;
     size_t aoff_[12] = {}, goff_[12] = {}, gsize_[12] = {};
     size_t o_out_ = 0, o_gout_ = 0, o_p_ = 0, o_pb_ = 0, o_gp_ = 0, o_m_ = 0, o_v_ = 0,
-           o_loss_ = 0;
+           o_loss_ = 0, o_err_ = 0;
     int step_ = 0;
 };
 

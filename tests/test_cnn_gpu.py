@@ -21,8 +21,13 @@ def _rel(a, b):
 
 
 @pytest.mark.parametrize("N,H,W,C,K,stride,relu", [(2, 9, 13, 16, 32, 1, True), (1, 12, 10, 32, 8, 2, False),
-                                                   (2, 7, 11, 48, 64, 2, True), (1, 16, 16, 160, 64, 1, True)])
+                                                   (2, 7, 11, 48, 64, 2, True), (1, 16, 16, 160, 64, 1, True),
+                                                   (2, 13, 17, 224, 96, 1, True), (1, 11, 9, 96, 128, 2, True),
+                                                   (3, 20, 30, 16, 32, 2, True)])
 def test_conv_products_match_cpu_oracle(of, N, H, W, C, K, stride, relu):
+    """Forward on both tensor-core kernels (mode 0: tcgen05 with the
+    accumulator in tensor memory; mode 3: mma.sync), backward-data and
+    backward-weight, against the float64 oracle."""
     import torch
     from oracle import cnn_ref
     g = torch.Generator().manual_seed(N * 1000 + C + K)
@@ -31,15 +36,16 @@ def test_conv_products_match_cpu_oracle(of, N, H, W, C, K, stride, relu):
     w = _bf16(torch.randn((K, 3, 3, C), generator=g) * 0.1)
     b = torch.randn(K, generator=g) * 0.1
     xd, wd, bd = x.cuda(), w.cuda(), b.cuda()
-    # forward, f32 output
-    y = torch.empty((N, P, Q, K), dtype=torch.float32, device="cuda")
-    of.conv3x3(0, N, H, W, C, K, stride, relu, True, xd, None, wd, y, bias=bd)
     ref = cnn_ref.forward(x.float().numpy(), w.float().numpy(), b.numpy(), stride, relu)
-    assert _rel(y.cpu().numpy(), ref) < REL
-    # forward, bf16 output (what the network stores)
-    yb = torch.empty((N, P, Q, K), dtype=torch.bfloat16, device="cuda")
-    of.conv3x3(0, N, H, W, C, K, stride, relu, False, xd, None, wd, yb, bias=bd)
-    assert _rel(yb.float().cpu().numpy(), ref) < 1e-2
+    for mode in (0, 3):
+        # forward, f32 output
+        y = torch.full((N, P, Q, K), float("nan"), dtype=torch.float32, device="cuda")
+        of.conv3x3(mode, N, H, W, C, K, stride, relu, True, xd, None, wd, y, bias=bd)
+        assert _rel(y.cpu().numpy(), ref) < REL, mode
+        # forward, bf16 output (what the network stores)
+        yb = torch.full((N, P, Q, K), float("nan"), dtype=torch.bfloat16, device="cuda")
+        of.conv3x3(mode, N, H, W, C, K, stride, relu, False, xd, None, wd, yb, bias=bd)
+        assert _rel(yb.float().cpu().numpy(), ref) < 1e-2, mode
     # backward: gradients of sum(gout * y); gout is rounded to bf16 by the
     # kernels, so the oracle gets the same rounded values
     gout = torch.randn((N, P, Q, K), generator=g)
