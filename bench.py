@@ -378,6 +378,32 @@ def our_arm(args, rank, world, local_rank):
         warm = warm_measure(oflow, synth, np, torch, pairs, d_in, prm, ctx, stream, args, P,
                             world, max_over_ranks, barrier)
 
+    # --- flowToColor of the step's flows (device in, device out); the argument
+    # arrays are built once so that the loop times the C call and the kernel
+    import ctypes
+    from oflow.capi import BgrImage, Flow, lib as oflow_lib
+    imgs = [torch.empty((H, W, 3), dtype=torch.uint8, device=dev) for _ in range(P)]
+    first = oflow.flow_to_color_batch(d_out, ctx, out=imgs)
+    fl = (Flow * P)(*[Flow(ctypes.cast(ctypes.c_void_p(u.data_ptr()), ctypes.POINTER(ctypes.c_float)),
+                           ctypes.cast(ctypes.c_void_p(v.data_ptr()), ctypes.POINTER(ctypes.c_float)),
+                           W, 1) for u, v in d_out])
+    im = (BgrImage * P)(*[BgrImage(t.data_ptr(), 3 * W, 1) for t in imgs])
+    for _ in range(3):
+        oflow_lib().oflow_flow_to_color(ctx.handle, P, W, H, fl, im)
+    torch.cuda.synchronize()
+    reps = 50
+    e0.record(stream)
+    for _ in range(reps):
+        oflow_lib().oflow_flow_to_color(ctx.handle, P, W, H, fl, im)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_col = e0.elapsed_time(e1) / 1e3 / reps
+    col_gbs = P * W * H * 11 / t_col / 1e9
+    assert first[0].shape == (H, W, 3)
+    color = {"flows_per_s": P / t_col, "ms_per_batch": 1e3 * t_col, "achieved_gbs": col_gbs,
+             "frac": col_gbs / measured_peak()[0],
+             "bytes_basis": "8 B in (u, v) + 3 B out (B, G, R) per pixel", "batch": P}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.cpu_pairs, args.cpu_seconds)
@@ -424,6 +450,7 @@ def our_arm(args, rank, world, local_rank):
     if warm:
         warm["speedup_vs_plain"] = warm["value"] / value
         line["warm_start"] = warm
+    line["flow_to_color"] = color
     print(json.dumps(line), flush=True)
     return 0
 

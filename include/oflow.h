@@ -259,6 +259,25 @@ oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_
                              double *energy_warm, double *energy_plain, int *accepted,
                              oflow_tvl1_stats *stats);
 
+/* ------------------------------------------------------------ visualisation */
+/* An 8-bit, 3-channel image (bytes B, G, R per pixel), caller-owned.  pitch in
+ * bytes (0 means 3 * width). */
+typedef struct {
+    uint8_t *data;
+    int pitch;
+    int location; /* oflow_location */
+} oflow_bgr_image;
+
+/* The demos' flowToColor (App::flowToColor, src/tvl1/sequential/main.cpp:
+ * 93-126) for n flows of width x height: V = 8-bit min(10 |(u,v)|, 255),
+ * H = 8-bit atan2(v, u) in degrees / 2 (negative angles saturate to 0),
+ * S = 255, converted HSV -> B, G, R (hexcone, H in 0..180) into out[i] instead
+ * of an OpenCV window.  Flows and images may each be host or device buffers;
+ * the call is synchronous unless a stream was set and everything is on the
+ * device. */
+oflow_status oflow_flow_to_color(oflow_ctx *ctx, int n, int width, int height,
+                                 const oflow_flow *flows, const oflow_bgr_image *out);
+
 /* One product of a 3x3 convolution (pad 1, stride 1 or 2) on device buffers,
  * for validating the network's kernels.  mode 0: y = conv(x, w) + bias (ReLU if
  * relu; y f32 if out_f32 else bf16) on the tcgen05 tensor-core kernel the

@@ -162,4 +162,17 @@ class LucasKanade {
     oflow_ctx *ctx_ = nullptr;
 };
 
+// ------------------------------------------------------------------ visualisation
+// App::flowToColor (src/tvl1/sequential/main.cpp:93) with the cv::Mat output
+// replaced by a caller buffer of width * height * 3 bytes (B, G, R).  flowData
+// is the planar [u | v] layout of TV_L1::getU().
+inline void flowToColor(int width, int height, const float *flowData, unsigned char *outBGR) {
+    oflow_ctx *&ctx = oflow::compat_global_ctx();
+    if (!ctx) oflow::compat_check(oflow_ctx_create(0, &ctx), nullptr);
+    const oflow_flow f{const_cast<float *>(flowData), const_cast<float *>(flowData) + (size_t)width * height,
+                       0, OFLOW_HOST};
+    const oflow_bgr_image o{outBGR, 0, OFLOW_HOST};
+    oflow::compat_check(oflow_flow_to_color(ctx, 1, width, height, &f, &o), ctx);
+}
+
 #endif  // OFLOW_COMPAT_HPP

@@ -116,6 +116,8 @@ def orc_lib():
         lib.orc_lk_f32.argtypes = [_f32p, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, _f32p, _f32p]
         lib.orc_lk_f32.restype = C.c_int
         lib.orc_bilinear_warp.argtypes = [_f32p, _f32p, _f32p, C.c_int, C.c_int, _f32p]
+        lib.orc_flow_to_color.argtypes = [_f32p, _f32p, C.c_int, C.c_int, C.c_void_p]
+        lib.orc_flow_to_color.restype = None
         lib.orc_pyrlk.argtypes = [_f32p, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                   C.c_int, _f32p, _f32p]
         lib.orc_pyrlk.restype = C.c_int
@@ -274,3 +276,13 @@ def ref_tvl1(I0_u8, I1_u8, params: TVL1Params | None = None):
     if rc < 0:
         raise ValueError("reference tvl1: image too small for the pyramid")
     return u, v
+
+
+def flow_to_color(u, v):
+    """BGR bytes [h, w, 3] of a flow by orc_flow_to_color."""
+    u = _f32(u)
+    v = _f32(v)
+    h, w = u.shape
+    out = np.zeros((h, w, 3), np.uint8)
+    orc_lib().orc_flow_to_color(u, v, w, h, out.ctypes.data_as(C.c_void_p))
+    return out

@@ -837,3 +837,60 @@ int orc_pyrlk(const float *I0, const float *I1, int w, int h, int levels, int it
     for (int l = 0; l < levels; l++) { free(P0[l]); free(P1[l]); }
     return rc;
 }
+
+
+/* ===================================================================== flowToColor */
+/* main.cpp:93-126.  The reference computes |f| and atan2 in float, scales with
+ * OpenCV Mat expressions and converts to 8 bits with saturate_cast (round to
+ * nearest even, clamp to 0..255), then converts HSV to BGR with cvtColor.
+ * OpenCV is not part of the reference tree; its HSV->BGR conversion is the
+ * hexcone model (Smith 1978) with H stored as degrees/2 and S, V scaled to
+ * 0..255, restated here in single precision:
+ *   h' = H * (6/180), sector = floor(h'), f = h' - sector, s = S/255, v = V/255
+ *   p = v(1-s), q = v(1-s f), t = v(1-s(1-f))
+ *   (R,G,B) = (v,t,p) (q,v,p) (p,v,t) (p,q,v) (t,p,v) (v,p,q) for sectors 0..5
+ *   byte = saturate(255 x).
+ * atan2 is taken in double and rounded to float, which equals a correctly
+ * rounded atan2f. */
+static uint8_t sat_u8(float x) {
+    if (!(x == x)) return 0;
+    const float r = rintf(x);
+    if (r <= 0.0f) return 0;
+    if (r >= 255.0f) return 255;
+    return (uint8_t)r;
+}
+
+void orc_flow_to_color(const float *u, const float *v, int w, int h, uint8_t *bgr) {
+    const float hue_scale = (float)(180.0 / 3.14159265358979323846 / 2.0);
+    for (size_t i = 0; i < (size_t)w * h; i++) {
+        const float fu = u[i], fv = v[i];
+        const float mag = sqrtf(fu * fu + fv * fv);
+        float m = mag * 10.0f;
+        if (m > 255.0f) m = 255.0f;
+        const uint8_t V = sat_u8(m);
+        const float ang = (float)atan2((double)fv, (double)fu);
+        const uint8_t H = sat_u8(ang * hue_scale);
+        const float hh = (float)H * (6.0f / 180.0f);
+        int sector = (int)floorf(hh);
+        float f = hh - (float)sector;
+        if (sector < 0 || sector > 5) {
+            sector = 0;
+            f = 0.0f;
+        }
+        const float s = 255.0f * (1.0f / 255.0f);
+        const float vv = (float)V * (1.0f / 255.0f);
+        const float p = vv * (1.0f - s), q = vv * (1.0f - s * f), t = vv * (1.0f - s * (1.0f - f));
+        float r, g, b;
+        switch (sector) {
+            case 0: r = vv; g = t; b = p; break;
+            case 1: r = q; g = vv; b = p; break;
+            case 2: r = p; g = vv; b = t; break;
+            case 3: r = p; g = q; b = vv; break;
+            case 4: r = t; g = p; b = vv; break;
+            default: r = vv; g = p; b = q; break;
+        }
+        bgr[3 * i + 0] = sat_u8(b * 255.0f);
+        bgr[3 * i + 1] = sat_u8(g * 255.0f);
+        bgr[3 * i + 2] = sat_u8(r * 255.0f);
+    }
+}

@@ -102,6 +102,13 @@ void orc_bilinear_warp(const float *src, const float *u, const float *v, int w, 
 int orc_pyrlk(const float *I0, const float *I1, int w, int h, int levels, int iters,
               int spac_size, int window, float *u, float *v);
 
+/* ---------------- flow visualisation ---------------- */
+/* flowToColor (src/tvl1/sequential/main.cpp:93-126): per pixel V = 8-bit
+ * min(10|f|, 255), H = 8-bit (atan2(v,u) in degrees)/2 (negative angles
+ * saturate to 0), S = 255, then HSV (H in 0..180) -> B, G, R bytes by the
+ * hexcone formulas.  u, v planar w x h floats; bgr w*h*3 bytes. */
+void orc_flow_to_color(const float *u, const float *v, int w, int h, uint8_t *bgr);
+
 #ifdef __cplusplus
 }
 #endif

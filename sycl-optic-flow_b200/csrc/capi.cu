@@ -14,6 +14,7 @@
 #include <tuple>
 #include <vector>
 
+#include "color.hpp"
 #include "hs.hpp"
 #include "internal.hpp"
 #include "lk.hpp"
@@ -92,6 +93,7 @@ struct oflow_ctx {
     TuneTable tune;  // autotuned kernel configurations, consulted by new plans
     std::vector<std::unique_ptr<TvPlan>> tv_warm;  // plans that start at scale 3
     std::vector<std::unique_ptr<MixedBatch>> mixed;
+    DevBuf color_scratch;  // host-side flows / images of oflow_flow_to_color
     cudaStream_t stream() const { return user ? user : own; }
 };
 
@@ -775,6 +777,84 @@ oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_
             if (accepted) accepted[b] = acc[b];
         }
         net->net->check_device_error(st);
+    });
+}
+
+oflow_status oflow_flow_to_color(oflow_ctx *ctx, int n, int width, int height,
+                                 const oflow_flow *flows, const oflow_bgr_image *out) {
+    return guard(ctx, [&] {
+        OF_CHECK(ctx != nullptr && n >= 0 && (n == 0 || (flows && out)), "flow_to_color: null argument");
+        OF_CHECK(width > 0 && height > 0, "flow_to_color: empty image");
+        for (int i = 0; i < n; i++) {
+            check_flow(&flows[i], width);
+            OF_CHECK(out[i].data != nullptr, "flow_to_color: null output");
+            OF_CHECK(out[i].location == OFLOW_HOST || out[i].location == OFLOW_DEVICE,
+                     "flow_to_color: bad output location");
+            OF_CHECK(out[i].pitch == 0 || out[i].pitch >= 3 * width, "flow_to_color: pitch < 3 * width");
+        }
+        const cudaStream_t st = ctx->stream();
+        const size_t plane = (size_t)width * height * 4, img = (size_t)width * height * 3;
+        bool host_side = false;
+        for (int s0 = 0; s0 < n; s0 += kColorMaxJobs) {
+            const int k = std::min(kColorMaxJobs, n - s0);
+            // scratch: staged u, v planes and images for host-side jobs of this chunk
+            size_t need = 0;
+            for (int i = 0; i < k; i++) {
+                if (flows[s0 + i].location == OFLOW_HOST) need += 2 * ((plane + 255) & ~size_t(255));
+                if (out[s0 + i].location == OFLOW_HOST) need += (img + 255) & ~size_t(255);
+            }
+            if (need > ctx->color_scratch.bytes()) {
+                OF_CUDA(cudaStreamSynchronize(st));  // earlier chunks may still use it
+                ctx->color_scratch.alloc(need);
+            }
+            char *sp = ctx->color_scratch.as<char>();
+            ColorJobs jobs{};
+            jobs.w = width;
+            jobs.h = height;
+            for (int i = 0; i < k; i++) {
+                const oflow_flow &f = flows[s0 + i];
+                const oflow_bgr_image &o = out[s0 + i];
+                ColorJob &j = jobs.j[i];
+                if (f.location == OFLOW_HOST) {
+                    float *du = reinterpret_cast<float *>(sp);
+                    sp += (plane + 255) & ~size_t(255);
+                    float *dv = reinterpret_cast<float *>(sp);
+                    sp += (plane + 255) & ~size_t(255);
+                    const size_t fp = (size_t)(f.pitch ? f.pitch : width) * 4;
+                    OF_CUDA(cudaMemcpy2DAsync(du, (size_t)width * 4, f.u, fp, (size_t)width * 4, height,
+                                              cudaMemcpyHostToDevice, st));
+                    OF_CUDA(cudaMemcpy2DAsync(dv, (size_t)width * 4, f.v, fp, (size_t)width * 4, height,
+                                              cudaMemcpyHostToDevice, st));
+                    j.u = du;
+                    j.v = dv;
+                    j.fpitch = width;
+                    host_side = true;
+                } else {
+                    j.u = f.u;
+                    j.v = f.v;
+                    j.fpitch = f.pitch ? f.pitch : width;
+                }
+                if (o.location == OFLOW_HOST) {
+                    j.bgr = reinterpret_cast<uint8_t *>(sp);
+                    sp += (img + 255) & ~size_t(255);
+                    j.bpitch = 3 * width;
+                    host_side = true;
+                } else {
+                    j.bgr = o.data;
+                    j.bpitch = o.pitch ? o.pitch : 3 * width;
+                }
+            }
+            launch_flow_to_color(jobs, k, st);
+            OF_CUDA(cudaGetLastError());
+            for (int i = 0; i < k; i++) {
+                const oflow_bgr_image &o = out[s0 + i];
+                if (o.location != OFLOW_HOST) continue;
+                OF_CUDA(cudaMemcpy2DAsync(o.data, o.pitch ? o.pitch : 3 * width, jobs.j[i].bgr,
+                                          (size_t)3 * width, (size_t)3 * width, height,
+                                          cudaMemcpyDeviceToHost, st));
+            }
+        }
+        if (host_side || !ctx->user) OF_CUDA(cudaStreamSynchronize(st));
     });
 }
 

@@ -22,13 +22,14 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .capi import (LIB_PATH, SOLVER_HS, SOLVER_TVL1, Flow, HsParams, Image, Job, LkParams,
+from .capi import (LIB_PATH, SOLVER_HS, SOLVER_TVL1, BgrImage, Flow, HsParams, Image, Job, LkParams,
                    OflowError, Tvl1Params, Tvl1Profile, Tvl1Stats, lib, status_string)
 
 __all__ = [
     "Context", "OflowError", "TVL1Params", "HSParams", "LKParams", "tvl1", "tvl1_batch",
     "tvl1_energy_trace", "hs", "hs_batch", "lk", "pyrlk", "TV_L1", "initFlow", "ComputeFlow",
-    "deleteFlow_mem", "LucasKanade", "nscales", "LIB_PATH",
+    "deleteFlow_mem", "LucasKanade", "nscales", "LIB_PATH", "flow_to_color", "flow_to_color_batch",
+    "save_ppm",
 ]
 
 
@@ -475,6 +476,67 @@ def pyrlk(I0, I1, params: LKParams | None = None, ctx: Context | None = None, ou
     h = _ctx(ctx)
     _check(lib().oflow_pyrlk(h, C.byref(a), C.byref(b), C.byref(p), C.byref(f)), h)
     return uv
+
+
+# ------------------------------------------------------------ visualisation
+def flow_to_color_batch(flows, ctx: Context | None = None, out=None):
+    """oflow_flow_to_color on a list of (u, v) flows of one size: returns B, G, R
+    images [h, w, 3] uint8 (torch CUDA tensors for CUDA flows, numpy otherwise)."""
+    n = len(flows)
+    if n == 0:
+        return []
+    F = (Flow * n)()
+    O = (BgrImage * n)()
+    keep, res = [], []
+    h, w = flows[0][0].shape
+    for i, (u, v) in enumerate(flows):
+        if tuple(u.shape) != (h, w) or tuple(v.shape) != (h, w):
+            raise ValueError("flow_to_color: flows must share one size")
+        if _is_torch(u):
+            if u.dtype != v.dtype or str(u.dtype) != "torch.float32":
+                raise ValueError("flow_to_color: float32 flows")
+            u, v = u.contiguous(), v.contiguous()
+            keep += [u, v]
+            F[i] = Flow(C.cast(C.c_void_p(u.data_ptr()), C.POINTER(C.c_float)),
+                        C.cast(C.c_void_p(v.data_ptr()), C.POINTER(C.c_float)), w,
+                        1 if u.is_cuda else 0)
+            dev = u.is_cuda
+        else:
+            u = np.ascontiguousarray(u, np.float32)
+            v = np.ascontiguousarray(v, np.float32)
+            keep += [u, v]
+            F[i] = Flow(u.ctypes.data_as(C.POINTER(C.c_float)), v.ctypes.data_as(C.POINTER(C.c_float)),
+                        w, 0)
+            dev = False
+        if out is not None:
+            img = out[i]
+        elif dev:
+            import torch
+            img = torch.empty((h, w, 3), dtype=torch.uint8, device=u.device)
+        else:
+            img = np.empty((h, w, 3), np.uint8)
+        if _is_torch(img):
+            O[i] = BgrImage(img.data_ptr(), img.stride(0), 1 if img.is_cuda else 0)
+        else:
+            O[i] = BgrImage(img.ctypes.data, img.strides[0], 0)
+        res.append(img)
+    hd = _ctx(ctx)
+    _check(lib().oflow_flow_to_color(hd, n, w, h, F, O), hd)
+    return res
+
+
+def flow_to_color(u, v, ctx: Context | None = None, out=None):
+    """B, G, R image [h, w, 3] uint8 of one flow (the demos' flowToColor)."""
+    return flow_to_color_batch([(u, v)], ctx, None if out is None else [out])[0]
+
+
+def save_ppm(path: str, bgr) -> None:
+    """Write a B, G, R byte image [h, w, 3] as a binary PPM (RGB) file."""
+    a = bgr.cpu().numpy() if _is_torch(bgr) else np.asarray(bgr)
+    h, w, _ = a.shape
+    with open(path, "wb") as f:
+        f.write(b"P6\n%d %d\n255\n" % (w, h))
+        f.write(np.ascontiguousarray(a[:, :, ::-1]).tobytes())
 
 
 from .compat import TV_L1, ComputeFlow, LucasKanade, deleteFlow_mem, initFlow  # noqa: E402

@@ -31,6 +31,10 @@ class Flow(C.Structure):
                 ("pitch", C.c_int), ("location", C.c_int)]
 
 
+class BgrImage(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("pitch", C.c_int), ("location", C.c_int)]
+
+
 class Tvl1Params(C.Structure):
     _fields_ = [("tau", C.c_float), ("lambda_", C.c_float), ("theta", C.c_float),
                 ("nscales", C.c_int), ("zfactor", C.c_float), ("warps", C.c_int),
@@ -109,6 +113,7 @@ SIGNATURES = {
     "oflow_tvl1_warm": (_I, [_VP, _VP, _I, C.POINTER(Image), C.POINTER(Image),
                              C.POINTER(Tvl1Params), C.POINTER(Tvl1Params), C.POINTER(Flow),
                              _VP, _VP, _VP, C.POINTER(Tvl1Stats)]),
+    "oflow_flow_to_color": (_I, [_VP, _I, _I, _I, C.POINTER(Flow), C.POINTER(BgrImage)]),
     "oflow_conv3x3": (_I, [_I, _I, _I, _I, _I, _I, _I, _I, _I, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "oflow_lk_default_params": (None, [C.POINTER(LkParams)]),
     "oflow_lk": (_I, [_VP, C.POINTER(Image), _I, C.POINTER(LkParams), C.POINTER(Flow)]),

@@ -209,3 +209,18 @@ def test_lk_oracle_ring_order_and_borders(orc):
     assert np.array_equal(u1, u2) and np.array_equal(v1, v2)
     assert np.all(u1[:2] == 0) and np.all(u1[:, :2] == 0) and np.all(u1[-2:] == 0)
     assert float(np.median(u1[5:-5, 5:-5])) > 0.5
+
+
+def test_flow_to_color_known_answers(orc):
+    """flowToColor restatement (main.cpp:93-126): V = round(10|f|) capped at
+    255, H = round(deg/2) with negative angles at 0, S = 255, hexcone BGR."""
+    u = np.array([[1, 0, 0, -1, 3, 30, 0]], np.float32)
+    v = np.array([[0, 1, -1, 0, 3, 0, 0]], np.float32)
+    got = orc.flow_to_color(u, v)[0].tolist()
+    assert got == [[0, 0, 10],      # 0 deg: red
+                   [0, 10, 5],      # 90 deg: H 45, sector 1
+                   [0, 0, 10],      # -90 deg saturates to H 0
+                   [10, 10, 0],     # 180 deg: H 90, sector 3
+                   [0, 31, 42],     # 45 deg: H 22 (22.5 rounds to even), |f| 4.24
+                   [0, 0, 255],     # magnitude capped
+                   [0, 0, 0]]       # zero flow
