@@ -259,6 +259,36 @@ oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_
                              double *energy_warm, double *energy_plain, int *accepted,
                              oflow_tvl1_stats *stats);
 
+/* ---------------------------------------------------------------- streaming */
+/* Frame streams: the streaming form of the reference's CUDA TV-L1
+ * (runDualTVL1Multiscale(const float *I), src/tvl1/cuda/tvl1.cu:122-130) --
+ * each new frame is paired with the previous one, which stays in device
+ * memory, so a frame crosses the bus once.  A stream carries `lanes`
+ * independent videos of one size and solver; one push takes one new frame per
+ * lane and solves all lanes' pairs (previous, new) as one batch.  Before a
+ * lane's first frame its previous frame is all zeros (the reference's
+ * buffer before its first call).  Uploads run on the stream's own copy
+ * stream: once a push's solve has taken its frames, the next push's upload
+ * overlaps the rest of that solve (pinned host frames, or device frames, and
+ * a stream set with oflow_ctx_set_stream with device outputs, make pushes
+ * asynchronous; otherwise a push returns with the flow in place). */
+typedef struct oflow_stream oflow_stream;
+typedef struct {
+    int solver; /* OFLOW_SOLVER_TVL1 or OFLOW_SOLVER_HS */
+    int width, height;
+    int dtype;  /* of the frames pushed: OFLOW_U8 or OFLOW_F32 */
+    int lanes;  /* videos per stream, >= 1 */
+    oflow_tvl1_params tvl1;
+    oflow_hs_params hs;
+} oflow_stream_desc;
+oflow_status oflow_stream_create(oflow_ctx *ctx, const oflow_stream_desc *desc, oflow_stream **out);
+oflow_status oflow_stream_destroy(oflow_stream *s);
+/* frames, out: arrays of `lanes`; stats (TV-L1, array of lanes) may be NULL */
+oflow_status oflow_stream_push(oflow_stream *s, const oflow_image *frames, const oflow_flow *out,
+                               oflow_tvl1_stats *stats);
+/* frames pushed so far */
+long long oflow_stream_frames(const oflow_stream *s);
+
 /* ------------------------------------------------------------ visualisation */
 /* An 8-bit, 3-channel image (bytes B, G, R per pixel), caller-owned.  pitch in
  * bytes (0 means 3 * width). */

@@ -49,8 +49,7 @@ class TV_L1 {
     TV_L1(int width, int height, float tau = 0.25, float lambda = 0.15, float theta = 0.3,
           int nscales = 100, float zfactor = 0.5, int warps = 5, float epsilon = 0.01,
           int max_iterations = 300, int device = 0)
-        : w_(width), h_(height), u_(2 * (size_t)width * height, 0.0f),
-          prev_((size_t)width * height, 0.0f) {
+        : w_(width), h_(height), u_(2 * (size_t)width * height, 0.0f) {
         p_.tau = tau;
         p_.lambda = lambda;
         p_.theta = theta;
@@ -61,7 +60,10 @@ class TV_L1 {
         p_.max_iterations = max_iterations;
         oflow::compat_check(oflow_ctx_create(device, &ctx_), nullptr);
     }
-    ~TV_L1() { oflow_ctx_destroy(ctx_); }
+    ~TV_L1() {
+        if (stream_) oflow_stream_destroy(stream_);
+        oflow_ctx_destroy(ctx_);
+    }
     TV_L1(const TV_L1 &) = delete;
     TV_L1 &operator=(const TV_L1 &) = delete;
 
@@ -73,11 +75,21 @@ class TV_L1 {
     }
     // Streaming form: one float frame, paired with the previous call's frame
     // (tvl1.cuh:19, tvl1.cu:122-130); before the first frame it is all zeros.
+    // The previous frame stays on the device (oflow_stream): one upload per call.
     void runDualTVL1Multiscale(const float *I) {
-        const oflow_image a{prev_.data(), w_, h_, 0, OFLOW_F32, OFLOW_HOST};
-        const oflow_image b{I, w_, h_, 0, OFLOW_F32, OFLOW_HOST};
-        solve(a, b);
-        std::memcpy(prev_.data(), I, sizeof(float) * (size_t)w_ * h_);
+        if (!stream_) {
+            oflow_stream_desc d{};
+            d.solver = OFLOW_SOLVER_TVL1;
+            d.width = w_;
+            d.height = h_;
+            d.dtype = OFLOW_F32;
+            d.lanes = 1;
+            d.tvl1 = p_;
+            oflow::compat_check(oflow_stream_create(ctx_, &d, &stream_), ctx_);
+        }
+        const oflow_image f{I, w_, h_, 0, OFLOW_F32, OFLOW_HOST};
+        const oflow_flow o{u_.data(), u_.data() + (size_t)w_ * h_, 0, OFLOW_HOST};
+        oflow::compat_check(oflow_stream_push(stream_, &f, &o, &st_), ctx_);
     }
     // Planar [u (w*h) | v (w*h)], valid until the next call.
     float *getU() { return u_.data(); }
@@ -91,7 +103,8 @@ class TV_L1 {
     int w_, h_;
     oflow_tvl1_params p_{};
     oflow_ctx *ctx_ = nullptr;
-    std::vector<float> u_, prev_;
+    oflow_stream *stream_ = nullptr;
+    std::vector<float> u_;
     oflow_tvl1_stats st_{};
 };
 

@@ -780,6 +780,121 @@ oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_
     });
 }
 
+}  // extern "C"
+
+// A frame stream: the latest frame of every lane in one of two device slots;
+// the plan's staged inputs are filled from the slots by device copies.
+struct oflow_stream {
+    oflow_ctx *ctx = nullptr;
+    oflow_stream_desc desc{};
+    std::unique_ptr<TvPlan> tv;
+    std::unique_ptr<HsPlan> hs;
+    DevBuf slots;  // [2][lanes][w*h] frames of the dtype
+    int cur = 0;   // slot holding each lane's latest frame
+    long long frames = 0;
+    cudaStream_t copy = nullptr;
+    cudaEvent_t uploaded = nullptr, consumed = nullptr;
+    size_t frame_bytes() const { return (size_t)desc.width * desc.height * dtype_size(desc.dtype); }
+    char *slot(int k, int lane) const {
+        return slots.as<char>() + ((size_t)k * desc.lanes + lane) * frame_bytes();
+    }
+    ~oflow_stream() {
+        if (copy) cudaStreamDestroy(copy);
+        if (uploaded) cudaEventDestroy(uploaded);
+        if (consumed) cudaEventDestroy(consumed);
+    }
+};
+
+extern "C" {
+
+oflow_status oflow_stream_create(oflow_ctx *ctx, const oflow_stream_desc *desc, oflow_stream **out) {
+    if (!out) return OFLOW_ERR_BAD_ARG;
+    *out = nullptr;
+    std::unique_ptr<oflow_stream> s;
+    const oflow_status st = guard(ctx, [&] {
+        OF_CHECK(ctx != nullptr && desc != nullptr, "stream: null argument");
+        OF_CHECK(desc->solver == OFLOW_SOLVER_TVL1 || desc->solver == OFLOW_SOLVER_HS, "stream: bad solver");
+        OF_CHECK(desc->width > 0 && desc->height > 0 && desc->lanes >= 1, "stream: bad size");
+        OF_CHECK(desc->dtype == OFLOW_U8 || desc->dtype == OFLOW_F32, "stream: bad dtype");
+        s.reset(new oflow_stream());
+        s->ctx = ctx;
+        s->desc = *desc;
+        if (desc->solver == OFLOW_SOLVER_TVL1) {
+            check_tvl1_params(&desc->tvl1);
+            s->tv.reset(new TvPlan(desc->width, desc->height, desc->lanes, desc->dtype, desc->tvl1, false,
+                                   &ctx->tune));
+        } else {
+            s->hs.reset(new HsPlan(desc->width, desc->height, desc->lanes, desc->dtype, desc->hs));
+        }
+        s->slots.alloc(2 * (size_t)desc->lanes * s->frame_bytes());
+        OF_CUDA(cudaMemset(s->slots.as<char>(), 0, s->slots.bytes()));
+        OF_CUDA(cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking));
+        OF_CUDA(cudaEventCreateWithFlags(&s->uploaded, cudaEventDisableTiming));
+        OF_CUDA(cudaEventCreateWithFlags(&s->consumed, cudaEventDisableTiming));
+    });
+    if (st == OFLOW_OK) *out = s.release();
+    return st;
+}
+
+oflow_status oflow_stream_destroy(oflow_stream *s) {
+    if (!s) return OFLOW_OK;
+    const oflow_status st = guard(s->ctx, [&] {
+        OF_CUDA(cudaStreamSynchronize(s->copy));
+        OF_CUDA(cudaStreamSynchronize(s->ctx->stream()));
+    });
+    delete s;
+    return st;
+}
+
+long long oflow_stream_frames(const oflow_stream *s) { return s ? s->frames : -1; }
+
+oflow_status oflow_stream_push(oflow_stream *s, const oflow_image *frames, const oflow_flow *out,
+                               oflow_tvl1_stats *stats) {
+    if (!s) return OFLOW_ERR_BAD_ARG;
+    return guard(s->ctx, [&] {
+        const oflow_stream_desc &d = s->desc;
+        OF_CHECK(frames != nullptr && out != nullptr, "stream: null arrays");
+        for (int i = 0; i < d.lanes; i++) {
+            check_image(&frames[i], "frame");
+            OF_CHECK(frames[i].width == d.width && frames[i].height == d.height && frames[i].dtype == d.dtype,
+                     "stream: frame differs from the stream's size or dtype");
+            check_flow(&out[i], d.width);
+        }
+        const cudaStream_t st = s->ctx->stream();
+        const int nxt = s->cur ^ 1;
+        // upload into the free slot once the previous solve has taken its frames
+        OF_CUDA(cudaStreamWaitEvent(s->copy, s->consumed, 0));
+        const size_t esz = dtype_size(d.dtype);
+        for (int i = 0; i < d.lanes; i++) stage_image(frames[i], s->slot(nxt, i), esz, s->copy);
+        OF_CUDA(cudaEventRecord(s->uploaded, s->copy));
+        OF_CUDA(cudaStreamWaitEvent(st, s->uploaded, 0));
+        const size_t fb = s->frame_bytes();
+        for (int i = 0; i < d.lanes; i++) {
+            void *r0 = s->tv ? s->tv->raw_input(i, 0) : s->hs->raw_input(i, 0);
+            void *r1 = s->tv ? s->tv->raw_input(i, 1) : s->hs->raw_input(i, 1);
+            OF_CUDA(cudaMemcpyAsync(r0, s->slot(s->cur, i), fb, cudaMemcpyDeviceToDevice, st));
+            OF_CUDA(cudaMemcpyAsync(r1, s->slot(nxt, i), fb, cudaMemcpyDeviceToDevice, st));
+        }
+        OF_CUDA(cudaEventRecord(s->consumed, st));
+        bool device_only = stats == nullptr;
+        if (s->tv)
+            s->tv->run(st);
+        else
+            s->hs->run(st);
+        for (int i = 0; i < d.lanes; i++) {
+            const float *ou = s->tv ? s->tv->out_u(i) : s->hs->out_u(i);
+            const float *ov = s->tv ? s->tv->out_v(i) : s->hs->out_v(i);
+            unstage_plane(ou, d.width, d.height, out[i].u, out[i].pitch, out[i].location, st);
+            unstage_plane(ov, d.width, d.height, out[i].v, out[i].pitch, out[i].location, st);
+            if (out[i].location == OFLOW_HOST) device_only = false;
+            if (stats && s->tv) s->tv->read_stats(i, &stats[i], st);
+        }
+        s->cur = nxt;
+        s->frames++;
+        finish(s->ctx, device_only);
+    });
+}
+
 oflow_status oflow_flow_to_color(oflow_ctx *ctx, int n, int width, int height,
                                  const oflow_flow *flows, const oflow_bgr_image *out) {
     return guard(ctx, [&] {

@@ -22,14 +22,14 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .capi import (LIB_PATH, SOLVER_HS, SOLVER_TVL1, BgrImage, Flow, HsParams, Image, Job, LkParams,
+from .capi import (LIB_PATH, SOLVER_HS, SOLVER_TVL1, BgrImage, Flow, StreamDesc, HsParams, Image, Job, LkParams,
                    OflowError, Tvl1Params, Tvl1Profile, Tvl1Stats, lib, status_string)
 
 __all__ = [
     "Context", "OflowError", "TVL1Params", "HSParams", "LKParams", "tvl1", "tvl1_batch",
     "tvl1_energy_trace", "hs", "hs_batch", "lk", "pyrlk", "TV_L1", "initFlow", "ComputeFlow",
     "deleteFlow_mem", "LucasKanade", "nscales", "LIB_PATH", "flow_to_color", "flow_to_color_batch",
-    "save_ppm",
+    "save_ppm", "FrameStream",
 ]
 
 
@@ -476,6 +476,62 @@ def pyrlk(I0, I1, params: LKParams | None = None, ctx: Context | None = None, ou
     h = _ctx(ctx)
     _check(lib().oflow_pyrlk(h, C.byref(a), C.byref(b), C.byref(p), C.byref(f)), h)
     return uv
+
+
+# ------------------------------------------------------------------ streams
+class FrameStream:
+    """oflow_stream_*: `lanes` videos of width x height; push() takes one new
+    frame per lane, uploads it once and returns the flows of the pairs
+    (previous frame, new frame); before a lane's first frame the previous
+    frame is all zeros (the reference's streaming TV-L1)."""
+
+    def __init__(self, width: int, height: int, solver: str = "tvl1", lanes: int = 1,
+                 params=None, dtype: str = "u8", ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        d = StreamDesc()
+        d.solver = {"tvl1": SOLVER_TVL1, "hs": SOLVER_HS}[solver]
+        d.width, d.height, d.lanes = width, height, lanes
+        d.dtype = {"u8": 0, "f32": 1}[dtype]
+        d.tvl1 = (params if solver == "tvl1" and params is not None else TVL1Params()).c()
+        d.hs = (params if solver == "hs" and params is not None else HSParams()).c()
+        self.width, self.height, self.lanes, self.solver = width, height, lanes, solver
+        self._h = C.c_void_p()
+        _check(lib().oflow_stream_create(self.ctx.handle, C.byref(d), C.byref(self._h)),
+               self.ctx.handle)
+
+    @property
+    def frames(self) -> int:
+        return int(lib().oflow_stream_frames(self._h))
+
+    def push(self, frames, out=None, stats: bool = False):
+        """frames: list of `lanes` 2-D frames (numpy or torch).  Returns a list
+        of (u, v) (and stats dicts for TV-L1 when stats=True)."""
+        if len(frames) != self.lanes:
+            raise ValueError("push: one frame per lane")
+        I = (Image * self.lanes)()
+        O = (Flow * self.lanes)()
+        keep, res = [], []
+        for i, f in enumerate(frames):
+            I[i], k = _image(f)
+            keep.append(k)
+            O[i], uv = _outputs(f, self.height, self.width, None if out is None else out[i])
+            res.append(uv)
+        st = (Tvl1Stats * self.lanes)() if stats and self.solver == "tvl1" else None
+        _check(lib().oflow_stream_push(self._h, I, O, st), self.ctx.handle)
+        if st is not None:
+            return res, [_stats_dict(x) for x in st]
+        return res
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().oflow_stream_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ------------------------------------------------------------ visualisation

@@ -57,6 +57,11 @@ class HsParams(C.Structure):
                 ("nsolver", C.c_int)]
 
 
+class StreamDesc(C.Structure):
+    _fields_ = [("solver", C.c_int), ("width", C.c_int), ("height", C.c_int), ("dtype", C.c_int),
+                ("lanes", C.c_int), ("tvl1", Tvl1Params), ("hs", HsParams)]
+
+
 class LkParams(C.Structure):
     _fields_ = [("spac", C.c_int), ("temp", C.c_int), ("window", C.c_int), ("levels", C.c_int),
                 ("iters", C.c_int)]
@@ -113,6 +118,10 @@ SIGNATURES = {
     "oflow_tvl1_warm": (_I, [_VP, _VP, _I, C.POINTER(Image), C.POINTER(Image),
                              C.POINTER(Tvl1Params), C.POINTER(Tvl1Params), C.POINTER(Flow),
                              _VP, _VP, _VP, C.POINTER(Tvl1Stats)]),
+    "oflow_stream_create": (_I, [_VP, C.POINTER(StreamDesc), C.POINTER(_VP)]),
+    "oflow_stream_destroy": (_I, [_VP]),
+    "oflow_stream_push": (_I, [_VP, C.POINTER(Image), C.POINTER(Flow), C.POINTER(Tvl1Stats)]),
+    "oflow_stream_frames": (C.c_longlong, [_VP]),
     "oflow_flow_to_color": (_I, [_VP, _I, _I, _I, C.POINTER(Flow), C.POINTER(BgrImage)]),
     "oflow_conv3x3": (_I, [_I, _I, _I, _I, _I, _I, _I, _I, _I, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "oflow_lk_default_params": (None, [C.POINTER(LkParams)]),

@@ -40,6 +40,16 @@ int main(int argc, char **argv) {
         o = fopen(argv[3], "wb");
         fwrite(u.data(), sizeof(float), w * h, o);
         fclose(o);
+        // streaming form: the second frame pairs with the first (tvl1.cu:122-130)
+        TV_L1 s(w, h, 0.25, 0.15, 0.3, 3, 0.5, 5, 0.01, 10);
+        s.runDualTVL1Multiscale(a.data());
+        s.runDualTVL1Multiscale(b.data());
+        std::vector<unsigned char> bgr(3 * w * h);
+        flowToColor(w, h, s.getU(), bgr.data());
+        o = fopen(argv[4], "wb");
+        fwrite(s.getU(), sizeof(float), 2 * w * h, o);
+        fwrite(bgr.data(), 1, 3 * w * h, o);
+        fclose(o);
     } catch (const oflow::compat_error &e) {
         printf("compat_error %d %s\n", (int)e.status, e.what());
         return 2;
@@ -69,7 +79,8 @@ def test_compat_program_compiles_and_reports_errors_without_device(tmp_path, of)
         pass
     (tmp_path / "in.bin").write_bytes(bytes(96 * 64 * 2))
     r = subprocess.run([str(exe), str(tmp_path / "in.bin"), str(tmp_path / "u.bin"),
-                        str(tmp_path / "l.bin")], capture_output=True, text=True)
+                        str(tmp_path / "l.bin"), str(tmp_path / "s.bin")], capture_output=True,
+                       text=True)
     assert r.returncode == 2 and "compat_error 4" in r.stdout
 
 
@@ -81,7 +92,8 @@ def test_compat_program_matches_c_abi(tmp_path, of):
     a, b = synth.quantize(p.I0), synth.quantize(p.I1)
     (tmp_path / "in.bin").write_bytes(a.tobytes() + b.tobytes())
     r = subprocess.run([str(exe), str(tmp_path / "in.bin"), str(tmp_path / "u.bin"),
-                        str(tmp_path / "l.bin")], capture_output=True, text=True)
+                        str(tmp_path / "l.bin"), str(tmp_path / "s.bin")], capture_output=True,
+                       text=True)
     assert r.returncode == 0, r.stdout + r.stderr
     U = np.fromfile(tmp_path / "u.bin", np.float32)
     u, v = of.tvl1(a, b, of.TVL1Params(nscales=3, max_iterations=10))
@@ -89,3 +101,10 @@ def test_compat_program_matches_c_abi(tmp_path, of):
     L = np.fromfile(tmp_path / "l.bin", np.float32).reshape(64, 96)
     lu, _ = of.lk([a, b], 1, of.LKParams(3, 2, 5))
     assert np.array_equal(L, lu)
+    S = np.fromfile(tmp_path / "s.bin", np.uint8)
+    su = S[: 2 * 96 * 64 * 4].view(np.float32)
+    fu, fv = of.tvl1(a.astype(np.float32), b.astype(np.float32),
+                     of.TVL1Params(nscales=3, max_iterations=10))
+    assert np.array_equal(su, np.concatenate([fu.ravel(), fv.ravel()]))
+    img = S[2 * 96 * 64 * 4:].reshape(64, 96, 3)
+    assert np.array_equal(img, of.flow_to_color(fu, fv))
