@@ -60,6 +60,14 @@ void unstage_plane(const float *src, int w, int h, float *dst, int pitch, int lo
                               s));
 }
 
+// Stages a pair into the plan's own buffers and points its frame table there.
+void stage_pair_raw(TvPlan &pl, int b, const oflow_image &I0, const oflow_image &I1, cudaStream_t s) {
+    stage_image(I0, pl.raw_input(b, 0), dtype_size(I0.dtype), s);
+    stage_image(I1, pl.raw_input(b, 1), dtype_size(I1.dtype), s);
+    pl.bind_raw(b, 0);
+    pl.bind_raw(b, 1);
+}
+
 }  // namespace oflow
 
 namespace {
@@ -200,13 +208,21 @@ void run_tvl1(oflow_ctx *ctx, int n, const oflow_image *I0, const oflow_image *I
     for (const Group &g : groups) {
         TvPlan &pl = tv_plan(ctx, g.w, g.h, (int)g.idx.size(), g.dtype, *p, energy_trace != nullptr);
         for (size_t b = 0; b < g.idx.size(); b++) {
-            stage_image(I0[g.idx[b]], pl.raw_input((int)b, 0), dtype_size(g.dtype), st);
-            stage_image(I1[g.idx[b]], pl.raw_input((int)b, 1), dtype_size(g.dtype), st);
+            // device frames are read in place (pitched); host frames are staged
+            const oflow_image *im[2] = {&I0[g.idx[b]], &I1[g.idx[b]]};
+            for (int k = 0; k < 2; k++) {
+                if (im[k]->location == OFLOW_DEVICE) {
+                    pl.bind_frame((int)b, k, im[k]->data, im[k]->pitch ? im[k]->pitch : im[k]->width);
+                } else {
+                    stage_image(*im[k], pl.raw_input((int)b, k), dtype_size(g.dtype), st);
+                    pl.bind_raw((int)b, k);
+                }
+            }
         }
         if (prof)
             pl.profile(st, prof);
         else if (energy_trace)
-            pl.record(st);
+            pl.run_eager(st);
         else
             pl.run(st);
         for (size_t b = 0; b < g.idx.size(); b++) {
@@ -362,10 +378,7 @@ oflow_status oflow_tvl1_autotune(oflow_ctx *ctx, int n, const oflow_image *I0,
         const Group &g = groups[0];
         const cudaStream_t st = ctx->stream();
         TvPlan &pl = tv_plan(ctx, g.w, g.h, n, g.dtype, *p, false);
-        for (int b = 0; b < n; b++) {
-            stage_image(I0[b], pl.raw_input(b, 0), dtype_size(g.dtype), st);
-            stage_image(I1[b], pl.raw_input(b, 1), dtype_size(g.dtype), st);
-        }
+        for (int b = 0; b < n; b++) stage_pair_raw(pl, b, I0[b], I1[b], st);
         pl.run(st);
         pl.autotune(st, &ctx->tune);
         OF_CUDA(cudaStreamSynchronize(st));
@@ -745,10 +758,7 @@ oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_
         }
         OF_CHECK(wp->level_w(3) == net->net->out_w() && wp->level_h(3) == net->net->out_h(),
                  "tvl1 warm: scale 3 does not match the network output");
-        for (int b = 0; b < n; b++) {
-            stage_image(I0[b], wp->raw_input(b, 0), dtype_size(g.dtype), st);
-            stage_image(I1[b], wp->raw_input(b, 1), dtype_size(g.dtype), st);
-        }
+        for (int b = 0; b < n; b++) stage_pair_raw(*wp, b, I0[b], I1[b], st);
         net->net->forward(wp->raw_input(0, 0), g.dtype, wp->plane_stride(), st);
         net->net->flow_to(wp->uz(), wp->plane_stride(), nullptr, st);
         wp->run(st);
@@ -760,10 +770,7 @@ oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_
         TvPlan *pp = nullptr;
         if (plain) {
             pp = &tv_plan(ctx, g.w, g.h, n, g.dtype, *plain, false);
-            for (int b = 0; b < n; b++) {
-                stage_image(I0[b], pp->raw_input(b, 0), dtype_size(g.dtype), st);
-                stage_image(I1[b], pp->raw_input(b, 1), dtype_size(g.dtype), st);
-            }
+            for (int b = 0; b < n; b++) stage_pair_raw(*pp, b, I0[b], I1[b], st);
             pp->run(st);
             pp->true_energy(ep.data(), st);
             for (int b = 0; b < n; b++) acc[b] = ew[b] <= 1.01 * ep[b] ? 1 : 0;
@@ -782,26 +789,30 @@ oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_
 
 }  // extern "C"
 
-// A frame stream: the latest frame of every lane in one of two device slots;
-// the plan's staged inputs are filled from the slots by device copies.
+// A frame stream: frame k of every lane goes to slot k % 3.  A TV-L1 solve
+// reads its two frames from the slots through the plan's frame table; an HS
+// solve copies them into its staging buffers.  Slot k % 3 last held frame
+// k - 3, read by the solves of pushes k - 3 and k - 2, so the upload of frame
+// k waits for the end of solve k - 2 only and overlaps solve k - 1.
 struct oflow_stream {
     oflow_ctx *ctx = nullptr;
     oflow_stream_desc desc{};
     std::unique_ptr<TvPlan> tv;
     std::unique_ptr<HsPlan> hs;
-    DevBuf slots;  // [2][lanes][w*h] frames of the dtype
-    int cur = 0;   // slot holding each lane's latest frame
+    DevBuf slots;  // [3][lanes][w*h] frames of the dtype; slot 2 starts as zeros
     long long frames = 0;
     cudaStream_t copy = nullptr;
-    cudaEvent_t uploaded = nullptr, consumed = nullptr;
+    cudaEvent_t uploaded = nullptr;
+    cudaEvent_t done[3] = {nullptr, nullptr, nullptr};
     size_t frame_bytes() const { return (size_t)desc.width * desc.height * dtype_size(desc.dtype); }
-    char *slot(int k, int lane) const {
-        return slots.as<char>() + ((size_t)k * desc.lanes + lane) * frame_bytes();
+    char *slot(long long k, int lane) const {
+        return slots.as<char>() + ((size_t)(k % 3) * desc.lanes + lane) * frame_bytes();
     }
     ~oflow_stream() {
         if (copy) cudaStreamDestroy(copy);
         if (uploaded) cudaEventDestroy(uploaded);
-        if (consumed) cudaEventDestroy(consumed);
+        for (cudaEvent_t e : done)
+            if (e) cudaEventDestroy(e);
     }
 };
 
@@ -826,11 +837,11 @@ oflow_status oflow_stream_create(oflow_ctx *ctx, const oflow_stream_desc *desc, 
         } else {
             s->hs.reset(new HsPlan(desc->width, desc->height, desc->lanes, desc->dtype, desc->hs));
         }
-        s->slots.alloc(2 * (size_t)desc->lanes * s->frame_bytes());
+        s->slots.alloc(3 * (size_t)desc->lanes * s->frame_bytes());
         OF_CUDA(cudaMemset(s->slots.as<char>(), 0, s->slots.bytes()));
         OF_CUDA(cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking));
         OF_CUDA(cudaEventCreateWithFlags(&s->uploaded, cudaEventDisableTiming));
-        OF_CUDA(cudaEventCreateWithFlags(&s->consumed, cudaEventDisableTiming));
+        for (cudaEvent_t &e : s->done) OF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     });
     if (st == OFLOW_OK) *out = s.release();
     return st;
@@ -861,26 +872,38 @@ oflow_status oflow_stream_push(oflow_stream *s, const oflow_image *frames, const
             check_flow(&out[i], d.width);
         }
         const cudaStream_t st = s->ctx->stream();
-        const int nxt = s->cur ^ 1;
-        // upload into the free slot once the previous solve has taken its frames
-        OF_CUDA(cudaStreamWaitEvent(s->copy, s->consumed, 0));
+        const long long k = s->frames;  // this push's frame index; the previous is k - 1
+        if (k >= 2) OF_CUDA(cudaStreamWaitEvent(s->copy, s->done[(k - 2) % 3], 0));
+        // a device frame may come from work queued on the solve stream: order
+        // its copy after that (host frames are ready when push is called)
+        bool any_device = false;
+        for (int i = 0; i < d.lanes; i++) any_device |= frames[i].location == OFLOW_DEVICE;
+        if (any_device) {
+            OF_CUDA(cudaEventRecord(s->uploaded, st));
+            OF_CUDA(cudaStreamWaitEvent(s->copy, s->uploaded, 0));
+        }
         const size_t esz = dtype_size(d.dtype);
-        for (int i = 0; i < d.lanes; i++) stage_image(frames[i], s->slot(nxt, i), esz, s->copy);
+        for (int i = 0; i < d.lanes; i++) stage_image(frames[i], s->slot(k, i), esz, s->copy);
         OF_CUDA(cudaEventRecord(s->uploaded, s->copy));
         OF_CUDA(cudaStreamWaitEvent(st, s->uploaded, 0));
-        const size_t fb = s->frame_bytes();
+        const long long kp = k + 2;  // slot of frame k - 1 (slot 2 holds zeros before frame 2)
         for (int i = 0; i < d.lanes; i++) {
-            void *r0 = s->tv ? s->tv->raw_input(i, 0) : s->hs->raw_input(i, 0);
-            void *r1 = s->tv ? s->tv->raw_input(i, 1) : s->hs->raw_input(i, 1);
-            OF_CUDA(cudaMemcpyAsync(r0, s->slot(s->cur, i), fb, cudaMemcpyDeviceToDevice, st));
-            OF_CUDA(cudaMemcpyAsync(r1, s->slot(nxt, i), fb, cudaMemcpyDeviceToDevice, st));
+            if (s->tv) {
+                s->tv->bind_frame(i, 0, s->slot(kp, i), d.width);
+                s->tv->bind_frame(i, 1, s->slot(k, i), d.width);
+            } else {
+                OF_CUDA(cudaMemcpyAsync(s->hs->raw_input(i, 0), s->slot(kp, i), s->frame_bytes(),
+                                        cudaMemcpyDeviceToDevice, st));
+                OF_CUDA(cudaMemcpyAsync(s->hs->raw_input(i, 1), s->slot(k, i), s->frame_bytes(),
+                                        cudaMemcpyDeviceToDevice, st));
+            }
         }
-        OF_CUDA(cudaEventRecord(s->consumed, st));
         bool device_only = stats == nullptr;
         if (s->tv)
             s->tv->run(st);
         else
             s->hs->run(st);
+        OF_CUDA(cudaEventRecord(s->done[k % 3], st));
         for (int i = 0; i < d.lanes; i++) {
             const float *ou = s->tv ? s->tv->out_u(i) : s->hs->out_u(i);
             const float *ov = s->tv ? s->tv->out_v(i) : s->hs->out_v(i);
@@ -889,7 +912,6 @@ oflow_status oflow_stream_push(oflow_stream *s, const oflow_image *frames, const
             if (out[i].location == OFLOW_HOST) device_only = false;
             if (stats && s->tv) s->tv->read_stats(i, &stats[i], st);
         }
-        s->cur = nxt;
         s->frames++;
         finish(s->ctx, device_only);
     });

@@ -104,22 +104,26 @@ __device__ __forceinline__ bool better_min(const NormRec &a, const NormRec &b) {
 }
 
 // ---------------------------------------------------------------- ingest
-// raw frames -> float planes T[b][k], and per-block |x| extrema for the
-// normalisation (tvl1.cpp:118-123, :302-317).  grid (blocks, B).
+// Per-block |x| extrema of both frames of a pair for the normalisation
+// (tvl1.cpp:118-123 conversion, :302-317 range), read through the frame table
+// (the plan's staging buffers or the caller's pitched device frames); the
+// conversion itself happens where the first blur loads the frames.  Indices
+// are those of the dense w x h frame, as in the reference.  grid (blocks, B).
 template <typename In>
-__global__ void __launch_bounds__(kIngestNT) k_ingest(const In *__restrict__ raw, float *T,
-                                                      int N, NormRec *recs, int nblk) {
+__global__ void __launch_bounds__(kIngestNT) k_ingest(const FrameRef *__restrict__ frames, int w,
+                                                      int h, NormRec *recs, int nblk) {
     const int b = blockIdx.y;
+    const int N = w * h;
     __shared__ NormRec sh[4][kIngestNT / 32];
     NormRec r[4];
     r[0] = {-1.0f, INT_MAX, 0.0f, 0}; r[1] = {INFINITY, INT_MAX, 0.0f, 0};
     r[2] = r[0]; r[3] = r[1];
     for (int k = 0; k < 2; k++) {
-        const In *src = raw + (size_t)(2 * b + k) * N;
-        float *dst = T + (size_t)(2 * b + k) * N;
+        const FrameRef f = frames[2 * b + k];
+        const In *src = static_cast<const In *>(f.p);
         for (int i = blockIdx.x * kIngestNT + threadIdx.x; i < N; i += nblk * kIngestNT) {
-            const float x = (float)src[i];
-            dst[i] = x;
+            const int y = i / w, xx = i - y * w;
+            const float x = (float)src[(size_t)y * f.pitch + xx];
             const NormRec c{fabsf(x), i, x, 0};
             if (better_max(c, r[2 * k])) r[2 * k] = c;
             if (better_min(c, r[2 * k + 1])) r[2 * k + 1] = c;
@@ -191,10 +195,13 @@ __device__ __forceinline__ int gauss_mirror(int x, int n) {
     return x;
 }
 
+// SRC 0: float planes at src; 1 / 2: uint8 / float frames through the frame
+// table (plane z = frame z of the table), converted to float on load.
+template <int SRC>
 __global__ void __launch_bounds__(kGaussNT) k_gauss(const float *__restrict__ src, float *dst,
                                                     int nx, int ny, size_t plane_stride,
                                                     GaussTaps taps, const TvCtrl *ctrl,
-                                                    int normalize) {
+                                                    int normalize, const FrameRef *frames) {
     constexpr int LW = kGaussTW + 2 * kGaussMaxR;
     __shared__ float sIn[(kGaussTH + 2 * kGaussMaxR) * LW];
     __shared__ float sRow[(kGaussTH + 2 * kGaussMaxR) * kGaussTW];
@@ -217,7 +224,14 @@ __global__ void __launch_bounds__(kGaussNT) k_gauss(const float *__restrict__ sr
         const int my = gauss_mirror(y0 - R + ly, ny), mx = gauss_mirror(x0 - R + lx, nx);
         float v = 0.0f;
         if (mx >= 0 && mx < nx && my >= 0 && my < ny) {
-            v = __ldg(in + (size_t)my * nx + mx);
+            if (SRC == 0) {
+                v = __ldg(in + (size_t)my * nx + mx);
+            } else {
+                const FrameRef f = frames[z];
+                const size_t q = (size_t)my * f.pitch + mx;
+                v = SRC == 1 ? (float)__ldg(static_cast<const uint8_t *>(f.p) + q)
+                             : __ldg(static_cast<const float *>(f.p) + q);
+            }
             if (apply) v = (float)(255.0 * (double)(v - mn) / (double)den);
         }
         sIn[ly * LW + lx] = v;
@@ -905,7 +919,7 @@ GaussTaps make_zoom_taps(float zfactor) { return make_taps(zoom_sigma(zfactor));
 void launch_gauss(const float *src, float *dst, int nx, int ny, size_t stride,
                   const GaussTaps &t, int planes, cudaStream_t st) {
     dim3 g(div_up(nx, kGaussTW), div_up(ny, kGaussTH), planes);
-    k_gauss<<<g, kGaussNT, 0, st>>>(src, dst, nx, ny, stride, t, nullptr, 0);
+    k_gauss<0><<<g, kGaussNT, 0, st>>>(src, dst, nx, ny, stride, t, nullptr, 0, nullptr);
 }
 
 void launch_resample(const float *src, size_t sstride, int nx, int ny, float *dst,
@@ -1018,11 +1032,31 @@ TvPlan::TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, boo
     o_energy_ = ar_.reserve((size_t)B * energy_slots_ * 8);
     o_tarr_ = ar_.reserve(sizeof(unsigned) * B);
     o_tout_ = ar_.reserve(sizeof(double) * B);
+    o_frames_ = ar_.reserve(sizeof(FrameRef) * 2 * B);
     ar_.commit();
+    frames_.resize(2 * (size_t)B);
+    for (int b = 0; b < B; b++)
+        for (int k = 0; k < 2; k++) bind_raw(b, k);
+    OF_CUDA(cudaMemcpy(ar_.at<FrameRef>(o_frames_), frames_.data(), sizeof(FrameRef) * frames_.size(),
+                       cudaMemcpyHostToDevice));
     OF_CUDA(cudaMemset(ar_.at<char>(o_ctrl_), 0, B * sizeof(TvCtrl)));
     // scales above a warm start's first scale never record a count
     OF_CUDA(cudaMemset(ar_.at<char>(o_iters_), 0, (size_t)B * iter_stride_ * 4));
     tb_set_smem_attrs();
+}
+
+void TvPlan::bind_frame(int b, int k, const void *p, int pitch) {
+    frames_[2 * (size_t)b + k] = FrameRef{p, pitch};
+}
+void TvPlan::bind_raw(int b, int k) { frames_[2 * (size_t)b + k] = FrameRef{raw_input(b, k), w_}; }
+void TvPlan::upload_frames(cudaStream_t st) {
+    // pageable source: the runtime copies it out before returning
+    OF_CUDA(cudaMemcpyAsync(ar_.at<FrameRef>(o_frames_), frames_.data(), sizeof(FrameRef) * frames_.size(),
+                            cudaMemcpyHostToDevice, st));
+}
+void TvPlan::run_eager(cudaStream_t st) {
+    upload_frames(st);
+    record(st);
 }
 
 void *TvPlan::raw_input(int b, int k) const {
@@ -1062,22 +1096,27 @@ void TvPlan::record(cudaStream_t st) {
     };
 
     OF_CUDA(cudaMemsetAsync(iters, 0, sizeof(int) * (size_t)B * iter_stride_, st));
-    // ingest + normalisation range
+    // normalisation range of both frames, read through the frame table
+    const FrameRef *frames = ar_.at<FrameRef>(o_frames_);
     {
         dim3 g(ingest_blocks_, B);
         if (dtype_ == OFLOW_U8)
-            k_ingest<uint8_t><<<g, kIngestNT, 0, st>>>(ar_.at<uint8_t>(o_raw_), T, (int)N0, recs,
-                                                       ingest_blocks_);
+            k_ingest<uint8_t><<<g, kIngestNT, 0, st>>>(frames, w_, h_, recs, ingest_blocks_);
         else
-            k_ingest<float><<<g, kIngestNT, 0, st>>>(ar_.at<float>(o_raw_), T, (int)N0, recs,
-                                                     ingest_blocks_);
+            k_ingest<float><<<g, kIngestNT, 0, st>>>(frames, w_, h_, recs, ingest_blocks_);
         k_norm_finalize<<<B, 32, 0, st>>>(recs, ingest_blocks_, ctrl);
         launches_ += 2;
     }
-    // normalised, pre-smoothed level 0 (tvl1.cpp:140-144)
+    // conversion, normalisation and pre-smoothing of level 0 in one pass
+    // (tvl1.cpp:137-144)
     {
         dim3 g(div_up(w_, kGaussTW), div_up(h_, kGaussTH), 2 * B);
-        k_gauss<<<g, kGaussNT, 0, st>>>(T, pyr + pyr_off_[0], w_, h_, N0, taps0_, ctrl, 1);
+        if (dtype_ == OFLOW_U8)
+            k_gauss<1><<<g, kGaussNT, 0, st>>>(nullptr, pyr + pyr_off_[0], w_, h_, N0, taps0_, ctrl, 1,
+                                               frames);
+        else
+            k_gauss<2><<<g, kGaussNT, 0, st>>>(nullptr, pyr + pyr_off_[0], w_, h_, N0, taps0_, ctrl, 1,
+                                               frames);
         launches_ += 1;
     }
     // pyramid (tvl1.cpp:147-154)
@@ -1085,7 +1124,8 @@ void TvPlan::record(cudaStream_t st) {
         const int nx = nx_[s - 1], ny = ny_[s - 1];
         const size_t sp = (size_t)nx * ny, dp = (size_t)nx_[s] * ny_[s];
         dim3 g(div_up(nx, kGaussTW), div_up(ny, kGaussTH), 2 * B);
-        k_gauss<<<g, kGaussNT, 0, st>>>(pyr + pyr_off_[s - 1], T, nx, ny, sp, tapsz_, ctrl, 0);
+        k_gauss<0><<<g, kGaussNT, 0, st>>>(pyr + pyr_off_[s - 1], T, nx, ny, sp, tapsz_, ctrl, 0,
+                                           nullptr);
         dim3 blk(32, 8), gr(div_up(nx_[s], 32), div_up(ny_[s], 8), 2 * B);
         k_resample<<<gr, blk, 0, st>>>(T, sp, nx, ny, pyr + pyr_off_[s], dp, nx_[s], ny_[s],
                                        prm_.zfactor, prm_.zfactor);
@@ -1186,6 +1226,7 @@ void TvPlan::profile(cudaStream_t st, oflow_tvl1_profile *out) {
             OF_CUDA(cudaEventRecordWithFlags(t1, s, cudaEventRecordExternal));
         });
         prof_ = nullptr;
+        upload_frames(st);
         g.launch(st);
         OF_CUDA(cudaStreamSynchronize(st));
         std::memset(out, 0, sizeof(*out));
@@ -1292,6 +1333,7 @@ void TvPlan::true_energy(double *host_out, cudaStream_t st) {
 }
 
 void TvPlan::run(cudaStream_t st) {
+    upload_frames(st);
     if (!graph_.ready()) graph_.capture(st, [&](cudaStream_t s) { record(s); });
     graph_.launch(st);
 }

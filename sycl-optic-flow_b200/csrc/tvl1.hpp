@@ -8,6 +8,8 @@
 
 #include "internal.hpp"
 
+#include <vector>
+
 namespace oflow {
 
 // Normalised Gaussian half-kernel (centre + radius taps), double precision.
@@ -36,6 +38,13 @@ void launch_resample(const float *src, size_t sstride, int nx, int ny, float *ds
                      size_t dstride, int nxx, int nyy, float dx, float dy, int planes,
                      cudaStream_t st);
 
+// Where a plan reads one input frame: a device pointer of the plan's dtype and
+// its row pitch in elements.
+struct FrameRef {
+    const void *p;
+    long long pitch;
+};
+
 class TvPlan {
   public:
     // start_scale >= 0: warm start -- the solve begins at that scale from the
@@ -56,13 +65,22 @@ class TvPlan {
     // Device destination of input frame k (0: I0, 1: I1) of pair b: a dense
     // w*h plane of the plan's dtype.
     void *raw_input(int b, int k) const;
+    // The next run reads frame k of pair b straight from `p` (device, the
+    // plan's dtype, `pitch` elements per row) instead of raw_input(b, k);
+    // bind_raw restores the staging buffer.  The table is uploaded by run(),
+    // run_eager() and profile().
+    void bind_frame(int b, int k, const void *p, int pitch);
+    void bind_raw(int b, int k);
     const float *out_u(int b) const;
     const float *out_v(int b) const;
     const int *iters_dev() const;
     // Enqueue the whole solve (captured into a graph on first use).
     void run(cudaStream_t st);
-    // Enqueue the launches directly on `st` (also what the graph captures).
+    // Enqueue the launches directly on `st` (also what the graph captures);
+    // reads the frame table as last uploaded.
     void record(cudaStream_t st);
+    // upload the frame table, then record(): an eager run
+    void run_eager(cudaStream_t st);
     void read_stats(int b, oflow_tvl1_stats *out, cudaStream_t st) const;
     // Eager run with events around each warp / inner-iteration launch.
     void profile(cudaStream_t st, oflow_tvl1_profile *out);
@@ -109,6 +127,9 @@ class TvPlan {
            o_Uz_ = 0, o_P0_ = 0, o_P1_ = 0, o_out_ = 0, o_ctrl_ = 0, o_part_ = 0, o_recs_ = 0,
            o_iters_ = 0, o_energy_ = 0;
     Graph graph_;
+    std::vector<FrameRef> frames_;  // [B][2], host copy of the device table
+    size_t o_frames_ = 0;
+    void upload_frames(cudaStream_t st);
 };
 
 }  // namespace oflow

@@ -124,6 +124,37 @@ def test_device_and_pitched_buffers(of, ctx):
     assert np.array_equal(ou.cpu().numpy(), u) and np.array_equal(ov.cpu().numpy(), v)
 
 
+def test_device_frames_read_in_place_then_host_frames(of, orc, ctx):
+    """Device frames (pitched u8 and f32) are read in place through the plan's
+    frame table, with conversion and normalisation in the first blur; later
+    calls on the same plan with host frames, and the autotuner, read their own
+    staged copies, never the earlier device pointers."""
+    import torch
+    prm = of.TVL1Params(nscales=4, max_iterations=15)
+    A = [_pair(500 + i, 90, 66)[1:] for i in range(2)]
+    Bp = [_pair(600 + i, 90, 66)[1:] for i in range(2)]
+
+    def pitched(img, dtype):
+        t = torch.zeros((66, 96), dtype=dtype, device="cuda")
+        t[:, :90] = torch.from_numpy(img).to(dtype).cuda()
+        return t[:, :90]
+
+    def check(pairs, res):
+        for (a, b), (u, v) in zip(pairs, res):
+            ou, ov, _, _ = _oracle(orc, a, b, prm)
+            u = u.cpu().numpy() if hasattr(u, "cpu") else u
+            v = v.cpu().numpy() if hasattr(v, "cpu") else v
+            assert np.array_equal(u, ou) and np.array_equal(v, ov)
+
+    check(A, of.tvl1_batch([(pitched(a, torch.uint8), pitched(b, torch.uint8)) for a, b in A], prm, ctx))
+    check(Bp, of.tvl1_batch(Bp, prm, ctx))
+    f32 = [(a.astype(np.float32), b.astype(np.float32)) for a, b in A]
+    check(A, of.tvl1_batch([(pitched(a, torch.float32), pitched(b, torch.float32)) for a, b in f32],
+                           prm, ctx))
+    of.tvl1_autotune(Bp, prm, ctx)
+    check(Bp, of.tvl1_batch(Bp, prm, ctx))
+
+
 def test_full_size_workload_against_oracle_and_reference(of, orc, ctx):
     """1024x436, 5 scales x 5 warps x 50 iterations (the benchmark workload)."""
     from oflow import synth
