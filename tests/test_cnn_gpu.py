@@ -115,3 +115,40 @@ def test_warm_start_judge(of):
         if not acc:
             pu, pv = of.tvl1(a, b, plain)
             assert np.array_equal(u, pu) and np.array_equal(v, pv)
+
+
+def test_trained_network_gains_over_no_network(of):
+    """What the trained network buys: the same reduced schedule (2 warps x 20
+    iterations) on 1024x436 pairs of the benchmark generator, started three
+    ways -- scale 3 from the trained network, scale 3 from zero flow (all
+    network weights zero), and the plain pyramid from the coarsest scale.
+    The trained start gives lower TV-L1 energy and lower EPE than both."""
+    from oflow import synth, warmstart
+    n = 8
+    gen = [synth.tvl1_pair(seed=20_000 + i) for i in range(n)]
+    pairs = [(synth.quantize(p.I0), synth.quantize(p.I1)) for p in gen]
+    ctx = of.Context(0)
+    net = of.WarmNet(1024, 436, n, ctx)
+    params, _ = warmstart.load()
+    reduced = of.TVL1Params(nscales=5, warps=2, max_iterations=20)
+
+    def epe(res):
+        return np.mean([synth.epe(u, v, p.u, p.v, p.valid, 8) for (u, v), p in zip(res, gen)])
+
+    net.set_params(params)
+    # the judge here is the plain pyramid with the same reduced schedule
+    _, info_t = of.tvl1_warm(pairs, net, reduced, reduced, ctx)
+    e_trained, e_plain = info_t["energy_warm"], info_t["energy_plain"]
+    plain_res = of.tvl1_batch(pairs, reduced, ctx)
+    net.set_params(np.zeros_like(params))
+    res_z, info_z = of.tvl1_warm(pairs, net, reduced, None, ctx)
+    e_zero = info_z["energy_warm"]
+    # energies are of the warm results themselves (not of the judged choice)
+    assert np.mean(e_trained) < np.mean(e_zero)
+    assert np.mean(e_trained) < np.mean(e_plain)
+    # EPE of the warm-started results (re-solved without the judge)
+    net.set_params(params)
+    res_t2, _ = of.tvl1_warm(pairs, net, reduced, None, ctx)
+    assert epe(res_t2) < epe(res_z)
+    assert epe(res_t2) < epe(plain_res)
+    ctx.close()
