@@ -348,7 +348,11 @@ def our_arm(args, rank, world, local_rank):
     traffic = ncu_traffic()
     if traffic is not None:
         traffic *= P  # DRAM traffic of a launch grows with the pairs it processes
-    launches_per_step = prof["launches"]
+    # the graph replays' launch count (inner iterations run as device-ended
+    # while-loops, so it depends on the data); the timed steps replay the same
+    # pairs, so each step launched the same kernels
+    oflow.tvl1_batch(d_in, prm, ctx, out=d_out)
+    launches_per_step = ctx.last_launches()
 
     # --- end to end through the public API: pinned host frames in, flow out
     h_in = []

@@ -71,6 +71,8 @@ typedef struct {
 
 /* ------------------------------------------------------------------ context */
 oflow_status oflow_ctx_create(int device, oflow_ctx **out);
+/* Waits for the context's work and frees it.  Nets and streams created on it
+ * become inert: they can still be destroyed (and nothing else). */
 oflow_status oflow_ctx_destroy(oflow_ctx *ctx);
 /* Run subsequent work on a caller-owned cudaStream_t (NULL: the context's own
  * stream). */
@@ -160,6 +162,11 @@ oflow_status oflow_tvl1_autotune(oflow_ctx *ctx, int n, const oflow_image *I0,
                                  const oflow_image *I1, const oflow_tvl1_params *p,
                                  int *cfg_per_scale);
 oflow_status oflow_ctx_save_tuning(oflow_ctx *ctx, const char *path);
+/* Kernel launches the last oflow_tvl1 / oflow_tvl1_batch call of this context
+ * executed on the device (the captured schedule: per warp ceil(max/4)+1
+ * inner-iteration launches, those after every pair stopped returning at
+ * once). */
+oflow_status oflow_ctx_last_launches(oflow_ctx *ctx, long long *launches);
 oflow_status oflow_ctx_load_tuning(oflow_ctx *ctx, const char *path);
 
 /* ------------------------------------------------------------ Horn-Schunck */

@@ -102,6 +102,10 @@ struct oflow_ctx {
     std::vector<std::unique_ptr<TvPlan>> tv_warm;  // plans that start at scale 3
     std::vector<std::unique_ptr<MixedBatch>> mixed;
     DevBuf color_scratch;  // host-side flows / images of oflow_flow_to_color
+    std::vector<TvPlan *> last_tv;  // plans run by the last oflow_tvl1(_batch) call
+    // objects created on this context; destroying the context detaches them
+    std::vector<oflow_net *> nets;
+    std::vector<oflow_stream *> streams;
     cudaStream_t stream() const { return user ? user : own; }
 };
 
@@ -157,6 +161,7 @@ TvPlan &tv_plan(oflow_ctx *ctx, int w, int h, int B, int dtype, const oflow_tvl1
             pl->traced() == trace && same(pl->params(), p))
             return *pl;
     ctx->tv.emplace_back(new TvPlan(w, h, B, dtype, p, trace, &ctx->tune));
+    if (ctx->tv.size() > kMaxPlans) ctx->last_tv.clear();  // an evicted plan may be listed
     keep_recent(ctx->tv);
     return *ctx->tv.back();
 }
@@ -205,8 +210,10 @@ void run_tvl1(oflow_ctx *ctx, int n, const oflow_image *I0, const oflow_image *I
     bool device_only = stats == nullptr && energy_trace == nullptr && prof == nullptr;
     const std::vector<Group> groups = group_pairs(n, I0, I1);
     OF_CHECK(prof == nullptr || groups.size() == 1, "tvl1 profile: pairs must share one size");
+    ctx->last_tv.clear();
     for (const Group &g : groups) {
         TvPlan &pl = tv_plan(ctx, g.w, g.h, (int)g.idx.size(), g.dtype, *p, energy_trace != nullptr);
+        if (!prof && !energy_trace) ctx->last_tv.push_back(&pl);
         for (size_t b = 0; b < g.idx.size(); b++) {
             // device frames are read in place (pitched); host frames are staged
             const oflow_image *im[2] = {&I0[g.idx[b]], &I1[g.idx[b]]};
@@ -238,6 +245,10 @@ void run_tvl1(oflow_ctx *ctx, int n, const oflow_image *I0, const oflow_image *I
 }
 
 }  // namespace
+
+// Detaches the nets and streams of a context being destroyed: their handles
+// stay valid for destroy calls but no longer reach the context.
+static void detach_children(oflow_ctx *ctx);
 
 extern "C" {
 
@@ -285,6 +296,7 @@ oflow_status oflow_ctx_destroy(oflow_ctx *ctx) {
     if (!ctx) return OFLOW_ERR_BAD_ARG;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream());
+    detach_children(ctx);
     ctx->tv.clear();
     ctx->hs.clear();
     ctx->pyrlk.clear();
@@ -306,6 +318,7 @@ oflow_status oflow_ctx_trim(oflow_ctx *ctx) {
     if (!ctx) return OFLOW_ERR_BAD_ARG;
     return guard(ctx, [&] {
         OF_CUDA(cudaStreamSynchronize(ctx->stream()));
+        ctx->last_tv.clear();
         ctx->tv.clear();
         ctx->hs.clear();
         ctx->pyrlk.clear();
@@ -677,13 +690,18 @@ oflow_status oflow_net_create(oflow_ctx *ctx, int width, int height, int batch, 
         std::unique_ptr<oflow_net> n(new oflow_net());
         n->ctx = ctx;
         n->net.reset(new WarmNet(width, height, batch));
+        ctx->nets.push_back(n.get());
         *out = n.release();
     });
 }
 
 oflow_status oflow_net_destroy(oflow_net *net) {
     if (!net) return OFLOW_ERR_BAD_ARG;
-    cudaStreamSynchronize(net->ctx->stream());
+    if (net->ctx) {  // null once its context was destroyed
+        cudaStreamSynchronize(net->ctx->stream());
+        auto &v = net->ctx->nets;
+        v.erase(std::remove(v.begin(), v.end(), net), v.end());
+    }
     delete net;
     return OFLOW_OK;
 }
@@ -696,18 +714,18 @@ oflow_status oflow_net_out_size(const oflow_net *net, int *w, int *h) {
 }
 
 oflow_status oflow_net_set_params(oflow_net *net, const float *params) {
-    if (!net || !params) return OFLOW_ERR_BAD_ARG;
+    if (!net || !net->ctx || !params) return OFLOW_ERR_BAD_ARG;
     return guard(net->ctx, [&] { net->net->set_params(params, net->ctx->stream()); });
 }
 
 oflow_status oflow_net_get_params(oflow_net *net, float *params) {
-    if (!net || !params) return OFLOW_ERR_BAD_ARG;
+    if (!net || !net->ctx || !params) return OFLOW_ERR_BAD_ARG;
     return guard(net->ctx, [&] { net->net->get_params(params, net->ctx->stream()); });
 }
 
 oflow_status oflow_net_train_step(oflow_net *net, const void *frames, int dtype,
                                   const float *target, float lr, double *loss) {
-    if (!net || !frames || !target) return OFLOW_ERR_BAD_ARG;
+    if (!net || !net->ctx || !frames || !target) return OFLOW_ERR_BAD_ARG;
     return guard(net->ctx, [&] {
         OF_CHECK(dtype == OFLOW_U8 || dtype == OFLOW_F32, "net: bad dtype");
         const size_t ps = (size_t)net->net->width() * net->net->height();
@@ -717,7 +735,7 @@ oflow_status oflow_net_train_step(oflow_net *net, const void *frames, int dtype,
 }
 
 oflow_status oflow_net_predict(oflow_net *net, const void *frames, int dtype, float *flow) {
-    if (!net || !frames || !flow) return OFLOW_ERR_BAD_ARG;
+    if (!net || !net->ctx || !frames || !flow) return OFLOW_ERR_BAD_ARG;
     return guard(net->ctx, [&] {
         OF_CHECK(dtype == OFLOW_U8 || dtype == OFLOW_F32, "net: bad dtype");
         const cudaStream_t st = net->ctx->stream();
@@ -736,6 +754,7 @@ oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_
                              oflow_tvl1_stats *stats) {
     return guard(ctx, [&] {
         OF_CHECK(ctx != nullptr && net != nullptr && I0 && I1 && out, "tvl1 warm: null argument");
+        OF_CHECK(net->ctx != nullptr, "tvl1 warm: the network's context was destroyed");
         OF_CHECK(n == net->net->batch(), "tvl1 warm: n must equal the network batch");
         check_tvl1_params(warm);
         if (plain) check_tvl1_params(plain);
@@ -843,16 +862,24 @@ oflow_status oflow_stream_create(oflow_ctx *ctx, const oflow_stream_desc *desc, 
         OF_CUDA(cudaEventCreateWithFlags(&s->uploaded, cudaEventDisableTiming));
         for (cudaEvent_t &e : s->done) OF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     });
-    if (st == OFLOW_OK) *out = s.release();
+    if (st == OFLOW_OK) {
+        ctx->streams.push_back(s.get());
+        *out = s.release();
+    }
     return st;
 }
 
 oflow_status oflow_stream_destroy(oflow_stream *s) {
     if (!s) return OFLOW_OK;
-    const oflow_status st = guard(s->ctx, [&] {
-        OF_CUDA(cudaStreamSynchronize(s->copy));
-        OF_CUDA(cudaStreamSynchronize(s->ctx->stream()));
-    });
+    oflow_status st = OFLOW_OK;
+    if (s->ctx) {  // null once its context was destroyed
+        st = guard(s->ctx, [&] {
+            OF_CUDA(cudaStreamSynchronize(s->copy));
+            OF_CUDA(cudaStreamSynchronize(s->ctx->stream()));
+        });
+        auto &v = s->ctx->streams;
+        v.erase(std::remove(v.begin(), v.end(), s), v.end());
+    }
     delete s;
     return st;
 }
@@ -861,7 +888,7 @@ long long oflow_stream_frames(const oflow_stream *s) { return s ? s->frames : -1
 
 oflow_status oflow_stream_push(oflow_stream *s, const oflow_image *frames, const oflow_flow *out,
                                oflow_tvl1_stats *stats) {
-    if (!s) return OFLOW_ERR_BAD_ARG;
+    if (!s || !s->ctx) return OFLOW_ERR_BAD_ARG;
     return guard(s->ctx, [&] {
         const oflow_stream_desc &d = s->desc;
         OF_CHECK(frames != nullptr && out != nullptr, "stream: null arrays");
@@ -914,6 +941,15 @@ oflow_status oflow_stream_push(oflow_stream *s, const oflow_image *frames, const
         }
         s->frames++;
         finish(s->ctx, device_only);
+    });
+}
+
+oflow_status oflow_ctx_last_launches(oflow_ctx *ctx, long long *launches) {
+    return guard(ctx, [&] {
+        OF_CHECK(ctx != nullptr && launches != nullptr, "last_launches: null argument");
+        long long total = 0;
+        for (TvPlan *pl : ctx->last_tv) total += pl->device_launches(ctx->stream());
+        *launches = total;
     });
 }
 
@@ -1038,3 +1074,13 @@ oflow_status oflow_conv3x3(int mode, int N, int H, int W, int C, int K, int stri
 }
 
 }  // extern "C"
+
+static void detach_children(oflow_ctx *ctx) {
+    for (oflow_net *n : ctx->nets) n->ctx = nullptr;
+    for (oflow_stream *st : ctx->streams) {
+        cudaStreamSynchronize(st->copy);
+        st->ctx = nullptr;
+    }
+    ctx->nets.clear();
+    ctx->streams.clear();
+}

@@ -1334,7 +1334,10 @@ void TvPlan::true_energy(double *host_out, cudaStream_t st) {
 
 void TvPlan::run(cudaStream_t st) {
     upload_frames(st);
-    if (!graph_.ready()) graph_.capture(st, [&](cudaStream_t s) { record(s); });
+    if (!graph_.ready()) {
+        graph_.capture(st, [&](cudaStream_t s) { record(s); });
+        graph_launches_ = launches_;
+    }
     graph_.launch(st);
 }
 

@@ -85,6 +85,9 @@ class TvPlan {
     // Eager run with events around each warp / inner-iteration launch.
     void profile(cudaStream_t st, oflow_tvl1_profile *out);
     int launches() const { return launches_; }
+    // kernel launches of one graph replay (run()): the fixed schedule, whose
+    // launches after every pair of a warp stage stopped return at once
+    long long device_launches(cudaStream_t) const { return graph_launches_; }
     void read_energy_trace(int b, double *dst, cudaStream_t st) const;
 
     int width() const { return w_; }
@@ -127,6 +130,7 @@ class TvPlan {
            o_Uz_ = 0, o_P0_ = 0, o_P1_ = 0, o_out_ = 0, o_ctrl_ = 0, o_part_ = 0, o_recs_ = 0,
            o_iters_ = 0, o_energy_ = 0;
     Graph graph_;
+    int graph_launches_ = 0;
     std::vector<FrameRef> frames_;  // [B][2], host copy of the device table
     size_t o_frames_ = 0;
     void upload_frames(cudaStream_t st);

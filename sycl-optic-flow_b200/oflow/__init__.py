@@ -104,6 +104,12 @@ class Context:
     def trim(self):
         _check(lib().oflow_ctx_trim(self._h), self._h)
 
+    def last_launches(self) -> int:
+        """Kernel launches the last tvl1 / tvl1_batch call executed on the device."""
+        n = C.c_longlong()
+        _check(lib().oflow_ctx_last_launches(self.handle, C.byref(n)), self.handle)
+        return n.value
+
     def save_tuning(self, path: str):
         _check(lib().oflow_ctx_save_tuning(self._h, os.fsencode(path)), self._h)
 

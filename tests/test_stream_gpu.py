@@ -76,3 +76,20 @@ def test_stream_rejects_wrong_frames(of):
         s.push([])
     s.close()
     ctx.close()
+
+
+def test_objects_outlive_their_context(of):
+    """A context destroyed before its network and stream leaves them inert:
+    using them is an error status, destroying them is safe."""
+    ctx = of.Context(0)
+    s = of.FrameStream(32, 24, "tvl1", lanes=1, params=of.TVL1Params(nscales=2, max_iterations=5),
+                       ctx=ctx)
+    net = of.WarmNet(64, 48, 1, ctx)
+    s.push([np.zeros((24, 32), np.uint8)])
+    ctx.close()
+    with pytest.raises(of.OflowError):
+        s.push([np.zeros((24, 32), np.uint8)])
+    with pytest.raises(of.OflowError):
+        net.set_params(np.zeros(of.net_num_params(), np.float32))
+    s.close()
+    net.close()

@@ -155,6 +155,21 @@ def test_device_frames_read_in_place_then_host_frames(of, orc, ctx):
     check(Bp, of.tvl1_batch(Bp, prm, ctx))
 
 
+def test_launch_count_of_the_schedule(of):
+    """oflow_ctx_last_launches reports the captured schedule: per warp stage
+    one warp launch and ceil(50/4)+1 inner-iteration launches, plus the
+    ingest, pyramid, gradient, zoom and output launches."""
+    ctx = of.Context(0)
+    pairs = [_pair(700 + i, 128, 96)[1:] for i in range(3)]
+    prm = of.TVL1Params(nscales=5, max_iterations=50)
+    _, st = of.tvl1_batch(pairs, prm, ctx, stats=True)
+    ns = st[0]["nscales"]
+    stages = ns * 5
+    n = ctx.last_launches()
+    assert stages * (1 + 14) < n < stages * (1 + 14) + 4 * ns + 8
+    ctx.close()
+
+
 def test_full_size_workload_against_oracle_and_reference(of, orc, ctx):
     """1024x436, 5 scales x 5 warps x 50 iterations (the benchmark workload)."""
     from oflow import synth
