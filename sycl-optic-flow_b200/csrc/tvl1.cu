@@ -78,7 +78,7 @@ void tvl1_zoom_size(int nx, int ny, int *nxx, int *nyy, float f) {
 
 // ---------------------------------------------------------------- device state
 struct TvCtrl {
-    int cur;            // ping-pong index of the current (U, P)
+    int cur;            // state buffer holding the accepted (U, P)
     int n;              // inner iterations done in the current warp
     int stop;           // current warp finished
     unsigned arrive;    // arrival counter of the last-block reduction
@@ -86,8 +86,16 @@ struct TvCtrl {
     int norm_apply;
     int redo;           // >0: the next launch re-runs this many iterations (early stop mid-block)
     double energy;
-    double pad1[3];
+    float last_err;     // error of the last accepted iteration of this warp (inf at its start)
+    float decay;        // last_err over the error of the iteration before it
+    double pad1[2];
 };
+
+// Snapshots are written in a launch when the error, extrapolated K
+// iterations ahead with the last iteration's decay ratio, comes within this
+// factor of the threshold (a stop inside the launch is plausible); elsewhere a
+// stop inside a launch falls back to re-running its iterations.
+constexpr float kSnapMargin = 2.0f;
 
 struct NormRec {  // |x|, first index, signed value
     float a;
@@ -101,6 +109,16 @@ __device__ __forceinline__ bool better_max(const NormRec &a, const NormRec &b) {
 }
 __device__ __forceinline__ bool better_min(const NormRec &a, const NormRec &b) {
     return a.a < b.a || (a.a == b.a && a.idx < b.idx);
+}
+
+// The flow state lives in kStateBufs consecutive buffers per quantity (b0 is
+// buffer 0, b1 buffer 1, and buffer k starts k*(b1-b0) after b0): 0 and 1
+// alternate as the accepted state; 2..4 and 5..7 are two sets of snapshots
+// the blocked kernel writes after its first K-1 iterations.  ctrl.cur names
+// the buffer that holds the accepted state.
+constexpr int kStateBufs = 2 + 2 * (kTbK - 1);
+template <typename T> __device__ __forceinline__ T *state_buf(T *b0, T *b1, int k) {
+    return b0 + (ptrdiff_t)k * (b1 - b0);
 }
 
 // ---------------------------------------------------------------- ingest
@@ -284,7 +302,7 @@ __global__ void k_zoom_flow(const float2 *U0, const float2 *U1, size_t stride, i
     const int i = blockIdx.y * blockDim.y + threadIdx.y;
     const int b = blockIdx.z;
     if (j >= nxx || i >= nyy) return;
-    const float2 *U = (ctrl[b].cur ? U1 : U0) + (size_t)b * stride;
+    const float2 *U = state_buf(U0, U1, ctrl[b].cur) + (size_t)b * stride;
     const float i2 = (float)i / fy, j2 = (float)j / fx;
     BicubicStencil s;
     bicubic_stencil(j2, i2, nx, ny, false, s);
@@ -340,11 +358,13 @@ __global__ void k_warp(const float *__restrict__ pyr, size_t pyr_stride, const f
         ctrl[b].stop = 0;
         ctrl[b].arrive = 0;
         ctrl[b].redo = 0;
+        ctrl[b].last_err = INFINITY;
+        ctrl[b].decay = 1.0f;
     }
     if (x >= nx || y >= ny) return;
     const int cur = ctrl[b].cur;
     const size_t off = (size_t)b * stride, p = (size_t)y * nx + x;
-    float2 *U = (cur ? U1 : U0) + off;
+    float2 *U = state_buf(U0, U1, cur) + off;
     float2 u;
     if (mode == kWarpFromU) {
         u = U[p];
@@ -355,7 +375,7 @@ __global__ void k_warp(const float *__restrict__ pyr, size_t pyr_stride, const f
         u = make_float2(0.0f, 0.0f);
         U[p] = u;
     }
-    if (first_warp) ((cur ? P1 : P0) + off)[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (first_warp) (state_buf(P0, P1, cur) + off)[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     const float uu = (float)x + u.x, vv = (float)y + u.y;
     float Iw = 0.0f, Iwx = 0.0f, Iwy = 0.0f;
     BicubicStencil s;
@@ -472,10 +492,10 @@ __global__ void __launch_bounds__(NT) k_tvl1_iter(IterArgs a) {
     const int cur = *((volatile int *)&ctrl->cur);
     const int nx = a.nx, ny = a.ny;
     const size_t off = (size_t)b * a.stride;
-    const float2 *__restrict__ Uin = (cur ? a.U1 : a.U0) + off;
-    float2 *__restrict__ Uout = (cur ? a.U0 : a.U1) + off;
-    const float4 *__restrict__ Pin = (cur ? a.P1 : a.P0) + off;
-    float4 *__restrict__ Pout = (cur ? a.P0 : a.P1) + off;
+    const float2 *__restrict__ Uin = state_buf(a.U0, a.U1, cur) + off;
+    float2 *__restrict__ Uout = state_buf(a.U0, a.U1, cur ^ 1) + off;
+    const float4 *__restrict__ Pin = state_buf(a.P0, a.P1, cur) + off;
+    float4 *__restrict__ Pout = state_buf(a.P0, a.P1, cur ^ 1) + off;
     const float2 *__restrict__ Wxy = a.Wxy + off;
     const float *__restrict__ Rc = a.Rc + off;
     const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
@@ -570,9 +590,10 @@ __global__ void __launch_bounds__(NT) k_tvl1_iter(IterArgs a) {
 // is loaded once and stored once per launch, so HBM traffic per iteration
 // drops by about K.  Each iteration's squared change over the owned pixels is
 // kept; the last block of a pair finds the first iteration that meets the
-// stopping rule (tvl1.cpp:216).  If that is not the last iteration of the
-// launch, nothing is accepted and the next launch re-runs exactly that many
-// iterations from the untouched input buffers.
+// stopping rule (tvl1.cpp:216).  When a stop is plausible (kSnapMargin), the
+// owned tile is also stored after each of the first K-1 iterations into a
+// snapshot buffer, so a stop in the middle of the launch accepts that
+// iteration's state; otherwise the next launch re-runs those iterations.
 struct TbArgs {
     const float2 *Wxy;
     const float *Rc;
@@ -658,15 +679,16 @@ __device__ __forceinline__ void tb_iteration(int j, float4 *sP, const float2 *sW
 
 // Per-iteration error sums of one block into its partial slots, then the
 // stopping decision by the last block of the pair to arrive: it finds the
-// first of the kk iterations meeting the stopping rule (tvl1.cpp:216).  If
-// that is the last one (or none does), the launch's state is accepted;
-// otherwise `redo` makes the next launch re-run exactly that many iterations
-// from the untouched input buffers.  Partials are summed in a fixed order, so
-// the decision does not depend on block scheduling.
+// first of the kk iterations meeting the stopping rule (tvl1.cpp:216) and
+// accepts the state after that iteration -- the final buffer, or the snapshot
+// written after it (snap >= 0).  Without a snapshot, `redo` makes the next
+// launch re-run exactly that many iterations from the untouched input.  The
+// result is that of one iteration per launch either way.  Partials are summed
+// in a fixed order, so the decision does not depend on block scheduling.
 template <int K, int NT>
 __device__ __forceinline__ void tb_decide(const TbArgs &a, TvCtrl *ctrl, int b,
-                                          const double (&err)[K], int kk, int redo, int cur,
-                                          int n0) {
+                                          const double (&err)[K], int kk, int fin, int snap,
+                                          int redo, int n0) {
     __shared__ double sred[NT / 32];
     __shared__ double sE[K];
     __shared__ int s_last;
@@ -698,16 +720,19 @@ __device__ __forceinline__ void tb_decide(const TbArgs &a, TvCtrl *ctrl, int b,
     }
     if (threadIdx.x == 0) {
         const float npx = (float)(a.nx * a.ny);
-        if (redo > 0) {
+        if (redo > 0) {  // the re-run ends exactly at the stopping iteration
             ctrl->n = n0 + redo;
-            ctrl->cur = cur ^ 1;
+            ctrl->cur = fin;
             ctrl->stop = 1;
             ctrl->redo = 0;
         } else {
             int stopj = 0;
+            float e_last = INFINITY, e_prev = INFINITY;
             for (int j = 0; j < kk; j++) {
                 float e = (float)sE[j];
                 e = e / npx;
+                e_prev = e_last;
+                e_last = e;
                 if (!(e > a.eps2) || n0 + j + 1 >= a.max_it) {
                     stopj = j + 1;
                     break;
@@ -715,10 +740,17 @@ __device__ __forceinline__ void tb_decide(const TbArgs &a, TvCtrl *ctrl, int b,
             }
             if (stopj == 0 || stopj == kk) {
                 ctrl->n = n0 + kk;
-                ctrl->cur = cur ^ 1;
+                ctrl->cur = fin;
+                ctrl->last_err = e_last;
+                ctrl->decay = (e_prev > 0.0f && e_prev < INFINITY) ? e_last / e_prev : 1.0f;
                 if (stopj) ctrl->stop = 1;
+            } else if (snap >= 0) {
+                // a stop after iteration stopj < kk accepts that iteration's snapshot
+                ctrl->n = n0 + stopj;
+                ctrl->cur = snap + stopj - 1;
+                ctrl->stop = 1;
             } else {
-                ctrl->redo = stopj;
+                ctrl->redo = stopj;  // no snapshot: re-run stopj iterations next launch
             }
         }
         a.iters[(size_t)b * a.iter_stride + a.stage] = ctrl->n;
@@ -728,7 +760,7 @@ __device__ __forceinline__ void tb_decide(const TbArgs &a, TvCtrl *ctrl, int b,
 }
 
 template <int TW, int TH, int K, int NT>
-__global__ void __launch_bounds__(NT) k_tvl1_tb(TbArgs a) {
+__global__ void __launch_bounds__(NT, 2) k_tvl1_tb(TbArgs a) {
     constexpr int RW = TW + 2 * K, RH = TH + 2 * K, RN = RW * RH;
     extern __shared__ float4 tb_smem[];
     float4 *sP = tb_smem;                                  // RN
@@ -740,15 +772,25 @@ __global__ void __launch_bounds__(NT) k_tvl1_tb(TbArgs a) {
     TvCtrl *ctrl = a.ctrl + b;
     if (*((volatile int *)&ctrl->stop)) return;
     const int cur = *((volatile int *)&ctrl->cur);
-    const int redo = *((volatile int *)&ctrl->redo);
     const int n0 = *((volatile int *)&ctrl->n);
+    const int redo = *((volatile int *)&ctrl->redo);
     const int kk = redo > 0 ? redo : imin(K, a.max_it - n0);
+    // block-uniform: every block of the pair reads the same control block
+    bool snaps = false;
+    if (redo == 0) {
+        const float q = fminf(*((volatile float *)&ctrl->decay), 1.0f), q2 = q * q;
+        snaps = *((volatile float *)&ctrl->last_err) * (q2 * q2) < kSnapMargin * a.eps2;
+    }
     const int nx = a.nx, ny = a.ny;
     const size_t off = (size_t)b * a.stride;
-    const float2 *__restrict__ Uin = (cur ? a.U1 : a.U0) + off;
-    float2 *__restrict__ Uout = (cur ? a.U0 : a.U1) + off;
-    const float4 *__restrict__ Pin = (cur ? a.P1 : a.P0) + off;
-    float4 *__restrict__ Pout = (cur ? a.P0 : a.P1) + off;
+    // accepted state in, final state to the other of buffers 0/1, snapshots
+    // after iterations 1..K-1 to the snapshot set not containing the input
+    const int fin = cur == 0 ? 1 : 0;
+    const int snap = (cur >= 2 && cur < 2 + (K - 1)) ? 2 + (K - 1) : 2;
+    const float2 *__restrict__ Uin = state_buf(a.U0, a.U1, cur) + off;
+    float2 *__restrict__ Uout = state_buf(a.U0, a.U1, fin) + off;
+    const float4 *__restrict__ Pin = state_buf(a.P0, a.P1, cur) + off;
+    float4 *__restrict__ Pout = state_buf(a.P0, a.P1, fin) + off;
     const float2 *__restrict__ Wg = a.Wxy + off;
     const float *__restrict__ Rg = a.Rc + off;
     const int ox = blockIdx.x * TW - K, oy = blockIdx.y * TH - K;
@@ -774,6 +816,18 @@ __global__ void __launch_bounds__(NT) k_tvl1_tb(TbArgs a) {
     }
     __syncthreads();
 
+    // the owned tile is exact after every iteration: store it
+    auto store_owned = [&](float2 *__restrict__ Ud, float4 *__restrict__ Pd) {
+        for (int i = threadIdx.x; i < TW * TH; i += NT) {
+            const int tx = i % TW, ty = i / TW;
+            const int x = ox + K + tx, y = oy + K + ty;
+            if (x >= nx || y >= ny) continue;
+            const int r = (ty + K) * RW + tx + K;
+            const size_t q = (size_t)y * nx + x;
+            Ud[q] = sU[r];
+            Pd[q] = sP[r];
+        }
+    };
     double err[K];
 #pragma unroll
     for (int j = 0; j < K; j++) {
@@ -785,19 +839,13 @@ __global__ void __launch_bounds__(NT) k_tvl1_tb(TbArgs a) {
             else
                 tb_iteration<TW, TH, K, NT, false>(j + 1, sP, sW, sR, sU, ox, oy, nx, ny, a.l_t,
                                                    a.theta, a.taut, err[j]);
+            if (snaps && j + 1 < kk)  // snapshot: the state a stop after iteration j+1 accepts
+                store_owned(state_buf(a.U0, a.U1, snap + j) + off, state_buf(a.P0, a.P1, snap + j) + off);
         }
     }
-    for (int i = threadIdx.x; i < TW * TH; i += NT) {
-        const int tx = i % TW, ty = i / TW;
-        const int x = ox + K + tx, y = oy + K + ty;
-        if (x >= nx || y >= ny) continue;
-        const int r = (ty + K) * RW + tx + K;
-        const size_t q = (size_t)y * nx + x;
-        Uout[q] = sU[r];
-        Pout[q] = sP[r];
-    }
+    store_owned(Uout, Pout);
 
-    tb_decide<K, NT>(a, ctrl, b, err, kk, redo, cur, n0);
+    tb_decide<K, NT>(a, ctrl, b, err, kk, fin, snaps ? snap : -1, redo, n0);
 }
 
 // ---------------------------------------------------------------- energy
@@ -814,7 +862,7 @@ __global__ void __launch_bounds__(kEnNT) k_energy(const float2 *Wxy, const float
                                                   int expect_n) {
     const int b = blockIdx.y;
     const size_t off = (size_t)b * stride;
-    const float2 *U = (ctrl[b].cur ? U1 : U0) + off;
+    const float2 *U = state_buf(U0, U1, ctrl[b].cur) + off;
     const int N = nx * ny;
     double tv = 0.0, data = 0.0;
     for (int i = blockIdx.x * kEnNT + threadIdx.x; i < N; i += gridDim.x * kEnNT) {
@@ -865,7 +913,7 @@ __global__ void __launch_bounds__(kEnNT) k_energy_true(const float *__restrict__
                                                        double *partials, int max_blocks,
                                                        unsigned *arrive, double *out) {
     const int b = blockIdx.y;
-    const float2 *U = (ctrl[b].cur ? U1 : U0) + (size_t)b * stride;
+    const float2 *U = state_buf(U0, U1, ctrl[b].cur) + (size_t)b * stride;
     const float *I0 = pyr + (size_t)(2 * b) * lp;
     const float *I1 = pyr + (size_t)(2 * b + 1) * lp;
     const int N = nx * ny;
@@ -905,7 +953,7 @@ __global__ void __launch_bounds__(kEnNT) k_energy_true(const float *__restrict__
 __global__ void k_split(const float2 *U0, const float2 *U1, size_t stride, int N, float *ou,
                         float *ov, const TvCtrl *ctrl) {
     const int b = blockIdx.y;
-    const float2 *U = (ctrl[b].cur ? U1 : U0) + (size_t)b * stride;
+    const float2 *U = state_buf(U0, U1, ctrl[b].cur) + (size_t)b * stride;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
         const float2 u = U[i];
         ou[(size_t)b * stride + i] = u.x;
@@ -1017,11 +1065,9 @@ TvPlan::TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, boo
     o_I1g_ = ar_.reserve(B * N0 * 16);
     o_Wxy_ = ar_.reserve(B * N0 * 8);
     o_Rc_ = ar_.reserve(B * N0 * 4);
-    o_U0_ = ar_.reserve(B * N0 * 8);
-    o_U1_ = ar_.reserve(B * N0 * 8);
+    o_U0_ = ar_.reserve(kStateBufs * B * N0 * 8);  // buffer k at U0 + k*B*N0
     o_Uz_ = ar_.reserve(B * N0 * 8);
-    o_P0_ = ar_.reserve(B * N0 * 16);
-    o_P1_ = ar_.reserve(B * N0 * 16);
+    o_P0_ = ar_.reserve(kStateBufs * B * N0 * 16);
     o_out_ = ar_.reserve(2 * B * N0 * 4);
     o_ctrl_ = ar_.reserve(B * sizeof(TvCtrl));
     o_part_ = ar_.reserve((size_t)B * max_blocks_ * 8);
@@ -1063,6 +1109,9 @@ void *TvPlan::raw_input(int b, int k) const {
     const size_t esz = dtype_ == OFLOW_U8 ? 1 : 4;
     return ar_.at<char>(o_raw_) + (size_t)(2 * b + k) * N0_ * esz;
 }
+float2 *TvPlan::ubuf(int k) const { return ar_.at<float2>(o_U0_) + (size_t)k * B_ * N0_; }
+float4 *TvPlan::pbuf(int k) const { return ar_.at<float4>(o_P0_) + (size_t)k * B_ * N0_; }
+
 const float *TvPlan::out_u(int b) const { return ar_.at<float>(o_out_) + (size_t)b * N0_; }
 const float *TvPlan::out_v(int b) const { return ar_.at<float>(o_out_) + (size_t)(B_ + b) * N0_; }
 const int *TvPlan::iters_dev() const { return ar_.at<int>(o_iters_); }
@@ -1070,6 +1119,7 @@ float2 *TvPlan::uz() const { return ar_.at<float2>(o_Uz_); }
 
 int TvPlan::iter_launches_per_stage() const {
     if (trace_) return prm_.max_iterations;
+    // ceil(max/K) launches plus one for a re-run after an unforeseen mid-launch stop
     return prm_.max_iterations > 0 ? div_up(prm_.max_iterations, kTbK) + 1 : 0;
 }
 
@@ -1082,8 +1132,8 @@ void TvPlan::record(cudaStream_t st) {
     float4 *I1g = ar_.at<float4>(o_I1g_);
     float2 *Wxy = ar_.at<float2>(o_Wxy_);
     float *Rc = ar_.at<float>(o_Rc_);
-    float2 *U0 = ar_.at<float2>(o_U0_), *U1 = ar_.at<float2>(o_U1_), *Uz = ar_.at<float2>(o_Uz_);
-    float4 *P0 = ar_.at<float4>(o_P0_), *P1 = ar_.at<float4>(o_P1_);
+    float2 *U0 = ubuf(0), *U1 = ubuf(1), *Uz = ar_.at<float2>(o_Uz_);
+    float4 *P0 = pbuf(0), *P1 = pbuf(1);
     TvCtrl *ctrl = ar_.at<TvCtrl>(o_ctrl_);
     double *part = ar_.at<double>(o_part_);
     NormRec *recs = ar_.at<NormRec>(o_recs_);
@@ -1284,8 +1334,8 @@ void TvPlan::autotune(cudaStream_t st, TuneTable *table, int reps) {
             float best = 1e30f;
             int best_c = tb_cfg_[s];
             for (int c = 0; c < kTbNumCfgs; c++) {
-                TbArgs ta{ar_.at<float2>(o_Wxy_), ar_.at<float>(o_Rc_), ar_.at<float2>(o_U0_),
-                          ar_.at<float2>(o_U1_), ar_.at<float4>(o_P0_), ar_.at<float4>(o_P1_), N0,
+                TbArgs ta{ar_.at<float2>(o_Wxy_), ar_.at<float>(o_Rc_), ubuf(0), ubuf(1), pbuf(0),
+                          pbuf(1), N0,
                           nx, ny, 1 << 30, l_t, prm_.theta, taut, -1.0f, ctrl,
                           ar_.at<double>(o_part_), max_blocks_ / kTbK, ar_.at<int>(o_iters_),
                           iter_stride_, 0};
@@ -1324,7 +1374,7 @@ void TvPlan::true_energy(double *host_out, cudaStream_t st) {
     double *out = ar_.at<double>(o_tout_);
     OF_CUDA(cudaMemsetAsync(arrive, 0, sizeof(unsigned) * B_, st));
     k_energy_true<<<dim3(energy_blocks_, B_), kEnNT, 0, st>>>(
-        ar_.at<float>(o_pyr_) + pyr_off_[0], N0_, ar_.at<float2>(o_U0_), ar_.at<float2>(o_U1_), N0_,
+        ar_.at<float>(o_pyr_) + pyr_off_[0], N0_, ubuf(0), ubuf(1), N0_,
         w_, h_, prm_.lambda, ar_.at<TvCtrl>(o_ctrl_), ar_.at<double>(o_part_), max_blocks_,
         arrive, out);
     OF_CUDA(cudaGetLastError());

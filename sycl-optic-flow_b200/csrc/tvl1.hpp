@@ -126,9 +126,10 @@ class TvPlan {
     size_t o_tarr_ = 0, o_tout_ = 0;
     int iter_launches_per_stage() const;
     size_t o_Wxy_ = 0, o_Rc_ = 0;
-    size_t o_raw_ = 0, o_T_ = 0, o_pyr_ = 0, o_I1g_ = 0, o_U0_ = 0, o_U1_ = 0,
-           o_Uz_ = 0, o_P0_ = 0, o_P1_ = 0, o_out_ = 0, o_ctrl_ = 0, o_part_ = 0, o_recs_ = 0,
-           o_iters_ = 0, o_energy_ = 0;
+    size_t o_raw_ = 0, o_T_ = 0, o_pyr_ = 0, o_I1g_ = 0, o_U0_ = 0, o_Uz_ = 0, o_P0_ = 0,
+           o_out_ = 0, o_ctrl_ = 0, o_part_ = 0, o_recs_ = 0, o_iters_ = 0, o_energy_ = 0;
+    float2 *ubuf(int k) const;  // state buffer k of u (all pairs)
+    float4 *pbuf(int k) const;  // state buffer k of p
     Graph graph_;
     int graph_launches_ = 0;
     std::vector<FrameRef> frames_;  // [B][2], host copy of the device table

@@ -157,7 +157,8 @@ def test_device_frames_read_in_place_then_host_frames(of, orc, ctx):
 
 def test_launch_count_of_the_schedule(of):
     """oflow_ctx_last_launches reports the captured schedule: per warp stage
-    one warp launch and ceil(50/4)+1 inner-iteration launches, plus the
+    one warp launch and ceil(50/4)+1 inner-iteration launches (one for a
+    re-run after a stop inside a launch that wrote no snapshots), plus the
     ingest, pyramid, gradient, zoom and output launches."""
     ctx = of.Context(0)
     pairs = [_pair(700 + i, 128, 96)[1:] for i in range(3)]
