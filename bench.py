@@ -278,6 +278,51 @@ def warm_measure(oflow, synth, np, torch, pairs, d_in, prm, ctx, stream, args, P
             "training": meta}
 
 
+def solver_measure(oflow, synth, np, torch, ctx, stream, dev, peak):
+    """Horn-Schunck on its 320x240 configuration (alpha 15, one level, one
+    warp, 200 Jacobi sweeps; 64 pairs per call) and pyramidal Lucas-Kanade on
+    its 640x480 configuration (3 levels x 3 refinements, 5x5 window; one pair
+    per call), device-resident, with EPE against the generators' ground truth.
+    Algorithmic bytes: HS 28 B/px per sweep plus 24 B/px for the warp and
+    derivatives; pyramidal LK 24 B/px per level-refinement."""
+    out = {}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, reps):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / reps
+
+    hp = oflow.HSParams(15.0, 1, 1, 200)
+    gen = [synth.hs_pair(seed=40_000 + i) for i in range(64)]
+    hs_in = [(torch.from_numpy(g.I0).to(dev), torch.from_numpy(g.I1).to(dev)) for g in gen]
+    hs_out = [(torch.empty((240, 320), device=dev), torch.empty((240, 320), device=dev)) for _ in gen]
+    t = timed(lambda: oflow.hs_batch(hs_in, hp, ctx, out=hs_out), 10)
+    per_pair = 320 * 240 * (200 * 28 + 24)
+    epe = float(np.mean([synth.epe(o[0].cpu().numpy(), o[1].cpu().numpy(), g.u, g.v, g.valid, 8)
+                         for o, g in zip(hs_out[:8], gen[:8])]))
+    out["hs_320x240"] = {"pairs_per_s": 64 / t, "achieved_gbs": 64 * per_pair / t / 1e9,
+                         "frac": 64 * per_pair / t / 1e9 / peak, "epe_vs_ground_truth": round(epe, 4),
+                         "config": "alpha 15, 1 level, 1 warp, 200 sweeps, 64 pairs per call"}
+    lp = oflow.LKParams(3, 2, 5, 3, 3)
+    g = synth.lk_pair(seed=41_000)
+    a, b = torch.from_numpy(g.I0).to(dev), torch.from_numpy(g.I1).to(dev)
+    lo = (torch.empty((480, 640), device=dev), torch.empty((480, 640), device=dev))
+    t = timed(lambda: oflow.pyrlk(a, b, lp, ctx, out=lo), 50)
+    per_pair = 3 * (640 * 480 + 320 * 240 + 160 * 120) * 24
+    epe = synth.epe(lo[0].cpu().numpy(), lo[1].cpu().numpy(), g.u, g.v, g.valid, 8)
+    out["pyrlk_640x480"] = {"pairs_per_s": 1 / t, "achieved_gbs": per_pair / t / 1e9,
+                            "frac": per_pair / t / 1e9 / peak, "epe_vs_ground_truth": round(float(epe), 4),
+                            "config": "3 levels x 3 refinements, 5x5 window, one pair per call"}
+    return out
+
+
 def our_arm(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -408,6 +453,9 @@ def our_arm(args, rank, world, local_rank):
              "frac": col_gbs / measured_peak()[0],
              "bytes_basis": "8 B in (u, v) + 3 B out (B, G, R) per pixel", "batch": P}
 
+    # --- the other two solvers on their configurations (device-resident)
+    solvers = solver_measure(oflow, synth, np, torch, ctx, stream, dev, measured_peak()[0])
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.cpu_pairs, args.cpu_seconds)
@@ -455,6 +503,7 @@ def our_arm(args, rank, world, local_rank):
         warm["speedup_vs_plain"] = warm["value"] / value
         line["warm_start"] = warm
     line["flow_to_color"] = color
+    line["solvers"] = solvers
     print(json.dumps(line), flush=True)
     return 0
 
