@@ -303,13 +303,17 @@ def solver_measure(oflow, synth, np, torch, ctx, stream, dev, peak):
     gen = [synth.hs_pair(seed=40_000 + i) for i in range(64)]
     hs_in = [(torch.from_numpy(g.I0).to(dev), torch.from_numpy(g.I1).to(dev)) for g in gen]
     hs_out = [(torch.empty((240, 320), device=dev), torch.empty((240, 320), device=dev)) for _ in gen]
+    t_fixed = timed(lambda: oflow.hs_batch(hs_in, hp, ctx, out=hs_out), 10)
+    hs_cfg = oflow.hs_autotune(hs_in, hp, ctx)
     t = timed(lambda: oflow.hs_batch(hs_in, hp, ctx, out=hs_out), 10)
     per_pair = 320 * 240 * (200 * 28 + 24)
     epe = float(np.mean([synth.epe(o[0].cpu().numpy(), o[1].cpu().numpy(), g.u, g.v, g.valid, 8)
                          for o, g in zip(hs_out[:8], gen[:8])]))
     out["hs_320x240"] = {"pairs_per_s": 64 / t, "achieved_gbs": 64 * per_pair / t / 1e9,
                          "frac": 64 * per_pair / t / 1e9 / peak, "epe_vs_ground_truth": round(epe, 4),
-                         "config": "alpha 15, 1 level, 1 warp, 200 sweeps, 64 pairs per call"}
+                         "jacobi_config_per_level": hs_cfg,
+                         "pairs_per_s_untuned": 64 / t_fixed,
+                         "config": "alpha 15, 1 level, 1 warp, 200 sweeps, 64 pairs per call, autotuned"}
     lp = oflow.LKParams(3, 2, 5, 3, 3)
     g = synth.lk_pair(seed=41_000)
     a, b = torch.from_numpy(g.I0).to(dev), torch.from_numpy(g.I1).to(dev)
@@ -566,9 +570,11 @@ def batch_arm(args, rank, world, local_rank):
     ctx = oflow.Context(local_rank)
     stream = torch.cuda.current_stream(dev)
     ctx.set_stream(stream.cuda_stream)
-    for (solver, w, h), idx in groups.items():  # tile shapes per TV-L1 group (untimed)
+    for (solver, w, h), idx in groups.items():  # tile shapes per group (untimed)
         if solver == "tvl1":
             oflow.tvl1_autotune([frames[i] for i in idx], tp, ctx)
+        else:
+            oflow.hs_autotune([frames[i] for i in idx], hp, ctx)
     for _ in range(args.warmup):
         oflow.batch(jobs, ctx, out=outs)
     torch.cuda.synchronize()

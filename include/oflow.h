@@ -185,6 +185,18 @@ oflow_status oflow_hs(oflow_ctx *ctx, const oflow_image *I0, const oflow_image *
 oflow_status oflow_hs_batch(oflow_ctx *ctx, int n, const oflow_image *I0,
                             const oflow_image *I1, const oflow_hs_params *p,
                             const oflow_flow *out);
+/* Autotuner for Horn-Schunck: solves the n given pairs (one size) once, then
+ * times every Jacobi configuration (tile shape and sweeps per launch: 0 =
+ * 32x16 tiles with 4 sweeps, 1 = 32x16 with 8, 2 = 64x32 with 8, 3 = 64x16
+ * with 4, 4 = 32x32 with 16) at every pyramid level and keeps the fastest for
+ * plans of this level size and batch (table entries with solver "hs", saved and
+ * loaded with the TV-L1 ones).  cfg_per_level (OFLOW_MAX_SCALES ints, may be
+ * NULL) receives the choice per level (coarsest first), -1 past the last.
+ * Every configuration gives the same bits.  The reference has one fixed
+ * configuration and no tuner. */
+oflow_status oflow_hs_autotune(oflow_ctx *ctx, int n, const oflow_image *I0,
+                               const oflow_image *I1, const oflow_hs_params *p,
+                               int *cfg_per_level);
 
 /* Horn-Schunck for callers that cannot allocate device memory: code running
  * while a CUDA graph is captured, real-time frame loops that cannot afford the

@@ -455,7 +455,8 @@ oflow_status oflow_batch(oflow_ctx *ctx, int n, const oflow_job *jobs) {
                                                   false, &ctx->tune));
                 } else {
                     m->slot.push_back((int)m->hs.size());
-                    m->hs.emplace_back(new HsPlan(j.I0.width, j.I0.height, B, j.I0.dtype, *j.hs));
+                    m->hs.emplace_back(new HsPlan(j.I0.width, j.I0.height, B, j.I0.dtype, *j.hs,
+                                                  &ctx->tune));
                 }
                 cudaStream_t s;
                 OF_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
@@ -560,6 +561,18 @@ void oflow_hs_default_params(oflow_hs_params *p) {
     p->nsolver = 150;
 }
 
+// cached Horn-Schunck plan of this size, batch, dtype and parameters
+static HsPlan &hs_plan(oflow_ctx *ctx, int w, int h, int B, int dtype, const oflow_hs_params &p) {
+    for (auto &q : ctx->hs)
+        if (q->width() == w && q->height() == h && q->batch() == B && q->dtype() == dtype &&
+            same(q->params(), p))
+            return *q;
+    ctx->hs.emplace_back(new HsPlan(w, h, B, dtype, p, &ctx->tune));
+    HsPlan *pl = ctx->hs.back().get();
+    keep_recent(ctx->hs);
+    return *pl;
+}
+
 oflow_status oflow_hs_batch(oflow_ctx *ctx, int n, const oflow_image *I0,
                             const oflow_image *I1, const oflow_hs_params *p,
                             const oflow_flow *out) {
@@ -570,17 +583,7 @@ oflow_status oflow_hs_batch(oflow_ctx *ctx, int n, const oflow_image *I0,
         const cudaStream_t st = ctx->stream();
         bool device_only = true;
         for (const Group &g : group_pairs(n, I0, I1)) {
-            HsPlan *pl = nullptr;
-            for (auto &q : ctx->hs)
-                if (q->width() == g.w && q->height() == g.h && q->batch() == (int)g.idx.size() &&
-                    q->dtype() == g.dtype && same(q->params(), *p))
-                    pl = q.get();
-            if (!pl) {
-                ctx->hs.emplace_back(new HsPlan(g.w, g.h, (int)g.idx.size(), g.dtype, *p));
-                pl = ctx->hs.back().get();
-                keep_recent(ctx->hs);
-                pl = ctx->hs.back().get();
-            }
+            HsPlan *pl = &hs_plan(ctx, g.w, g.h, (int)g.idx.size(), g.dtype, *p);
             for (size_t b = 0; b < g.idx.size(); b++) {
                 stage_image(I0[g.idx[b]], pl->raw_input((int)b, 0), dtype_size(g.dtype), st);
                 stage_image(I1[g.idx[b]], pl->raw_input((int)b, 1), dtype_size(g.dtype), st);
@@ -600,6 +603,30 @@ oflow_status oflow_hs_batch(oflow_ctx *ctx, int n, const oflow_image *I0,
 oflow_status oflow_hs(oflow_ctx *ctx, const oflow_image *I0, const oflow_image *I1,
                       const oflow_hs_params *p, const oflow_flow *out) {
     return oflow_hs_batch(ctx, 1, I0, I1, p, out);
+}
+
+oflow_status oflow_hs_autotune(oflow_ctx *ctx, int n, const oflow_image *I0,
+                               const oflow_image *I1, const oflow_hs_params *p,
+                               int *cfg_per_level) {
+    return guard(ctx, [&] {
+        OF_CHECK(ctx != nullptr, "null context");
+        OF_CHECK(n >= 1 && I0 && I1 && p, "hs autotune: empty batch or null arrays");
+        const std::vector<Group> groups = group_pairs(n, I0, I1);
+        OF_CHECK(groups.size() == 1, "hs autotune: pairs must share one size");
+        const Group &g = groups[0];
+        const cudaStream_t st = ctx->stream();
+        HsPlan &pl = hs_plan(ctx, g.w, g.h, n, g.dtype, *p);
+        for (int b = 0; b < n; b++) {
+            stage_image(I0[g.idx[b]], pl.raw_input(b, 0), dtype_size(g.dtype), st);
+            stage_image(I1[g.idx[b]], pl.raw_input(b, 1), dtype_size(g.dtype), st);
+        }
+        pl.run(st);
+        pl.autotune(st, &ctx->tune);
+        OF_CUDA(cudaStreamSynchronize(st));
+        if (cfg_per_level)
+            for (int l = 0; l < OFLOW_MAX_SCALES; l++)
+                cfg_per_level[l] = l < pl.levels() ? pl.jacobi_config(l) : -1;
+    });
 }
 
 void oflow_lk_default_params(oflow_lk_params *p) {
@@ -854,7 +881,8 @@ oflow_status oflow_stream_create(oflow_ctx *ctx, const oflow_stream_desc *desc, 
             s->tv.reset(new TvPlan(desc->width, desc->height, desc->lanes, desc->dtype, desc->tvl1, false,
                                    &ctx->tune));
         } else {
-            s->hs.reset(new HsPlan(desc->width, desc->height, desc->lanes, desc->dtype, desc->hs));
+            s->hs.reset(new HsPlan(desc->width, desc->height, desc->lanes, desc->dtype, desc->hs,
+                                   &ctx->tune));
         }
         s->slots.alloc(3 * (size_t)desc->lanes * s->frame_bytes());
         OF_CUDA(cudaMemset(s->slots.as<char>(), 0, s->slots.bytes()));

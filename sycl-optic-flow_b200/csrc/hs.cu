@@ -218,7 +218,61 @@ void launch_split2(const float2 *U, size_t stride, int N, float *out, int B, cud
 // ================================================================ host plan
 constexpr int kJTW = 32, kJTH = 16, kJK = 4, kJNT = 256;
 
-HsPlan::HsPlan(int w, int h, int B, int dtype, const oflow_hs_params &prm)
+// Jacobi configurations: tile tw x th, up to k sweeps per launch (halo k),
+// nt threads; 32 B of shared memory per region pixel (D 16, two u buffers).
+struct HsJCfg {
+    int tw, th, k, nt;
+};
+constexpr HsJCfg kHsCfgs[] = {{32, 16, 4, 256}, {32, 16, 8, 256}, {64, 32, 8, 512},
+                              {64, 16, 4, 256}, {32, 32, 16, 512}};
+constexpr int kHsNumCfgs = 5;
+constexpr size_t hs_smem(const HsJCfg &c) { return (size_t)(c.tw + 2 * c.k) * (c.th + 2 * c.k) * 32; }
+
+template <int TW, int TH, int KH, int NT>
+static void hs_jacobi_launch(dim3 g, cudaStream_t st, const float4 *D, size_t dstride,
+                             const float2 *in, float2 *out, float2 *U, size_t stride, int w,
+                             int h, int sweeps, int first, int last) {
+    const size_t smem = (size_t)(TW + 2 * KH) * (TH + 2 * KH) * 32;
+    k_hs_jacobi<TW, TH, KH, NT><<<g, NT, smem, st>>>(D, dstride, in, out, U, stride, w, h, sweeps,
+                                                     first, last);
+}
+
+static void hs_jacobi_cfg(int c, dim3 g, cudaStream_t st, const float4 *D, size_t dstride,
+                          const float2 *in, float2 *out, float2 *U, size_t stride, int w, int h,
+                          int sweeps, int first, int last) {
+    switch (c) {
+        case 1: hs_jacobi_launch<32, 16, 8, 256>(g, st, D, dstride, in, out, U, stride, w, h, sweeps, first, last); break;
+        case 2: hs_jacobi_launch<64, 32, 8, 512>(g, st, D, dstride, in, out, U, stride, w, h, sweeps, first, last); break;
+        case 3: hs_jacobi_launch<64, 16, 4, 256>(g, st, D, dstride, in, out, U, stride, w, h, sweeps, first, last); break;
+        case 4: hs_jacobi_launch<32, 32, 16, 512>(g, st, D, dstride, in, out, U, stride, w, h, sweeps, first, last); break;
+        default: hs_jacobi_launch<32, 16, 4, 256>(g, st, D, dstride, in, out, U, stride, w, h, sweeps, first, last); break;
+    }
+}
+
+static void hs_set_smem_attrs() {
+    OF_CUDA(cudaFuncSetAttribute(k_hs_jacobi<32, 16, 4, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)hs_smem(kHsCfgs[0])));
+    OF_CUDA(cudaFuncSetAttribute(k_hs_jacobi<32, 16, 8, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)hs_smem(kHsCfgs[1])));
+    OF_CUDA(cudaFuncSetAttribute(k_hs_jacobi<64, 32, 8, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)hs_smem(kHsCfgs[2])));
+    OF_CUDA(cudaFuncSetAttribute(k_hs_jacobi<64, 16, 4, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)hs_smem(kHsCfgs[3])));
+    OF_CUDA(cudaFuncSetAttribute(k_hs_jacobi<32, 32, 16, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)hs_smem(kHsCfgs[4])));
+}
+
+// OFLOW_HS_CFG forces one configuration (used to test and time them); else
+// configuration 0 unless the tuning table has the level
+static int hs_pick() {
+    if (const char *e = getenv("OFLOW_HS_CFG")) {
+        const int c = atoi(e);
+        if (c >= 0 && c < kHsNumCfgs) return c;
+    }
+    return 0;
+}
+
+HsPlan::HsPlan(int w, int h, int B, int dtype, const oflow_hs_params &prm, const TuneTable *tuned)
     : w_(w), h_(h), B_(B), dtype_(dtype), prm_(prm) {
     OF_CHECK(B >= 1, "hs: empty batch");
     OF_CHECK(prm.nlevels >= 1 && prm.nlevels <= 16, "hs: nlevels out of range");
@@ -247,9 +301,12 @@ HsPlan::HsPlan(int w, int h, int B, int dtype, const oflow_hs_params &prm)
     o_Ub_ = ar_.reserve(B * N_ * 8);
     o_out_ = ar_.reserve(2 * B * N_ * 4);
     ar_.commit();
-    OF_CUDA(cudaFuncSetAttribute(k_hs_jacobi<kJTW, kJTH, kJK, kJNT>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (kJTW + 2 * kJK) * (kJTH + 2 * kJK) * 32));
+    hs_set_smem_attrs();
+    for (int l = 0; l < L_; l++) {
+        const auto it = tuned ? tuned->find(tune_key(W_[l], H_[l], B, kTuneHs)) : TuneTable::const_iterator();
+        const bool ok = tuned && it != tuned->end() && it->second >= 0 && it->second < kHsNumCfgs;
+        jcfg_[l] = ok ? it->second : hs_pick();
+    }
 }
 
 void *HsPlan::raw_input(int b, int k) const {
@@ -282,22 +339,22 @@ void HsPlan::record(cudaStream_t st) {
     }
     int ub = 0;  // Ubuf index holding the flow of the current level
     OF_CUDA(cudaMemsetAsync(Ubuf[ub], 0, B * N_ * 8, st));
-    const size_t smem = (size_t)(kJTW + 2 * kJK) * (kJTH + 2 * kJK) * 32;
     for (int l = 0; l < L_; l++) {
+        const HsJCfg &jc = kHsCfgs[jcfg_[l]];
         const int lw = W_[l], lh = H_[l];
         const size_t lp = (size_t)lw * lh;
         for (int wi = 0; wi < prm_.nwarp; wi++) {
             dim3 dg(div_up(lw, kDTW), div_up(lh, kDTH), B);
             k_hs_warp_deriv<<<dg, dim3(kDTW, kDTH), 0, st>>>(pyr + pyr_off_[l], lp, lw, lh,
                                                              Ubuf[ub], N_, 0, prm_.alpha, D, N_);
-            dim3 jg(div_up(lw, kJTW), div_up(lh, kJTH), B);
+            dim3 jg(div_up(lw, jc.tw), div_up(lh, jc.th), B);
             int done = 0, cur = 0;
             if (prm_.nsolver == 0) continue;  // du = 0: the flow is unchanged
             while (done < prm_.nsolver) {
-                const int k = imin(kJK, prm_.nsolver - done);
+                const int k = imin(jc.k, prm_.nsolver - done);
                 const bool first = done == 0, last = done + k == prm_.nsolver;
-                k_hs_jacobi<kJTW, kJTH, kJK, kJNT><<<jg, kJNT, smem, st>>>(
-                    D, N_, dU[cur], dU[cur ^ 1], Ubuf[ub], N_, lw, lh, k, first, last);
+                hs_jacobi_cfg(jcfg_[l], jg, st, D, N_, dU[cur], dU[cur ^ 1], Ubuf[ub], N_, lw, lh, k,
+                              first, last);
                 cur ^= 1;
                 done += k;
             }
@@ -317,6 +374,61 @@ void HsPlan::record(cudaStream_t st) {
 void HsPlan::run(cudaStream_t st) {
     if (!graph_.ready()) graph_.capture(st, [&](cudaStream_t s) { record(s); });
     graph_.launch(st);
+}
+
+// Best of `reps` timed runs of 16 sweeps (in launches of the configuration's
+// depth) per configuration and level.  The sweep has no data-dependent control
+// flow, so the derivative buffer the last solve left is fine input at every
+// level size; the runs write only the du scratch, never the flow or outputs.
+void HsPlan::autotune(cudaStream_t st, TuneTable *table, int reps) {
+    float4 *D = ar_.at<float4>(o_D_);
+    float2 *dU[2] = {ar_.at<float2>(o_dU0_), ar_.at<float2>(o_dU1_)};
+    float2 *U = ar_.at<float2>(o_Ua_);
+    cudaEvent_t e0, e1;
+    OF_CUDA(cudaEventCreate(&e0));
+    OF_CUDA(cudaEventCreate(&e1));
+    constexpr int kSweeps = 16;
+    try {
+        for (int l = 0; l < L_; l++) {
+            const int lw = W_[l], lh = H_[l];
+            float best = 1e30f;
+            int best_c = jcfg_[l];
+            for (int c = 0; c < kHsNumCfgs; c++) {
+                const HsJCfg &jc = kHsCfgs[c];
+                dim3 jg(div_up(lw, jc.tw), div_up(lh, jc.th), B_);
+                float ms_min = 1e30f;
+                for (int r = 0; r <= reps; r++) {  // the first round warms up
+                    OF_CUDA(cudaEventRecord(e0, st));
+                    int done = 0, cur = 0;
+                    while (done < kSweeps) {
+                        const int k = imin(jc.k, kSweeps - done);
+                        hs_jacobi_cfg(c, jg, st, D, N_, dU[cur], dU[cur ^ 1], U, N_, lw, lh, k,
+                                      done == 0, 0);
+                        cur ^= 1;
+                        done += k;
+                    }
+                    OF_CUDA(cudaEventRecord(e1, st));
+                    OF_CUDA(cudaEventSynchronize(e1));
+                    float ms = 0.0f;
+                    OF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                    if (r > 0) ms_min = ms < ms_min ? ms : ms_min;
+                }
+                if (ms_min < best) {
+                    best = ms_min;
+                    best_c = c;
+                }
+            }
+            jcfg_[l] = best_c;
+            if (table) (*table)[tune_key(lw, lh, B_, kTuneHs)] = best_c;
+        }
+    } catch (...) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    graph_.reset();  // the next run captures the new configurations
 }
 
 // ================================================================ caller scratch

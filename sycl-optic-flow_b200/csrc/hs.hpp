@@ -2,17 +2,26 @@
 #pragma once
 
 #include "internal.hpp"
+#include "tvl1.hpp"
 
 namespace oflow {
 
 class HsPlan {
   public:
-    HsPlan(int w, int h, int B, int dtype, const oflow_hs_params &prm);
+    // tuned: per-level Jacobi configurations chosen by the autotuner (may be null)
+    HsPlan(int w, int h, int B, int dtype, const oflow_hs_params &prm,
+           const TuneTable *tuned = nullptr);
     void *raw_input(int b, int k) const;
     const float *out_u(int b) const;
     const float *out_v(int b) const;
     void run(cudaStream_t st);
     void record(cudaStream_t st);
+    // Times every Jacobi configuration (tile shape, sweeps per launch) at every
+    // level on the plan's current buffers (run a solve first), keeps the
+    // fastest per sweep and records it in `table`.
+    void autotune(cudaStream_t st, TuneTable *table, int reps = 3);
+    int levels() const { return L_; }
+    int jacobi_config(int l) const { return jcfg_[l]; }
     int width() const { return w_; }
     int height() const { return h_; }
     int batch() const { return B_; }
@@ -29,6 +38,7 @@ class HsPlan {
     Arena ar_;
     size_t o_raw_ = 0, o_pyr_ = 0, o_D_ = 0, o_dU0_ = 0, o_dU1_ = 0, o_Ua_ = 0, o_Ub_ = 0,
            o_out_ = 0;
+    int jcfg_[16] = {};
     Graph graph_;
 };
 

@@ -324,6 +324,25 @@ def hs(I0, I1, params: HSParams | None = None, ctx: Context | None = None, out=N
     return hs_batch([(I0, I1)], params, ctx, None if out is None else [out])[0]
 
 
+def hs_autotune(pairs, params: HSParams | None = None, ctx: Context | None = None):
+    """Tune the Jacobi configuration (tile shape, sweeps per launch) per
+    pyramid level for this size and batch (see oflow_hs_autotune).  Returns
+    the chosen config per level, coarsest first."""
+    p = (params or HSParams()).c()
+    n = len(pairs)
+    I0 = (Image * n)()
+    I1 = (Image * n)()
+    keep = []
+    for i, (a, b) in enumerate(pairs):
+        I0[i], ka = _image(a)
+        I1[i], kb = _image(b)
+        keep += [ka, kb]
+    cfg = (C.c_int * 16)()
+    h = _ctx(ctx)
+    _check(lib().oflow_hs_autotune(h, n, I0, I1, C.byref(p), cfg), h)
+    return [c for c in cfg if c >= 0]
+
+
 # ------------------------------------------------------------------ mixed batches
 def batch(jobs, ctx: Context | None = None, out=None):
     """Solve a mixed list of jobs ("tvl1" | "hs", I0, I1, params) as one

@@ -105,6 +105,8 @@ SIGNATURES = {
                       C.POINTER(Flow)]),
     "oflow_hs_batch": (_I, [_VP, _I, C.POINTER(Image), C.POINTER(Image), C.POINTER(HsParams),
                             C.POINTER(Flow)]),
+    "oflow_hs_autotune": (_I, [_VP, _I, C.POINTER(Image), C.POINTER(Image),
+                               C.POINTER(HsParams), C.POINTER(C.c_int)]),
     "oflow_hs_noalloc": (_I, [_VP, _VP, _I, _I, _I, C.POINTER(HsParams), _VP, _VP, _I, _VP]),
     "oflow_batch": (_I, [_VP, _I, C.POINTER(Job)]),
     "oflow_net_num_params": (_I, []),

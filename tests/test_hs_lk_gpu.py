@@ -25,6 +25,50 @@ def test_hs_bit_identical_to_oracle(of, orc, ctx, alpha, L, nw, ns, w, h):
     assert _same(u, ou) and _same(v, ov)
 
 
+@pytest.mark.parametrize("cfg", range(5))
+def test_hs_every_jacobi_config_bit_identical(of, orc, monkeypatch, cfg):
+    """Each Jacobi configuration (tile shape, sweeps per launch), forced by
+    OFLOW_HS_CFG, gives the oracle's bits: 37 sweeps exercise a partial last
+    launch at every depth, the odd size ragged tiles."""
+    from oflow import synth
+    monkeypatch.setenv("OFLOW_HS_CFG", str(cfg))
+    c = of.Context(0)
+    q = synth.hs_pair(seed=5, w=203, h=117)
+    u, v = of.hs(q.I0, q.I1, of.HSParams(3.0, 2, 2, 37), c)
+    ou, ov = orc.hs(q.I0, q.I1, 3.0, 2, 2, 37)
+    c.close()
+    assert _same(u, ou) and _same(v, ov)
+
+
+def test_hs_autotune_keeps_results_and_roundtrips(of, tmp_path):
+    """The HS autotuner picks a configuration per level; the flow after tuning
+    is identical; the choices are saved as "hs" lines and picked up by a fresh
+    context."""
+    from oflow import synth
+    ctx = of.Context(0)
+    qs = [synth.hs_pair(seed=s, w=240, h=160) for s in (7, 8)]
+    pairs = [(q.I0, q.I1) for q in qs]
+    prm = of.HSParams(15.0, 3, 1, 24)
+    before = of.hs_batch(pairs, prm, ctx)
+    cfg = of.hs_autotune(pairs, prm, ctx)
+    assert len(cfg) == 3 and all(0 <= c < 5 for c in cfg)
+    after = of.hs_batch(pairs, prm, ctx)
+    for (u0, v0), (u1, v1) in zip(before, after):
+        assert _same(u0, u1) and _same(v0, v1)
+    path = str(tmp_path / "tune_hs.txt")
+    ctx.save_tuning(path)
+    lines = [l.split() for l in open(path) if not l.startswith("#")]
+    assert len(lines) == 3 and all(l[0] == "hs" and l[3] == "2" for l in lines)
+    assert sorted(int(l[4]) for l in lines) == sorted(cfg)
+    ctx2 = of.Context(0)
+    ctx2.load_tuning(path)
+    again = of.hs_batch(pairs, prm, ctx2)
+    for (u0, v0), (u1, v1) in zip(before, again):
+        assert _same(u0, u1) and _same(v0, v1)
+    ctx.close()
+    ctx2.close()
+
+
 def test_hs_golden(of, ctx):
     d = dict(np.load(os.path.join(GOLDEN, "hs_64x48.npz")))
     u, v = of.hs(d["I0"], d["I1"], of.HSParams(15.0, 1, 1, 50), ctx)
