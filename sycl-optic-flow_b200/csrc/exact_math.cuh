@@ -41,14 +41,16 @@ __host__ __device__ __forceinline__ float hypot_ref(float a, float b) {
 // to the midpoints y0 +- ulp/2 (at |e| = y0*ulp to first order).  When it is
 // more than 2^-20 of that distance away, single rounding of sqrt(S) and the
 // reference's double-then-single rounding agree, and the fast answer is
-// returned; otherwise (and for zero, tiny, huge or non-finite input) the
-// double formula decides.
-__host__ __device__ __forceinline__ float hypot_fast(float a, float b) {
+// certain; otherwise (and for tiny, huge or non-finite input) the double
+// formula decides.  The lower bound 2^-50 on the larger operand keeps every
+// low-order product term (bl, yl) a normal number, so the rounding errors of
+// the subnormal small-operand terms stay far below the 2^-20 margin.
+// hypot_try returns the fast candidate and whether it is certain, without
+// branches, so two lanes can share one branch to the fallback.
+__host__ __device__ __forceinline__ float hypot_try(float a, float b, bool &ok) {
     a = fabsf(a);
     b = fabsf(b);
     const float big = fmaxf(a, b), small = fminf(a, b);
-    if (small == 0.0f && big == big) return big;  // sqrt(x^2) = |x| exactly
-    if (!(big < 0x1p60f) || !(small > 0x1p-60f)) return hypot_ref(a, b);
     const float bh = big * big, bl = OF_FMAF(big, big, -bh);
     const float sh = small * small, sl = OF_FMAF(small, small, -sh);
     const float y0 = sqrtf(bh + sh);
@@ -59,20 +61,52 @@ __host__ __device__ __forceinline__ float hypot_fast(float a, float b) {
     const float ulp = __int_as_float_hd((__float_as_int_hd(y0) & 0x7f800000) - (23 << 23));
     const float T = y0 * ulp;
     const float margin = T * 0x1p-20f;
-    if (fabsf(e) < T - margin) return y0;
-    if (e > T + margin) return __int_as_float_hd(__float_as_int_hd(y0) + 1);
-    if (e < -(T + margin)) return __int_as_float_hd(__float_as_int_hd(y0) - 1);
-    return hypot_ref(a, b);
+    const bool up = e > T + margin, dn = e < -(T + margin), mid = fabsf(e) < T - margin;
+    // fmaxf / fminf drop a NaN operand; the sum keeps it (and big <= s <= 2 big)
+    const float s = a + b;
+    const bool in_range = s >= 0x1p-49f && s < 0x1p60f;
+    const bool zero = small == 0.0f && s == s;  // sqrt(x^2) = |x| exactly
+    ok = (in_range && (up || dn || mid)) || zero;
+    const float y = __int_as_float_hd(__float_as_int_hd(y0) + (up ? 1 : 0) - (dn ? 1 : 0));
+    return zero ? big : y;
+}
+
+__host__ __device__ __forceinline__ float hypot_fast(float a, float b) {
+    bool ok;
+    const float y = hypot_try(a, b, ok);
+    return ok ? y : hypot_ref(a, b);
+}
+
+// Both hypots of a dual update with one (rarely taken) branch to the fallback.
+__host__ __device__ __forceinline__ void hypot2_fast(float a1, float b1, float a2, float b2,
+                                                     float &h1, float &h2) {
+    bool ok1, ok2;
+    h1 = hypot_try(a1, b1, ok1);
+    h2 = hypot_try(a2, b2, ok2);
+    if (!(ok1 && ok2)) {
+        if (!ok1) h1 = hypot_ref(a1, b1);
+        if (!ok2) h2 = hypot_ref(a2, b2);
+    }
 }
 
 // p / g correctly rounded (IEEE division) from y = RN(1/g): q0 = RN(p*y),
 // r = p - q0*g (exact by FMA), q = RN(q0 + r*y) (Markstein).  Valid while
-// neither the quotient nor p underflows; smaller p take the plain division.
-__host__ __device__ __forceinline__ float div_by_rcp(float p, float g, float y) {
-    if (!(fabsf(p) > 0x1p-100f)) return p / g;
+// neither the quotient nor p underflows (|p| > 2^-100 for the g >= 1 of the
+// dual update) and for p = +0; markstein_safe says so.  Other p take the
+// plain division.
+__host__ __device__ __forceinline__ float markstein(float p, float g, float y) {
     const float q0 = p * y;
     const float r = OF_FMAF(-q0, g, p);
     return OF_FMAF(r, y, q0);
+}
+
+__host__ __device__ __forceinline__ bool markstein_safe(float p) {
+    return fabsf(p) > 0x1p-100f || __float_as_int_hd(p) == 0;
+}
+
+__host__ __device__ __forceinline__ float div_by_rcp(float p, float g, float y) {
+    if (markstein_safe(p)) return markstein(p, g, y);
+    return p / g;
 }
 
 }  // namespace oflow

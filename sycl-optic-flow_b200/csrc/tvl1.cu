@@ -9,17 +9,19 @@
 //   T[b][2]        float scratch planes (ingest output, blur output)
 //   pyr_s[b][2]    pyramid level s of I0 / I1, dense nx_s*ny_s
 //   I1g[b]         float4 (I1, I1x, I1y, 0) of the current level
-//   W[b]           float4 (I1wx, I1wy, rho_c, |grad I1w|^2) of the current warp
-//   U0/U1[b]       float2 (u1, u2) ping-pong; Uz[b] upsampled flow
-//   P0/P1[b]       float4 (p11, p12, p21, p22) ping-pong
-// Level planes are packed at the start of their level-0-sized buffers.
+//   WR[b]          float4 (I1wx, I1wy, rho_c, |grad I1w|^2) of the current warp
+//   U[k][b]        float2 (u1, u2), k = 0..7; Uz[b] upsampled flow
+//   P[k][b]        float4 (p11, p12, p21, p22), k = 0..7
+// State buffers 0/1 alternate as the accepted state; 2-4 and 5-7 are two sets
+// of snapshots of the blocked kernel.  Level planes are packed at the start of
+// their level-0-sized buffers.
 //
-// Control: one TvCtrl per pair on the device.  The inner-iteration kernel is
-// launched max_iterations times per warp; its last block to finish reduces the
-// squared change in a fixed order, flips the ping-pong index and sets `stop`
-// once error <= epsilon^2 (tvl1.cpp:216), after which later launches of that
-// warp return at once.  The host never synchronises inside a solve, so the
-// whole schedule is captured into one CUDA graph.
+// Control: one TvCtrl per pair on the device.  The blocked inner-iteration
+// kernel runs up to 4 iterations per launch; its last block to finish reduces
+// the squared change of each iteration in a fixed order, picks the state of the
+// stopping iteration (tvl1.cpp:216) and sets `stop`, after which later launches
+// of that warp return at once.  The host never synchronises inside a solve, so
+// the whole schedule is captured into one CUDA graph.
 #include "common.cuh"
 #include "internal.hpp"
 #include "tvl1.hpp"
@@ -33,7 +35,7 @@ namespace oflow {
 constexpr int kIterTW = 32, kIterTH = 8, kIterNT = 256;
 // blocked inner iterations: iterations per launch (= halo) and the tile
 // configurations, largest first (tile TW x TH, threads); shared memory is
-// 36 B per region pixel (p 16, u 8, I1wx/I1wy 8, rho_c 4)
+// 40 B per region pixel (p 16, (I1wx, I1wy, rho_c, |grad I1w|^2) 16, u 8)
 constexpr int kTbK = 4;
 // Inner-iteration configurations of k_tvl1_tb: tile tw x th, nt threads.
 struct TbCfg {
@@ -48,7 +50,7 @@ constexpr int kNumIterCfgs = 5;
 constexpr int kLvNT = 1024;
 constexpr int kLvMaxPx = 9216;  // u (8 B) + p (16 B) per pixel: 221,184 B of shared memory
 inline bool level_fits(int nx, int ny) { return (long long)nx * ny <= kLvMaxPx; }
-constexpr size_t tb_smem_bytes(int tw, int th) { return (size_t)(tw + 2 * kTbK) * (th + 2 * kTbK) * 36; }
+constexpr size_t tb_smem_bytes(int tw, int th) { return (size_t)(tw + 2 * kTbK) * (th + 2 * kTbK) * 40; }
 constexpr int kGaussTW = 32, kGaussTH = 16, kGaussNT = 256, kGaussMaxR = 15;
 constexpr int kIngestNT = 256, kIngestPPT = 8;
 
@@ -347,14 +349,14 @@ __global__ void k_grad_pack(const float *__restrict__ pyr, size_t pyr_stride, in
 
 // ---------------------------------------------------------------- warping
 // Per warp (tvl1.cpp:197-212): bicubic samples of I1, I1x, I1y at (x+u1,
-// y+u2) with border zeroing, then rho_c.  |grad I1w|^2 (tvl1.cpp:202-206) is
-// recomputed from (I1wx, I1wy) where it is used, with the same expression.  mode 0: u from U[cur];
+// y+u2) with border zeroing, then rho_c and |grad I1w|^2 (tvl1.cpp:202-212),
+// packed as one float4 per pixel.  mode 0: u from U[cur];
 // 1: u from the upsampled Uz (copied into U[cur]); 2: u = 0 (coarsest scale).
 // With first_warp, p is zeroed (tvl1.cpp:190-193).
 enum { kWarpFromU = 0, kWarpFromUz = 1, kWarpZero = 2 };
 
 __global__ void k_warp(const float *__restrict__ pyr, size_t pyr_stride, const float4 *I1g,
-                       float2 *Wxy, float *Rc, float2 *U0, float2 *U1, const float2 *Uz, float4 *P0,
+                       float4 *WR, float2 *U0, float2 *U1, const float2 *Uz, float4 *P0,
                        float4 *P1, size_t stride, int nx, int ny, int mode, int first_warp,
                        TvCtrl *ctrl) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -406,8 +408,7 @@ __global__ void k_warp(const float *__restrict__ pyr, size_t pyr_stride, const f
     }
     const float I0v = __ldg(pyr + (size_t)(2 * b) * pyr_stride + p);
     const float rho_c = (Iw - Iwx * u.x - Iwy * u.y - I0v);
-    Wxy[off + p] = make_float2(Iwx, Iwy);
-    Rc[off + p] = rho_c;
+    WR[off + p] = make_float4(Iwx, Iwy, rho_c, (Iwx * Iwx) + (Iwy * Iwy));
 }
 
 // ---------------------------------------------------------------- iteration
@@ -426,27 +427,23 @@ __device__ __forceinline__ float div_border(float a1c, float a1l, float a2c, flo
     return -a1l - a2u;
 }
 
-// TH step (tvl1.cpp:221-245) and u update (:252-265) for one pixel.
-__device__ __forceinline__ float2 th_u_update(float2 u, float2 w, float rc, float4 pc,
-                                              float4 pl, float4 pu, bool L, bool R, bool T,
-                                              bool B, float l_t, float theta) {
-    const float grad = (w.x * w.x) + (w.y * w.y);
-    const float rho = rc + (w.x * u.x + w.y * u.y);
+// TH step (tvl1.cpp:221-245) and u update (:252-265) for one pixel.  wr holds
+// (I1wx, I1wy, rho_c, |grad I1w|^2).  The branches of the reference pick the
+// coefficient of (I1wx, I1wy): l_t where rho < -l_t*grad, -l_t where rho >
+// l_t*grad, 0 where the gradient vanishes, else -rho/grad; the products are
+// the reference's, so the result is identical.  The quotient is formed for
+// every pixel (most need it) rather than behind a branch.
+__device__ __forceinline__ float2 th_u_update(float2 u, float4 wr, float4 pc, float4 pl, float4 pu,
+                                              bool L, bool R, bool T, bool B, float l_t,
+                                              float theta) {
+    const float grad = wr.w;
+    const float rho = wr.z + (wr.x * u.x + wr.y * u.y);
     const float lg = l_t * grad;
-    float d1, d2;
-    if (!(rho >= -lg)) {
-        d1 = l_t * w.x;
-        d2 = l_t * w.y;
-    } else if (rho > lg) {
-        d1 = -l_t * w.x;
-        d2 = -l_t * w.y;
-    } else if (grad < 1E-10f) {
-        d1 = d2 = 0.0f;
-    } else {
-        const float fi = -rho / grad;
-        d1 = fi * w.x;
-        d2 = fi * w.y;
-    }
+    const bool c1 = rho >= -lg, c2 = rho > lg, c3 = grad < 1E-10f;
+    const float fi = -rho / grad;
+    const float k = !c1 ? l_t : (c2 ? -l_t : fi);
+    float d1 = k * wr.x, d2 = k * wr.y;
+    if (c1 && !c2 && c3) d1 = d2 = 0.0f;
     const float v1 = u.x + d1, v2 = u.y + d2;
     const float div1 = div_border(pc.x, pl.x, pc.y, pu.y, L, R, T, B);
     const float div2 = div_border(pc.z, pl.z, pc.w, pu.w, L, R, T, B);
@@ -455,23 +452,33 @@ __device__ __forceinline__ float2 th_u_update(float2 u, float2 w, float rc, floa
 
 // Dual update (tvl1.cpp:268-291) from the forward differences of u(new):
 // g = 1 + tau/theta*hypot(grad u), p = (p + tau/theta*grad u) / g, with the
-// hypot and the divisions in their exact fast forms (exact_math.cuh).
+// hypot and the divisions in their exact fast forms (exact_math.cuh); the
+// rare inputs those forms do not cover share one branch per kind.
 __device__ __forceinline__ float4 dual_update(float4 po, float f1x, float f1y, float f2x,
                                               float f2y, float taut) {
-    const float g1 = 1.0f + taut * hypot_fast(f1x, f1y);
-    const float g2 = 1.0f + taut * hypot_fast(f2x, f2y);
+    float h1, h2;
+    hypot2_fast(f1x, f1y, f2x, f2y, h1, h2);
+    const float g1 = 1.0f + taut * h1;
+    const float g2 = 1.0f + taut * h2;
     const float r1 = OF_RCP(g1), r2 = OF_RCP(g2);
+    const float n1 = taut * f1x + po.x, n2 = taut * f1y + po.y;
+    const float n3 = taut * f2x + po.z, n4 = taut * f2y + po.w;
     float4 pn;
-    pn.x = div_by_rcp(taut * f1x + po.x, g1, r1);
-    pn.y = div_by_rcp(taut * f1y + po.y, g1, r1);
-    pn.z = div_by_rcp(taut * f2x + po.z, g2, r2);
-    pn.w = div_by_rcp(taut * f2y + po.w, g2, r2);
+    pn.x = markstein(n1, g1, r1);
+    pn.y = markstein(n2, g1, r1);
+    pn.z = markstein(n3, g2, r2);
+    pn.w = markstein(n4, g2, r2);
+    if (!(markstein_safe(n1) && markstein_safe(n2) && markstein_safe(n3) && markstein_safe(n4))) {
+        pn.x = n1 / g1;
+        pn.y = n2 / g1;
+        pn.z = n3 / g2;
+        pn.w = n4 / g2;
+    }
     return pn;
 }
 
 struct IterArgs {
-    const float2 *Wxy;
-    const float *Rc;
+    const float4 *WR;  // (I1wx, I1wy, rho_c, |grad I1w|^2) per pixel
     float2 *U0, *U1;
     float4 *P0, *P1;
     size_t stride;  // elements between pairs
@@ -503,8 +510,7 @@ __global__ void __launch_bounds__(NT) k_tvl1_iter(IterArgs a) {
     float2 *__restrict__ Uout = state_buf(a.U0, a.U1, cur ^ 1) + off;
     const float4 *__restrict__ Pin = state_buf(a.P0, a.P1, cur) + off;
     float4 *__restrict__ Pout = state_buf(a.P0, a.P1, cur ^ 1) + off;
-    const float2 *__restrict__ Wxy = a.Wxy + off;
-    const float *__restrict__ Rc = a.Rc + off;
+    const float4 *__restrict__ WR = a.WR + off;
     const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
 
     __shared__ float4 sP[(TH + 2) * (TW + 2)];
@@ -528,7 +534,7 @@ __global__ void __launch_bounds__(NT) k_tvl1_iter(IterArgs a) {
         const size_t p = (size_t)y * nx + x;
         const float2 u = Uin[p];
         const float4 *c = sP + (ry + 1) * (TW + 2) + (rx + 1);
-        const float2 un = th_u_update(u, Wxy[p], Rc[p], c[0], c[-1], c[-(TW + 2)], x == 0,
+        const float2 un = th_u_update(u, WR[p], c[0], c[-1], c[-(TW + 2)], x == 0,
                                       x == nx - 1, y == 0, y == ny - 1, a.l_t, a.theta);
         sU[i] = un;
         if (rx < TW && ry < TH) {
@@ -602,8 +608,7 @@ __global__ void __launch_bounds__(NT) k_tvl1_iter(IterArgs a) {
 // snapshot buffer, so a stop in the middle of the launch accepts that
 // iteration's state; otherwise the next launch re-runs those iterations.
 struct TbArgs {
-    const float2 *Wxy;
-    const float *Rc;
+    const float4 *WR;
     float2 *U0, *U1;
     float4 *P0, *P1;
     size_t stride;
@@ -642,8 +647,7 @@ __device__ __forceinline__ void for_rect(int x0, int x1, int y0, int y1, F &&f) 
 // ever leaves the region.  INTERIOR: no region pixel lies on the image border
 // (no bounds or border tests).
 template <int TW, int TH, int K, int NT, bool INTERIOR>
-__device__ __forceinline__ void tb_iteration(int j, float4 *sP, const float2 *sW,
-                                             const float *sR, float2 *sU, int ox, int oy, int nx,
+__device__ __forceinline__ void tb_iteration(int j, float4 *sP, const float4 *sWR, float2 *sU, int ox, int oy, int nx,
                                              int ny, float l_t, float theta, float taut,
                                              double &err) {
     constexpr int RW = TW + 2 * K, RH = TH + 2 * K;
@@ -652,7 +656,7 @@ __device__ __forceinline__ void tb_iteration(int j, float4 *sP, const float2 *sW
         const int x = ox + rx, y = oy + ry;
         if (!INTERIOR && (x >= nx || y >= ny || x < 0 || y < 0)) return;
         const float2 u = sU[i];
-        const float2 un = th_u_update(u, sW[i], sR[i], sP[i], sP[i - 1], sP[i - RW],
+        const float2 un = th_u_update(u, sWR[i], sP[i], sP[i - 1], sP[i - RW],
                                       !INTERIOR && x == 0, !INTERIOR && x == nx - 1,
                                       !INTERIOR && y == 0, !INTERIOR && y == ny - 1, l_t, theta);
         sU[i] = un;
@@ -771,9 +775,8 @@ __global__ void __launch_bounds__(NT, 2) k_tvl1_tb(TbArgs a) {
     constexpr int RW = TW + 2 * K, RH = TH + 2 * K, RN = RW * RH;
     extern __shared__ float4 tb_smem[];
     float4 *sP = tb_smem;                                  // RN
-    float2 *sU = reinterpret_cast<float2 *>(sP + RN);      // RN
-    float2 *sW = sU + RN;                                  // RN
-    float *sR = reinterpret_cast<float *>(sW + RN);        // RN
+    float4 *sWR = sP + RN;                                 // RN
+    float2 *sU = reinterpret_cast<float2 *>(sWR + RN);     // RN
 
     const int b = blockIdx.z;
     TvCtrl *ctrl = a.ctrl + b;
@@ -798,27 +801,23 @@ __global__ void __launch_bounds__(NT, 2) k_tvl1_tb(TbArgs a) {
     float2 *__restrict__ Uout = state_buf(a.U0, a.U1, fin) + off;
     const float4 *__restrict__ Pin = state_buf(a.P0, a.P1, cur) + off;
     float4 *__restrict__ Pout = state_buf(a.P0, a.P1, fin) + off;
-    const float2 *__restrict__ Wg = a.Wxy + off;
-    const float *__restrict__ Rg = a.Rc + off;
+    const float4 *__restrict__ Wg = a.WR + off;
     const int ox = blockIdx.x * TW - K, oy = blockIdx.y * TH - K;
     const bool interior = ox >= 1 && oy >= 1 && ox + RW <= nx - 1 && oy + RH <= ny - 1;
 
     // all loads of the region issued before any use
     for (int i = threadIdx.x; i < RN; i += NT) {
         const int x = ox + i % RW, y = oy + i / RW;
-        float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
-        float2 u = make_float2(0.f, 0.f), w = u;
-        float r = 0.0f;
+        float4 p = make_float4(0.f, 0.f, 0.f, 0.f), w = p;
+        float2 u = make_float2(0.f, 0.f);
         if (x >= 0 && x < nx && y >= 0 && y < ny) {
             const size_t q = (size_t)y * nx + x;
             p = Pin[q];
             w = Wg[q];
-            r = Rg[q];
             u = Uin[q];
         }
         sP[i] = p;
-        sW[i] = w;
-        sR[i] = r;
+        sWR[i] = w;
         sU[i] = u;
     }
     __syncthreads();
@@ -841,10 +840,10 @@ __global__ void __launch_bounds__(NT, 2) k_tvl1_tb(TbArgs a) {
         err[j] = 0.0;
         if (j < kk) {  // uniform over the block
             if (interior)
-                tb_iteration<TW, TH, K, NT, true>(j + 1, sP, sW, sR, sU, ox, oy, nx, ny, a.l_t,
+                tb_iteration<TW, TH, K, NT, true>(j + 1, sP, sWR, sU, ox, oy, nx, ny, a.l_t,
                                                   a.theta, a.taut, err[j]);
             else
-                tb_iteration<TW, TH, K, NT, false>(j + 1, sP, sW, sR, sU, ox, oy, nx, ny, a.l_t,
+                tb_iteration<TW, TH, K, NT, false>(j + 1, sP, sWR, sU, ox, oy, nx, ny, a.l_t,
                                                    a.theta, a.taut, err[j]);
             if (snaps && j + 1 < kk)  // snapshot: the state a stop after iteration j+1 accepts
                 store_owned(state_buf(a.U0, a.U1, snap + j) + off, state_buf(a.P0, a.P1, snap + j) + off);
@@ -880,8 +879,7 @@ __global__ void __launch_bounds__(kLvNT) k_tvl1_level(TbArgs a) {
     const float4 *__restrict__ Pin = state_buf(a.P0, a.P1, cur) + off;
     float2 *__restrict__ Uout = state_buf(a.U0, a.U1, fin) + off;
     float4 *__restrict__ Pout = state_buf(a.P0, a.P1, fin) + off;
-    const float2 *__restrict__ Wg = a.Wxy + off;
-    const float *__restrict__ Rg = a.Rc + off;
+    const float4 *__restrict__ Wg = a.WR + off;
     for (int i = tid; i < N; i += kLvNT) {
         sU[i] = Uin[i];
         sP[i] = Pin[i];
@@ -898,7 +896,7 @@ __global__ void __launch_bounds__(kLvNT) k_tvl1_level(TbArgs a) {
             const float4 pc = sP[i];
             const float4 pl = x > 0 ? sP[i - 1] : pc;   // unused on the left border
             const float4 pu = y > 0 ? sP[i - nx] : pc;  // unused on the top border
-            const float2 un = th_u_update(u, __ldg(Wg + i), __ldg(Rg + i), pc, pl, pu, x == 0,
+            const float2 un = th_u_update(u, __ldg(Wg + i), pc, pl, pu, x == 0,
                                           x == nx - 1, y == 0, y == ny - 1, a.l_t, a.theta);
             sU[i] = un;
             const float e1 = un.x - u.x, e2 = un.y - u.y;
@@ -950,8 +948,7 @@ __global__ void __launch_bounds__(kLvNT) k_tvl1_level(TbArgs a) {
 // sum |rho(u)| with rho linearised at the current warp.  Last block of a pair
 // writes ctrl.energy and, if slot >= 0, energy_out[b * slots + slot].
 constexpr int kEnNT = 256;
-__global__ void __launch_bounds__(kEnNT) k_energy(const float2 *Wxy, const float *Rc,
-                                                  const float2 *U0,
+__global__ void __launch_bounds__(kEnNT) k_energy(const float4 *WR, const float2 *U0,
                                                   const float2 *U1, size_t stride, int nx,
                                                   int ny, float lambda, TvCtrl *ctrl,
                                                   double *partials, int max_blocks,
@@ -969,8 +966,8 @@ __global__ void __launch_bounds__(kEnNT) k_energy(const float2 *Wxy, const float
         if (x < nx - 1) { const float2 r = U[i + 1]; f1x = (double)(r.x - uc.x); f2x = (double)(r.y - uc.y); }
         if (y < ny - 1) { const float2 d = U[i + nx]; f1y = (double)(d.x - uc.x); f2y = (double)(d.y - uc.y); }
         tv += sqrt(f1x * f1x + f1y * f1y) + sqrt(f2x * f2x + f2y * f2y);
-        const float2 w = Wxy[off + i];
-        const float rho = Rc[off + i] + (w.x * uc.x + w.y * uc.y);
+        const float4 w = WR[off + i];
+        const float rho = w.z + (w.x * uc.x + w.y * uc.y);
         data += fabs((double)rho);
     }
     __shared__ double sred[kEnNT / 32];
@@ -1177,8 +1174,7 @@ TvPlan::TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, boo
     o_T_ = ar_.reserve(2 * B * N0 * 4);
     o_pyr_ = ar_.reserve(pyr_total * 4);
     o_I1g_ = ar_.reserve(B * N0 * 16);
-    o_Wxy_ = ar_.reserve(B * N0 * 8);
-    o_Rc_ = ar_.reserve(B * N0 * 4);
+    o_WR_ = ar_.reserve(B * N0 * 16);
     o_U0_ = ar_.reserve(kStateBufs * B * N0 * 8);  // buffer k at U0 + k*B*N0
     o_Uz_ = ar_.reserve(B * N0 * 8);
     o_P0_ = ar_.reserve(kStateBufs * B * N0 * 16);
@@ -1244,8 +1240,7 @@ void TvPlan::record(cudaStream_t st) {
     float *T = ar_.at<float>(o_T_);
     float *pyr = ar_.at<float>(o_pyr_);
     float4 *I1g = ar_.at<float4>(o_I1g_);
-    float2 *Wxy = ar_.at<float2>(o_Wxy_);
-    float *Rc = ar_.at<float>(o_Rc_);
+    float4 *WR = ar_.at<float4>(o_WR_);
     float2 *U0 = ubuf(0), *U1 = ubuf(1), *Uz = ar_.at<float2>(o_Uz_);
     float4 *P0 = pbuf(0), *P1 = pbuf(1);
     TvCtrl *ctrl = ar_.at<TvCtrl>(o_ctrl_);
@@ -1311,7 +1306,7 @@ void TvPlan::record(cudaStream_t st) {
         }
         k_grad_pack<<<gr, blk, 0, st>>>(pyr + pyr_off_[s], lp, nx, ny, I1g, N0);
         launches_ += 1;
-        IterArgs ia{Wxy, Rc, U0, U1, P0, P1, N0, nx, ny, l_t, prm_.theta, taut, eps2, ctrl, part,
+        IterArgs ia{WR, U0, U1, P0, P1, N0, nx, ny, l_t, prm_.theta, taut, eps2, ctrl, part,
                     max_blocks_, iters, iter_stride_, 0};
         dim3 ig(div_up(nx, kIterTW), div_up(ny, kIterTH), B);
         const int cfg = tb_cfg_[s];
@@ -1319,7 +1314,7 @@ void TvPlan::record(cudaStream_t st) {
             const int mode = wi > 0 ? kWarpFromU
                                     : (s == s0_ ? (warm_ ? kWarpFromUz : kWarpZero) : kWarpFromUz);
             mark();
-            k_warp<<<gr, blk, 0, st>>>(pyr + pyr_off_[s], lp, I1g, Wxy, Rc, U0, U1, Uz, P0, P1,
+            k_warp<<<gr, blk, 0, st>>>(pyr + pyr_off_[s], lp, I1g, WR, U0, U1, Uz, P0, P1,
                                        N0, nx, ny, mode, wi == 0, ctrl);
             mark();
             launches_ += 1;
@@ -1327,7 +1322,7 @@ void TvPlan::record(cudaStream_t st) {
             if (!trace_) {
                 // blocked schedule: ceil(max/K) launches plus one for a
                 // possible re-run after a mid-block stop
-                TbArgs ta{Wxy, Rc, U0, U1, P0, P1, N0, nx, ny, prm_.max_iterations, l_t,
+                TbArgs ta{WR, U0, U1, P0, P1, N0, nx, ny, prm_.max_iterations, l_t,
                           prm_.theta, taut, eps2, ctrl, part, max_blocks_ / kTbK, iters,
                           iter_stride_, ia.stage};
                 dim3 tg(div_up(nx, kTbCfgs[cfg].tw), div_up(ny, kTbCfgs[cfg].th), B);
@@ -1360,14 +1355,14 @@ void TvPlan::record(cudaStream_t st) {
                 launches_ += 1;
                 const int slot = (s * prm_.warps + wi) * prm_.max_iterations + it;
                 k_energy<<<dim3(imin(energy_blocks_, div_up(nx * ny, kEnNT * 4)), B), kEnNT, 0,
-                           st>>>(Wxy, Rc, U0, U1, N0, nx, ny, prm_.lambda, ctrl, part, max_blocks_,
+                           st>>>(WR, U0, U1, N0, nx, ny, prm_.lambda, ctrl, part, max_blocks_,
                                  energy, energy_slots_, slot, it + 1);
                 launches_ += 1;
             }
         }
     }
     // final energy at the finest scale, last warp
-    k_energy<<<dim3(energy_blocks_, B), kEnNT, 0, st>>>(Wxy, Rc, U0, U1, N0, w_, h_, prm_.lambda,
+    k_energy<<<dim3(energy_blocks_, B), kEnNT, 0, st>>>(WR, U0, U1, N0, w_, h_, prm_.lambda,
                                                         ctrl, part, max_blocks_, energy,
                                                         energy_slots_, trace_ ? -1 : 0, -1);
     k_split<<<dim3(imin(div_up((int)N0, 256 * 4), 1024), B), 256, 0, st>>>(
@@ -1465,7 +1460,7 @@ void TvPlan::autotune(cudaStream_t st, TuneTable *table, int reps) {
                 // per-iteration time: a tiled launch runs K iterations (no
                 // stop); the whole-level kernel is given 2K
                 const int iters_run = c == kLevelCfg ? 2 * kTbK : kTbK;
-                TbArgs ta{ar_.at<float2>(o_Wxy_), ar_.at<float>(o_Rc_), ubuf(0), ubuf(1), pbuf(0),
+                TbArgs ta{ar_.at<float4>(o_WR_), ubuf(0), ubuf(1), pbuf(0),
                           pbuf(1), N0,
                           nx, ny, c == kLevelCfg ? iters_run : 1 << 30, l_t, prm_.theta, taut, -1.0f,
                           ctrl, ar_.at<double>(o_part_), max_blocks_ / kTbK, ar_.at<int>(o_iters_),

@@ -125,7 +125,7 @@ class TvPlan {
     bool warm_ = false;
     size_t o_tarr_ = 0, o_tout_ = 0;
     int iter_launches_per_stage() const;
-    size_t o_Wxy_ = 0, o_Rc_ = 0;
+    size_t o_WR_ = 0;
     size_t o_raw_ = 0, o_T_ = 0, o_pyr_ = 0, o_I1g_ = 0, o_U0_ = 0, o_Uz_ = 0, o_P0_ = 0,
            o_out_ = 0, o_ctrl_ = 0, o_part_ = 0, o_recs_ = 0, o_iters_ = 0, o_energy_ = 0;
     float2 *ubuf(int k) const;  // state buffer k of u (all pairs)
