@@ -214,6 +214,7 @@ void run_tvl1(oflow_ctx *ctx, int n, const oflow_image *I0, const oflow_image *I
     for (const Group &g : groups) {
         TvPlan &pl = tv_plan(ctx, g.w, g.h, (int)g.idx.size(), g.dtype, *p, energy_trace != nullptr);
         if (!prof && !energy_trace) ctx->last_tv.push_back(&pl);
+        pl.check_device_error();  // a failure of an earlier, unsynchronised call
         for (size_t b = 0; b < g.idx.size(); b++) {
             // device frames are read in place (pitched); host frames are staged
             const oflow_image *im[2] = {&I0[g.idx[b]], &I1[g.idx[b]]};
@@ -242,6 +243,7 @@ void run_tvl1(oflow_ctx *ctx, int n, const oflow_image *I0, const oflow_image *I
         if (energy_trace) pl.read_energy_trace(0, energy_trace, st);
     }
     finish(ctx, device_only);
+    for (TvPlan *pl : ctx->last_tv) pl->check_device_error();
 }
 
 }  // namespace
@@ -395,6 +397,7 @@ oflow_status oflow_tvl1_autotune(oflow_ctx *ctx, int n, const oflow_image *I0,
         pl.run(st);
         pl.autotune(st, &ctx->tune);
         OF_CUDA(cudaStreamSynchronize(st));
+        pl.check_device_error();
         if (cfg_per_scale)
             for (int s = 0; s < OFLOW_MAX_SCALES; s++)
                 cfg_per_scale[s] = s < pl.nscales() ? pl.tb_config(s) : -1;
@@ -514,6 +517,7 @@ oflow_status oflow_batch(oflow_ctx *ctx, int n, const oflow_job *jobs) {
                 if (j.out.location == OFLOW_HOST) device_only = false;
             }
         finish(ctx, device_only);
+        for (auto &t : mb->tv) t->check_device_error();
     });
 }
 
@@ -810,7 +814,8 @@ oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_
         wp->run(st);
         std::vector<double> ew(n), ep(n, 0.0);
         std::vector<int> acc(n, 1);
-        wp->true_energy(ew.data(), st);
+        wp->true_energy(ew.data(), st);  // synchronises
+        wp->check_device_error();
         if (stats)
             for (int b = 0; b < n; b++) wp->read_stats(b, &stats[b], st);
         TvPlan *pp = nullptr;
@@ -819,6 +824,7 @@ oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_
             for (int b = 0; b < n; b++) stage_pair_raw(*pp, b, I0[b], I1[b], st);
             pp->run(st);
             pp->true_energy(ep.data(), st);
+            pp->check_device_error();
             for (int b = 0; b < n; b++) acc[b] = ew[b] <= 1.01 * ep[b] ? 1 : 0;
         }
         for (int b = 0; b < n; b++) {
@@ -969,6 +975,7 @@ oflow_status oflow_stream_push(oflow_stream *s, const oflow_image *frames, const
         }
         s->frames++;
         finish(s->ctx, device_only);
+        if (s->tv) s->tv->check_device_error();
     });
 }
 

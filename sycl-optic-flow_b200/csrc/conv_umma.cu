@@ -17,7 +17,7 @@
 // accumulator back with tcgen05.ld (warp w holds TMEM lanes 32w..32w+31, one
 // pixel per thread), adds the bias, applies the ReLU and stores bf16 or f32.
 //
-// Every wait on an mbarrier is bounded (one second of %globaltimer); when one
+// Every wait on an mbarrier is bounded (kWaitNs of %globaltimer); when one
 // gives up, the kernel sets *err, waits (bounded) for its own copies, frees
 // its tensor memory and returns.
 #include <cuda_bf16.h>
@@ -27,6 +27,7 @@
 #include "cnn.cuh"
 #include "common.cuh"
 #include "internal.hpp"
+#include "ptx.cuh"
 
 namespace oflow {
 namespace {
@@ -35,11 +36,6 @@ constexpr int kUmBM = 128;       // output pixels per CTA (UMMA M)
 constexpr int kUmNT = 128;       // threads per CTA
 constexpr int kUmStages = 4;     // shared-memory stage buffers
 constexpr int kUmAhead = 2;      // stages gathered ahead of the one being multiplied
-constexpr unsigned long long kUmWaitNs = 1000000000ull;
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, bool valid) {
     const int n = valid ? 16 : 0;  // 0 bytes read: the destination is zero-filled
@@ -51,43 +47,11 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-__device__ __forceinline__ unsigned long long globaltimer() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// Waits for the phase with the given parity to complete; false after one second.
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
-    if (mbar_try_wait(bar, parity)) return true;
-    const unsigned long long t0 = globaltimer();
-    while (!mbar_try_wait(bar, parity))
-        if (globaltimer() - t0 > kUmWaitNs) return false;
-    return true;
-}
-
 __device__ __forceinline__ void tc_fence_before() {
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
 }
 __device__ __forceinline__ void tc_fence_after() {
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-}
-__device__ __forceinline__ void fence_async_smem() {
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
 }
 
 // Shared-memory matrix descriptor, no swizzle, K-major: start address, LBO =
@@ -164,7 +128,7 @@ __global__ void __launch_bounds__(kUmNT) k_conv_fwd_umma(ConvDims d, const __nv_
     }
     if (tid == 0) {
         for (int i = 0; i < kUmStages; i++) mbar_init(smem_u32(&mbar[i]), 1);
-        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        fence_mbar_init();
     }
     tc_fence_before();
     __syncthreads();
