@@ -795,19 +795,23 @@ __global__ void __launch_bounds__(NT, 2) k_tvl1_tb(const __grid_constant__ TbArg
 
     const int b = blockIdx.z;
     TvCtrl *ctrl = a.ctrl + b;
-    if (*((volatile int *)&ctrl->stop)) return;
-    const int cur = *((volatile int *)&ctrl->cur);
-    const int n0 = *((volatile int *)&ctrl->n);
-    const int redo = *((volatile int *)&ctrl->redo);
+    // The pair's control block changes in this launch only once all of the
+    // pair's blocks have read it (the last to arrive writes it), so the reads
+    // may be served from L1: blocks after the first on an SM, and the blocks of
+    // a pair that already stopped, leave without a trip to L2.
+    if (__ldca(&ctrl->stop)) return;
+    const int cur = __ldca(&ctrl->cur);
+    const int n0 = __ldca(&ctrl->n);
+    const int redo = __ldca(&ctrl->redo);
     const int kk = redo > 0 ? redo : imin(K, a.max_it - n0);
     // block-uniform: every block of the pair reads the same control block
     bool snaps = false;
     if (redo == 0) {
-        const float q = fminf(*((volatile float *)&ctrl->decay), 1.0f);
+        const float q = fminf(__ldca(&ctrl->decay), 1.0f);
         float qk = 1.0f;
 #pragma unroll
         for (int j = 1; j < K; j++) qk *= q;
-        snaps = *((volatile float *)&ctrl->last_err) * qk < kSnapMargin * a.eps2;
+        snaps = __ldca(&ctrl->last_err) * qk < kSnapMargin * a.eps2;
     }
     const int nx = a.nx, ny = a.ny;
     const size_t off = (size_t)b * a.stride;
