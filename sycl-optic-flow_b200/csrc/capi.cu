@@ -89,6 +89,12 @@ struct MixedBatch {
 };
 }  // namespace
 
+// A TV-L1 batch with frames or flows in host memory is solved in up to this
+// many chunks, each a plan of its own on a side stream, so that the copies of
+// one chunk overlap the solves of the others.
+constexpr int kHostChunks = 4;
+constexpr int kChunkMinPairs = 4;
+
 struct oflow_ctx {
     int device = 0;
     cudaStream_t own = nullptr;
@@ -106,6 +112,10 @@ struct oflow_ctx {
     // objects created on this context; destroying the context detaches them
     std::vector<oflow_net *> nets;
     std::vector<oflow_stream *> streams;
+    // chunked host solves: one plan cache and one stream per chunk slot
+    std::vector<std::unique_ptr<TvPlan>> tv_side[kHostChunks];
+    cudaStream_t side[kHostChunks] = {};
+    cudaEvent_t fork = nullptr, join[kHostChunks] = {};
     cudaStream_t stream() const { return user ? user : own; }
 };
 
@@ -152,6 +162,30 @@ template <typename F> oflow_status guard(oflow_ctx *ctx, F &&f) {
 void finish(oflow_ctx *ctx, bool device_only) {
     if (ctx->user && device_only) return;
     OF_CUDA(cudaStreamSynchronize(ctx->stream()));
+}
+
+// Side streams and events of the chunked host solves, created on first use.
+void make_side_streams(oflow_ctx *ctx) {
+    if (ctx->fork) return;
+    for (int c = 0; c < kHostChunks; c++) {
+        OF_CUDA(cudaStreamCreateWithFlags(&ctx->side[c], cudaStreamNonBlocking));
+        OF_CUDA(cudaEventCreateWithFlags(&ctx->join[c], cudaEventDisableTiming));
+    }
+    OF_CUDA(cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming));
+}
+
+// The plan of chunk slot c for this size and batch (chunks run at once, so
+// each slot has plans of its own).
+TvPlan &side_plan(oflow_ctx *ctx, int c, int w, int h, int B, int dtype, const oflow_tvl1_params &p) {
+    auto &v = ctx->tv_side[c];
+    for (auto &pl : v)
+        if (pl->width() == w && pl->height() == h && pl->batch() == B && pl->dtype() == dtype &&
+            same(pl->params(), p))
+            return *pl;
+    v.emplace_back(new TvPlan(w, h, B, dtype, p, false, &ctx->tune));
+    if (v.size() > kMaxPlans) ctx->last_tv.clear();  // an evicted plan may be listed
+    keep_recent(v);
+    return *v.back();
 }
 
 TvPlan &tv_plan(oflow_ctx *ctx, int w, int h, int B, int dtype, const oflow_tvl1_params &p,
@@ -211,39 +245,70 @@ void run_tvl1(oflow_ctx *ctx, int n, const oflow_image *I0, const oflow_image *I
     const std::vector<Group> groups = group_pairs(n, I0, I1);
     OF_CHECK(prof == nullptr || groups.size() == 1, "tvl1 profile: pairs must share one size");
     ctx->last_tv.clear();
-    for (const Group &g : groups) {
-        TvPlan &pl = tv_plan(ctx, g.w, g.h, (int)g.idx.size(), g.dtype, *p, energy_trace != nullptr);
-        if (!prof && !energy_trace) ctx->last_tv.push_back(&pl);
-        pl.check_device_error();  // a failure of an earlier, unsynchronised call
-        for (size_t b = 0; b < g.idx.size(); b++) {
-            // device frames are read in place (pitched); host frames are staged
+    // stages the group's pairs [b0, b1) into plan pl on stream s: device frames
+    // are read in place (pitched), host frames are copied
+    auto bind = [&](TvPlan &pl, const Group &g, int b0, int b1, cudaStream_t s) {
+        for (int b = b0; b < b1; b++) {
             const oflow_image *im[2] = {&I0[g.idx[b]], &I1[g.idx[b]]};
             for (int k = 0; k < 2; k++) {
                 if (im[k]->location == OFLOW_DEVICE) {
-                    pl.bind_frame((int)b, k, im[k]->data, im[k]->pitch ? im[k]->pitch : im[k]->width);
+                    pl.bind_frame(b - b0, k, im[k]->data, im[k]->pitch ? im[k]->pitch : im[k]->width);
                 } else {
-                    stage_image(*im[k], pl.raw_input((int)b, k), dtype_size(g.dtype), st);
-                    pl.bind_raw((int)b, k);
+                    stage_image(*im[k], pl.raw_input(b - b0, k), dtype_size(g.dtype), s);
+                    pl.bind_raw(b - b0, k);
                 }
             }
         }
+    };
+    auto collect = [&](TvPlan &pl, const Group &g, int b0, int b1, cudaStream_t s) {
+        for (int b = b0; b < b1; b++) {
+            const oflow_flow &o = out[g.idx[b]];
+            unstage_plane(pl.out_u(b - b0), g.w, g.h, o.u, o.pitch, o.location, s);
+            unstage_plane(pl.out_v(b - b0), g.w, g.h, o.v, o.pitch, o.location, s);
+            if (o.location == OFLOW_HOST) device_only = false;
+            if (stats) pl.read_stats(b - b0, &stats[g.idx[b]], s);
+        }
+    };
+    for (const Group &g : groups) {
+        const int ng = (int)g.idx.size();
+        bool host_io = false;
+        for (int i : g.idx)
+            host_io = host_io || I0[i].location == OFLOW_HOST || I1[i].location == OFLOW_HOST ||
+                      out[i].location == OFLOW_HOST;
+        const int chunks = (host_io && !prof && !energy_trace)
+                               ? std::max(1, std::min(kHostChunks, ng / kChunkMinPairs))
+                               : 1;
+        if (chunks > 1) {
+            // chunk c: pairs [c*ng/chunks, (c+1)*ng/chunks) on side stream c
+            make_side_streams(ctx);
+            OF_CUDA(cudaEventRecord(ctx->fork, st));
+            for (int c = 0; c < chunks; c++) {
+                const int b0 = c * ng / chunks, b1 = (c + 1) * ng / chunks;
+                const cudaStream_t sc = ctx->side[c];
+                TvPlan &pl = side_plan(ctx, c, g.w, g.h, b1 - b0, g.dtype, *p);
+                ctx->last_tv.push_back(&pl);
+                OF_CUDA(cudaStreamWaitEvent(sc, ctx->fork, 0));
+                bind(pl, g, b0, b1, sc);
+                pl.run(sc);
+                collect(pl, g, b0, b1, sc);
+                OF_CUDA(cudaEventRecord(ctx->join[c], sc));
+                OF_CUDA(cudaStreamWaitEvent(st, ctx->join[c], 0));
+            }
+            continue;
+        }
+        TvPlan &pl = tv_plan(ctx, g.w, g.h, ng, g.dtype, *p, energy_trace != nullptr);
+        if (!prof && !energy_trace) ctx->last_tv.push_back(&pl);
+        bind(pl, g, 0, ng, st);
         if (prof)
             pl.profile(st, prof);
         else if (energy_trace)
             pl.run_eager(st);
         else
             pl.run(st);
-        for (size_t b = 0; b < g.idx.size(); b++) {
-            const oflow_flow &o = out[g.idx[b]];
-            unstage_plane(pl.out_u((int)b), g.w, g.h, o.u, o.pitch, o.location, st);
-            unstage_plane(pl.out_v((int)b), g.w, g.h, o.v, o.pitch, o.location, st);
-            if (o.location == OFLOW_HOST) device_only = false;
-            if (stats) pl.read_stats((int)b, &stats[g.idx[b]], st);
-        }
+        collect(pl, g, 0, ng, st);
         if (energy_trace) pl.read_energy_trace(0, energy_trace, st);
     }
     finish(ctx, device_only);
-    for (TvPlan *pl : ctx->last_tv) pl->check_device_error();
 }
 
 }  // namespace
@@ -305,6 +370,13 @@ oflow_status oflow_ctx_destroy(oflow_ctx *ctx) {
     ctx->lk.clear();
     ctx->mixed.clear();
     ctx->tv_warm.clear();
+    for (int c = 0; c < kHostChunks; c++) {
+        if (ctx->side[c]) cudaStreamSynchronize(ctx->side[c]);
+        ctx->tv_side[c].clear();
+        if (ctx->side[c]) cudaStreamDestroy(ctx->side[c]);
+        if (ctx->join[c]) cudaEventDestroy(ctx->join[c]);
+    }
+    if (ctx->fork) cudaEventDestroy(ctx->fork);
     if (ctx->own) cudaStreamDestroy(ctx->own);
     delete ctx;
     return OFLOW_OK;
@@ -327,6 +399,7 @@ oflow_status oflow_ctx_trim(oflow_ctx *ctx) {
         ctx->lk.clear();
         ctx->mixed.clear();
         ctx->tv_warm.clear();
+        for (auto &v : ctx->tv_side) v.clear();
     });
 }
 
@@ -397,7 +470,6 @@ oflow_status oflow_tvl1_autotune(oflow_ctx *ctx, int n, const oflow_image *I0,
         pl.run(st);
         pl.autotune(st, &ctx->tune);
         OF_CUDA(cudaStreamSynchronize(st));
-        pl.check_device_error();
         if (cfg_per_scale)
             for (int s = 0; s < OFLOW_MAX_SCALES; s++)
                 cfg_per_scale[s] = s < pl.nscales() ? pl.tb_config(s) : -1;
@@ -517,7 +589,6 @@ oflow_status oflow_batch(oflow_ctx *ctx, int n, const oflow_job *jobs) {
                 if (j.out.location == OFLOW_HOST) device_only = false;
             }
         finish(ctx, device_only);
-        for (auto &t : mb->tv) t->check_device_error();
     });
 }
 
@@ -553,6 +624,8 @@ oflow_status oflow_ctx_load_tuning(oflow_ctx *ctx, const char *path) {
         fclose(f);
         OF_CHECK(!bad, "load tuning: malformed line");
         ctx->tv.clear();  // plans pick the table up when rebuilt
+        for (auto &v : ctx->tv_side) v.clear();
+        ctx->last_tv.clear();
         ctx->hs.clear();
     });
 }
@@ -774,7 +847,6 @@ oflow_status oflow_net_predict(oflow_net *net, const void *frames, int dtype, fl
         net->net->forward(frames, dtype, ps, st);
         net->net->flow_to(nullptr, 0, flow, st);
         OF_CUDA(cudaGetLastError());
-        net->net->check_device_error(st);
     });
 }
 
@@ -814,8 +886,7 @@ oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_
         wp->run(st);
         std::vector<double> ew(n), ep(n, 0.0);
         std::vector<int> acc(n, 1);
-        wp->true_energy(ew.data(), st);  // synchronises
-        wp->check_device_error();
+        wp->true_energy(ew.data(), st);
         if (stats)
             for (int b = 0; b < n; b++) wp->read_stats(b, &stats[b], st);
         TvPlan *pp = nullptr;
@@ -824,7 +895,6 @@ oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_
             for (int b = 0; b < n; b++) stage_pair_raw(*pp, b, I0[b], I1[b], st);
             pp->run(st);
             pp->true_energy(ep.data(), st);
-            pp->check_device_error();
             for (int b = 0; b < n; b++) acc[b] = ew[b] <= 1.01 * ep[b] ? 1 : 0;
         }
         for (int b = 0; b < n; b++) {
@@ -835,7 +905,6 @@ oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_
             if (energy_plain) energy_plain[b] = ep[b];
             if (accepted) accepted[b] = acc[b];
         }
-        net->net->check_device_error(st);
     });
 }
 
@@ -975,7 +1044,6 @@ oflow_status oflow_stream_push(oflow_stream *s, const oflow_image *frames, const
         }
         s->frames++;
         finish(s->ctx, device_only);
-        if (s->tv) s->tv->check_device_error();
     });
 }
 

@@ -155,6 +155,25 @@ def test_device_frames_read_in_place_then_host_frames(of, orc, ctx):
     check(Bp, of.tvl1_batch(Bp, prm, ctx))
 
 
+def test_host_batch_in_chunks_matches_device_batch(of, ctx):
+    """A batch with host frames and host flows runs as up to four chunks on
+    side streams (copies of one chunk overlap the solves of the others); the
+    flows and statistics equal those of the same batch solved as one plan from
+    device frames, including a batch that does not split evenly."""
+    import torch
+    prm = of.TVL1Params(nscales=3, max_iterations=14)
+    for n in (8, 13):
+        pairs = [_pair(900 + i, 84, 60)[1:] for i in range(n)]
+        host, st_h = of.tvl1_batch(pairs, prm, ctx, stats=True)
+        dev = of.tvl1_batch([(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda())
+                             for a, b in pairs], prm, ctx)
+        _, st_d = of.tvl1_batch(pairs[:1], prm, ctx, stats=True)
+        for (hu, hv), (du, dv) in zip(host, dev):
+            assert np.array_equal(hu, du.cpu().numpy()) and np.array_equal(hv, dv.cpu().numpy())
+        assert np.array_equal(st_h[0]["iterations"], st_d[0]["iterations"])
+        assert all(s["energy"] > 0 for s in st_h)
+
+
 def test_launch_count_of_the_schedule(of):
     """oflow_ctx_last_launches reports the captured schedule: per warp stage
     one warp launch and, for levels larger than 9216 pixels, ceil(50/4)+1
