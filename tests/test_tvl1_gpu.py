@@ -214,6 +214,25 @@ def test_full_size_workload_against_oracle_and_reference(of, orc, ctx):
     assert synth.epe(u, v, p.u, p.v, p.valid, 8) < 0.5
 
 
+@pytest.mark.parametrize("cfg", [None, "3"])
+def test_repeated_full_size_solves_match_the_oracle(of, orc, monkeypatch, cfg):
+    """Five solves of the 1024x436 pair, each on a fresh context (new plan,
+    new graph, reused device memory), with the tile shapes the plan picks and
+    with the smallest tile forced everywhere: every solve equals the oracle.
+    Catches order-dependent faults that a single solve can miss."""
+    if cfg:
+        monkeypatch.setenv("OFLOW_TB_CFG", cfg)
+    p, a, b = _pair(0, 1024, 436, radius=80.0)
+    prm = of.TVL1Params(nscales=5, warps=1, max_iterations=50)
+    ou, ov, its, _ = _oracle(orc, a, b, prm, mode=1)
+    for _ in range(5):
+        c = of.Context(0)
+        u, v, st = of.tvl1(a, b, prm, c, stats=True)
+        c.close()
+        assert np.array_equal(st["iterations"], its)
+        assert np.array_equal(u, ou) and np.array_equal(v, ov)
+
+
 def test_known_answers_on_gpu(of, ctx):
     I = np.full((96, 128), 90, np.uint8)
     u, v = of.tvl1(I, I, of.TVL1Params(nscales=3, max_iterations=20), ctx)
