@@ -287,6 +287,7 @@ void run_tvl1(oflow_ctx *ctx, int n, const oflow_image *I0, const oflow_image *I
                 const cudaStream_t sc = ctx->side[c];
                 TvPlan &pl = side_plan(ctx, c, g.w, g.h, b1 - b0, g.dtype, *p);
                 ctx->last_tv.push_back(&pl);
+                pl.check_device_error();  // a failure of an earlier, unsynchronised call
                 OF_CUDA(cudaStreamWaitEvent(sc, ctx->fork, 0));
                 bind(pl, g, b0, b1, sc);
                 pl.run(sc);
@@ -298,6 +299,7 @@ void run_tvl1(oflow_ctx *ctx, int n, const oflow_image *I0, const oflow_image *I
         }
         TvPlan &pl = tv_plan(ctx, g.w, g.h, ng, g.dtype, *p, energy_trace != nullptr);
         if (!prof && !energy_trace) ctx->last_tv.push_back(&pl);
+        pl.check_device_error();  // a failure of an earlier, unsynchronised call
         bind(pl, g, 0, ng, st);
         if (prof)
             pl.profile(st, prof);
@@ -309,6 +311,7 @@ void run_tvl1(oflow_ctx *ctx, int n, const oflow_image *I0, const oflow_image *I
         if (energy_trace) pl.read_energy_trace(0, energy_trace, st);
     }
     finish(ctx, device_only);
+    for (TvPlan *pl : ctx->last_tv) pl->check_device_error();
 }
 
 }  // namespace
@@ -470,6 +473,7 @@ oflow_status oflow_tvl1_autotune(oflow_ctx *ctx, int n, const oflow_image *I0,
         pl.run(st);
         pl.autotune(st, &ctx->tune);
         OF_CUDA(cudaStreamSynchronize(st));
+        pl.check_device_error();
         if (cfg_per_scale)
             for (int s = 0; s < OFLOW_MAX_SCALES; s++)
                 cfg_per_scale[s] = s < pl.nscales() ? pl.tb_config(s) : -1;
@@ -589,6 +593,7 @@ oflow_status oflow_batch(oflow_ctx *ctx, int n, const oflow_job *jobs) {
                 if (j.out.location == OFLOW_HOST) device_only = false;
             }
         finish(ctx, device_only);
+        for (auto &t : mb->tv) t->check_device_error();
     });
 }
 
@@ -886,7 +891,8 @@ oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_
         wp->run(st);
         std::vector<double> ew(n), ep(n, 0.0);
         std::vector<int> acc(n, 1);
-        wp->true_energy(ew.data(), st);
+        wp->true_energy(ew.data(), st);  // synchronises
+        wp->check_device_error();
         if (stats)
             for (int b = 0; b < n; b++) wp->read_stats(b, &stats[b], st);
         TvPlan *pp = nullptr;
@@ -895,6 +901,7 @@ oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_
             for (int b = 0; b < n; b++) stage_pair_raw(*pp, b, I0[b], I1[b], st);
             pp->run(st);
             pp->true_energy(ep.data(), st);
+            pp->check_device_error();
             for (int b = 0; b < n; b++) acc[b] = ew[b] <= 1.01 * ep[b] ? 1 : 0;
         }
         for (int b = 0; b < n; b++) {
@@ -1044,6 +1051,7 @@ oflow_status oflow_stream_push(oflow_stream *s, const oflow_image *frames, const
         }
         s->frames++;
         finish(s->ctx, device_only);
+        if (s->tv) s->tv->check_device_error();
     });
 }
 

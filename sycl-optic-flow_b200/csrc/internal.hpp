@@ -79,6 +79,32 @@ class Arena {
     DevBuf buf_;
 };
 
+// An int in pinned host memory that kernels can set through its device
+// address: an error flag the host reads without synchronising.
+class HostFlag {
+  public:
+    HostFlag() {
+        OF_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&h_), sizeof(int), cudaHostAllocMapped));
+        *h_ = 0;
+        OF_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void **>(&d_), h_, 0));
+    }
+    ~HostFlag() {
+        if (h_) cudaFreeHost(h_);
+    }
+    HostFlag(const HostFlag &) = delete;
+    HostFlag &operator=(const HostFlag &) = delete;
+    int *device() const { return d_; }
+    // the flag's value, cleared
+    int take() {
+        const int v = *reinterpret_cast<volatile int *>(h_);
+        if (v) *reinterpret_cast<volatile int *>(h_) = 0;
+        return v;
+    }
+
+  private:
+    int *h_ = nullptr, *d_ = nullptr;
+};
+
 // A captured launch sequence replayed as one CUDA graph.
 class Graph {
   public:

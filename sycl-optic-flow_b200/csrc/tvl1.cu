@@ -24,7 +24,10 @@
 // the whole schedule is captured into one CUDA graph.
 #include "common.cuh"
 #include "internal.hpp"
+#include "ptx.cuh"
 #include "tvl1.hpp"
+
+#include <cudaTypedefs.h>
 
 #include <cmath>
 #include <cstring>
@@ -623,6 +626,14 @@ struct TbArgs {
     int max_tiles;
     int *iters;
     int iter_stride, stage;
+    // TMA region loads (k_tvl1_tb): use_tma set when the maps below describe
+    // this level for the launched tile shape; err is set when a load's
+    // bounded wait gives up
+    int use_tma;
+    int *err;
+    CUtensorMap tmP;  // p: (2 nx, ny, pair, buffer) 8-byte elements
+    CUtensorMap tmU;  // u: (nx, ny, pair, buffer) 8-byte elements
+    CUtensorMap tmW;  // (I1wx, I1wy, rho_c, grad): (2 nx, ny, pair) 8-byte elements
 };
 
 // Visits the inclusive rectangle [x0,x1] x [y0,y1] of a region of width RW
@@ -775,28 +786,32 @@ __device__ __forceinline__ void tb_decide(const TbArgs &a, TvCtrl *ctrl, int b,
 }
 
 template <int TW, int TH, int K, int NT>
-__global__ void __launch_bounds__(NT, 2) k_tvl1_tb(TbArgs a) {
+__global__ void __launch_bounds__(NT, 2) k_tvl1_tb(const __grid_constant__ TbArgs a) {
     constexpr int RW = TW + 2 * K, RH = TH + 2 * K, RN = RW * RH;
-    extern __shared__ float4 tb_smem[];
+    extern __shared__ __align__(128) float4 tb_smem[];
     float4 *sP = tb_smem;                                  // RN
     float4 *sWR = sP + RN;                                 // RN
     float2 *sU = reinterpret_cast<float2 *>(sWR + RN);     // RN
 
     const int b = blockIdx.z;
     TvCtrl *ctrl = a.ctrl + b;
-    if (*((volatile int *)&ctrl->stop)) return;
-    const int cur = *((volatile int *)&ctrl->cur);
-    const int n0 = *((volatile int *)&ctrl->n);
-    const int redo = *((volatile int *)&ctrl->redo);
+    // The pair's control block changes in this launch only once all of the
+    // pair's blocks have read it (the last to arrive writes it), so the reads
+    // may be served from L1: blocks after the first on an SM, and the blocks of
+    // a pair that already stopped, leave without a trip to L2.
+    if (__ldca(&ctrl->stop)) return;
+    const int cur = __ldca(&ctrl->cur);
+    const int n0 = __ldca(&ctrl->n);
+    const int redo = __ldca(&ctrl->redo);
     const int kk = redo > 0 ? redo : imin(K, a.max_it - n0);
     // block-uniform: every block of the pair reads the same control block
     bool snaps = false;
     if (redo == 0) {
-        const float q = fminf(*((volatile float *)&ctrl->decay), 1.0f);
+        const float q = fminf(__ldca(&ctrl->decay), 1.0f);
         float qk = 1.0f;
 #pragma unroll
         for (int j = 1; j < K; j++) qk *= q;
-        snaps = *((volatile float *)&ctrl->last_err) * qk < kSnapMargin * a.eps2;
+        snaps = __ldca(&ctrl->last_err) * qk < kSnapMargin * a.eps2;
     }
     const int nx = a.nx, ny = a.ny;
     const size_t off = (size_t)b * a.stride;
@@ -812,22 +827,46 @@ __global__ void __launch_bounds__(NT, 2) k_tvl1_tb(TbArgs a) {
     const int ox = blockIdx.x * TW - K, oy = blockIdx.y * TH - K;
     const bool interior = ox >= 1 && oy >= 1 && ox + RW <= nx - 1 && oy + RH <= ny - 1;
 
-    // all loads of the region issued before any use
-    for (int i = threadIdx.x; i < RN; i += NT) {
-        const int x = ox + i % RW, y = oy + i / RW;
-        float4 p = make_float4(0.f, 0.f, 0.f, 0.f), w = p;
-        float2 u = make_float2(0.f, 0.f);
-        if (x >= 0 && x < nx && y >= 0 && y < ny) {
-            const size_t q = (size_t)y * nx + x;
-            p = Pin[q];
-            w = Wg[q];
-            u = Uin[q];
+    // the region: three TMA boxes (zero outside the level) completing on one
+    // mbarrier, or plain loads where no tensor maps describe the level
+    const uint32_t sbase = smem_u32(tb_smem);
+    if (a.use_tma && (sbase & 127u) == 0) {
+        __shared__ __align__(8) unsigned long long s_bar;
+        const uint32_t bar = smem_u32(&s_bar);
+        if (threadIdx.x == 0) {
+            mbar_init(bar, 1);
+            fence_mbar_init();
+            mbar_arrive_expect_tx(bar, (uint32_t)RN * 40u);
+            tma_load_4d(sbase, &a.tmP, 2 * ox, oy, b, cur, bar);
+            tma_load_3d(sbase + RN * 16, &a.tmW, 2 * ox, oy, b, bar);
+            tma_load_4d(sbase + RN * 32, &a.tmU, ox, oy, b, cur, bar);
         }
-        sP[i] = p;
-        sWR[i] = w;
-        sU[i] = u;
+        __syncthreads();  // the barrier is initialised before anyone waits on it
+        const bool ok = mbar_wait_bounded(bar, 0);
+        if (__syncthreads_or(!ok)) {
+            // give up this tile: report, let the copies land (bounded), leave
+            // without arriving (the host treats the plan's results as lost)
+            if (threadIdx.x == 0) atomicExch(a.err, 1);
+            mbar_wait_bounded(bar, 0);
+            return;
+        }
+    } else {
+        for (int i = threadIdx.x; i < RN; i += NT) {
+            const int x = ox + i % RW, y = oy + i / RW;
+            float4 p = make_float4(0.f, 0.f, 0.f, 0.f), w = p;
+            float2 u = make_float2(0.f, 0.f);
+            if (x >= 0 && x < nx && y >= 0 && y < ny) {
+                const size_t q = (size_t)y * nx + x;
+                p = Pin[q];
+                w = Wg[q];
+                u = Uin[q];
+            }
+            sP[i] = p;
+            sWR[i] = w;
+            sU[i] = u;
+        }
+        __syncthreads();
     }
-    __syncthreads();
 
     // the owned tile is exact after every iteration: store it
     auto store_owned = [&](float2 *__restrict__ Ud, float4 *__restrict__ Pd) {
@@ -852,8 +891,12 @@ __global__ void __launch_bounds__(NT, 2) k_tvl1_tb(TbArgs a) {
             else
                 tb_iteration<TW, TH, K, NT, false>(j + 1, sP, sWR, sU, ox, oy, nx, ny, a.l_t,
                                                    a.theta, a.taut, err[j]);
-            if (snaps && j + 1 < kk)  // snapshot: the state a stop after iteration j+1 accepts
+            if (snaps && j + 1 < kk) {  // snapshot: the state a stop after iteration j+1 accepts
                 store_owned(state_buf(a.U0, a.U1, snap + j) + off, state_buf(a.P0, a.P1, snap + j) + off);
+                // the next iteration updates u and p in place: every thread must
+                // have read its share of the snapshot first
+                __syncthreads();
+            }
         }
     }
     store_owned(Uout, Pout);
@@ -1079,6 +1122,56 @@ void launch_resample(const float *src, size_t sstride, int nx, int ny, float *ds
 }
 
 // ================================================================ host plan
+// cuTensorMapEncodeTiled, looked up in the driver once (null if unavailable).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// A tiled map of 8-byte elements, zero fill outside; dims innermost first,
+// byte strides of dims 1..rank-1.
+static bool encode_map8(CUtensorMap *m, void *base, int rank, const cuuint64_t *dims,
+                        const cuuint64_t *strides, const cuuint32_t *box) {
+    const PFN_cuTensorMapEncodeTiled_v12000 fn = tensor_map_encoder();
+    if (!fn) return false;
+    const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT64, (cuuint32_t)rank, base, dims, strides, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Tensor maps of k_tvl1_tb's region loads for tile configuration cfg on a
+// level of nx x ny (planes of N0 elements, B pairs, kStateBufs buffers of u
+// and p).  TMA wants 16-byte row and plane strides, so u (8 bytes a pixel)
+// needs even nx and N0; otherwise the kernel loads the region itself.
+static void tb_maps(TbArgs &ta, int cfg, int nx, int ny, int B, size_t N0, float4 *P0, float2 *U0,
+                    const float4 *WR, int *err) {
+    ta.use_tma = 0;
+    ta.err = err;
+    if (cfg >= kTbNumCfgs || (nx & 1) || (N0 & 1)) return;
+    const cuuint32_t rw = (cuuint32_t)(kTbCfgs[cfg].tw + 2 * kTbK), rh = (cuuint32_t)(kTbCfgs[cfg].th + 2 * kTbK);
+    const cuuint64_t X = (cuuint64_t)nx, Y = (cuuint64_t)ny, NB = (cuuint64_t)B, N = N0;
+    const cuuint64_t dp[4] = {2 * X, Y, NB, (cuuint64_t)kStateBufs}, sp[3] = {16 * X, 16 * N, 16 * N * NB};
+    const cuuint32_t bp[4] = {2 * rw, rh, 1, 1};
+    const cuuint64_t du[4] = {X, Y, NB, (cuuint64_t)kStateBufs}, su[3] = {8 * X, 8 * N, 8 * N * NB};
+    const cuuint32_t bu[4] = {rw, rh, 1, 1};
+    const cuuint64_t dw[3] = {2 * X, Y, NB}, sw[2] = {16 * X, 16 * N};
+    const cuuint32_t bw[3] = {2 * rw, rh, 1};
+    ta.use_tma = encode_map8(&ta.tmP, P0, 4, dp, sp, bp) && encode_map8(&ta.tmU, U0, 4, du, su, bu) &&
+                 encode_map8(&ta.tmW, const_cast<float4 *>(WR), 3, dw, sw, bw);
+}
+
+void TvPlan::check_device_error() {
+    if (err_.take()) throw Error(OFLOW_ERR_TIMEOUT, "tvl1: a tile's TMA load gave up its bounded wait");
+}
+
 template <int TW, int TH, int NT>
 static void tb_launch(dim3 g, cudaStream_t st, const TbArgs &ta) {
     k_tvl1_tb<TW, TH, kTbK, NT><<<g, NT, tb_smem_bytes(TW, TH), st>>>(ta);
@@ -1332,6 +1425,7 @@ void TvPlan::record(cudaStream_t st) {
                 TbArgs ta{WR, U0, U1, P0, P1, N0, nx, ny, prm_.max_iterations, l_t,
                           prm_.theta, taut, eps2, ctrl, part, max_blocks_ / kTbK, iters,
                           iter_stride_, ia.stage};
+                tb_maps(ta, cfg, nx, ny, B, N0, P0, U0, WR, err_.device());
                 dim3 tg(div_up(nx, kTbCfgs[cfg].tw), div_up(ny, kTbCfgs[cfg].th), B);
                 const int nl = iter_launches_per_stage();
                 if (cfg == kLevelCfg) {
@@ -1472,6 +1566,7 @@ void TvPlan::autotune(cudaStream_t st, TuneTable *table, int reps) {
                           nx, ny, c == kLevelCfg ? iters_run : 1 << 30, l_t, prm_.theta, taut, -1.0f,
                           ctrl, ar_.at<double>(o_part_), max_blocks_ / kTbK, ar_.at<int>(o_iters_),
                           iter_stride_, 0};
+                tb_maps(ta, c, nx, ny, B_, N0, pbuf(0), ubuf(0), ar_.at<float4>(o_WR_), err_.device());
                 dim3 tg(div_up(nx, kTbCfgs[c].tw), div_up(ny, kTbCfgs[c].th), B_);
                 float ms_min = 1e30f;
                 for (int r = 0; r <= reps; r++) {  // first launch warms up

@@ -101,6 +101,9 @@ class TvPlan {
     bool traced() const { return trace_; }
     const oflow_tvl1_params &params() const { return prm_; }
     size_t device_bytes() const { return ar_.size(); }
+    // Throws OFLOW_ERR_TIMEOUT if a kernel of this plan gave up a bounded wait
+    // (a tile's TMA load) since the last check; reads host memory only.
+    void check_device_error();
 
   private:
     int w_, h_, B_, dtype_;
@@ -133,6 +136,7 @@ class TvPlan {
     Graph graph_;
     int graph_launches_ = 0;
     std::vector<FrameRef> frames_;  // [B][2], host copy of the device table
+    HostFlag err_;
     size_t o_frames_ = 0;
     void upload_frames(cudaStream_t st);
 };
