@@ -553,45 +553,73 @@ oflow_status oflow_batch(oflow_ctx *ctx, int n, const oflow_job *jobs) {
         }
         const cudaStream_t st = ctx->stream();
         const size_t G = mb->kind.size();
-        // stage inputs (outside the graph: host copies from pageable memory)
-        for (size_t g = 0; g < G; g++)
+        auto stage = [&](size_t g, cudaStream_t s) {
             for (size_t b = 0; b < mb->members[g].size(); b++) {
                 const oflow_job &j = jobs[mb->members[g][b]];
                 void *d0 = mb->kind[g] == OFLOW_SOLVER_TVL1 ? mb->tv[mb->slot[g]]->raw_input((int)b, 0)
                                                             : mb->hs[mb->slot[g]]->raw_input((int)b, 0);
                 void *d1 = mb->kind[g] == OFLOW_SOLVER_TVL1 ? mb->tv[mb->slot[g]]->raw_input((int)b, 1)
                                                             : mb->hs[mb->slot[g]]->raw_input((int)b, 1);
-                stage_image(j.I0, d0, dtype_size(j.I0.dtype), st);
-                stage_image(j.I1, d1, dtype_size(j.I1.dtype), st);
+                stage_image(j.I0, d0, dtype_size(j.I0.dtype), s);
+                stage_image(j.I1, d1, dtype_size(j.I1.dtype), s);
             }
-        if (!mb->graph.ready()) {
-            mb->graph.capture(st, [&](cudaStream_t s) {
-                cudaEvent_t fork = mb->events.back();
-                OF_CUDA(cudaEventRecord(fork, s));
-                for (size_t g = 0; g < G; g++) {
-                    OF_CUDA(cudaStreamWaitEvent(mb->streams[g], fork, 0));
-                    if (mb->kind[g] == OFLOW_SOLVER_TVL1)
-                        mb->tv[mb->slot[g]]->record(mb->streams[g]);
-                    else
-                        mb->hs[mb->slot[g]]->record(mb->streams[g]);
-                    OF_CUDA(cudaEventRecord(mb->events[g], mb->streams[g]));
-                    OF_CUDA(cudaStreamWaitEvent(s, mb->events[g], 0));
-                }
-            });
-        }
-        mb->graph.launch(st);
+        };
         bool device_only = true;
-        for (size_t g = 0; g < G; g++)
+        auto unstage = [&](size_t g, cudaStream_t s) {
             for (size_t b = 0; b < mb->members[g].size(); b++) {
                 const oflow_job &j = jobs[mb->members[g][b]];
                 const float *ou = mb->kind[g] == OFLOW_SOLVER_TVL1 ? mb->tv[mb->slot[g]]->out_u((int)b)
                                                                    : mb->hs[mb->slot[g]]->out_u((int)b);
                 const float *ov = mb->kind[g] == OFLOW_SOLVER_TVL1 ? mb->tv[mb->slot[g]]->out_v((int)b)
                                                                    : mb->hs[mb->slot[g]]->out_v((int)b);
-                unstage_plane(ou, j.I0.width, j.I0.height, j.out.u, j.out.pitch, j.out.location, st);
-                unstage_plane(ov, j.I0.width, j.I0.height, j.out.v, j.out.pitch, j.out.location, st);
+                unstage_plane(ou, j.I0.width, j.I0.height, j.out.u, j.out.pitch, j.out.location, s);
+                unstage_plane(ov, j.I0.width, j.I0.height, j.out.v, j.out.pitch, j.out.location, s);
                 if (j.out.location == OFLOW_HOST) device_only = false;
             }
+        };
+        bool host_io = false;
+        for (int i = 0; i < n; i++)
+            host_io = host_io || jobs[i].I0.location == OFLOW_HOST || jobs[i].I1.location == OFLOW_HOST ||
+                      jobs[i].out.location == OFLOW_HOST;
+        if (host_io) {
+            // each group on its own stream: its copies in and out overlap the
+            // other groups' solves (each plan replays its own graph)
+            cudaEvent_t fork = mb->events.back();
+            OF_CUDA(cudaEventRecord(fork, st));
+            for (size_t g = 0; g < G; g++) {
+                const cudaStream_t sg = mb->streams[g];
+                OF_CUDA(cudaStreamWaitEvent(sg, fork, 0));
+                stage(g, sg);
+                if (mb->kind[g] == OFLOW_SOLVER_TVL1)
+                    mb->tv[mb->slot[g]]->run(sg);
+                else
+                    mb->hs[mb->slot[g]]->run(sg);
+                unstage(g, sg);
+                OF_CUDA(cudaEventRecord(mb->events[g], sg));
+                OF_CUDA(cudaStreamWaitEvent(st, mb->events[g], 0));
+            }
+        } else {
+            // device buffers: copies on the context stream, then all groups as
+            // the branches of one graph
+            for (size_t g = 0; g < G; g++) stage(g, st);
+            if (!mb->graph.ready()) {
+                mb->graph.capture(st, [&](cudaStream_t s) {
+                    cudaEvent_t fork = mb->events.back();
+                    OF_CUDA(cudaEventRecord(fork, s));
+                    for (size_t g = 0; g < G; g++) {
+                        OF_CUDA(cudaStreamWaitEvent(mb->streams[g], fork, 0));
+                        if (mb->kind[g] == OFLOW_SOLVER_TVL1)
+                            mb->tv[mb->slot[g]]->record(mb->streams[g]);
+                        else
+                            mb->hs[mb->slot[g]]->record(mb->streams[g]);
+                        OF_CUDA(cudaEventRecord(mb->events[g], mb->streams[g]));
+                        OF_CUDA(cudaStreamWaitEvent(s, mb->events[g], 0));
+                    }
+                });
+            }
+            mb->graph.launch(st);
+            for (size_t g = 0; g < G; g++) unstage(g, st);
+        }
         finish(ctx, device_only);
         for (auto &t : mb->tv) t->check_device_error();
     });

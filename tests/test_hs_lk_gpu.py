@@ -161,3 +161,10 @@ def test_mixed_batch_matches_single_solves(of, ctx):
         for (solver, a, b, prm), (u, v) in zip(jobs, res):
             su, sv = (of.tvl1 if solver == "tvl1" else of.hs)(a, b, prm, ctx)
             assert _same(u, su) and _same(v, sv)
+    # host buffers run each group on its own stream, device buffers as one
+    # multi-branch graph: same flows
+    import torch
+    djobs = [(s_, torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda(), p_) for s_, a, b, p_ in jobs]
+    for _ in range(2):
+        for (u, v), (du, dv) in zip(res, of.batch(djobs, ctx)):
+            assert _same(u, du.cpu().numpy()) and _same(v, dv.cpu().numpy())
