@@ -26,39 +26,59 @@ namespace {
 
 constexpr int kColorNT = 128;
 
-__device__ __forceinline__ uint32_t sat_u8(float x) {
-    if (!(x == x)) return 0u;
-    const float r = rintf(x);
-    if (r <= 0.0f) return 0u;
-    if (r >= 255.0f) return 255u;
-    return (uint32_t)r;
+// Rounding to an integer without the conversion pipe: for |x| < 2^22,
+// x + 1.5*2^23 rounds x to an integer (nearest even, as rintf), whose value
+// sits in the low mantissa bits.  Returns that integer and sets r = rintf(x).
+constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23
+constexpr int kMagicBits = 0x4B400000;
+__device__ __forceinline__ int rint_small(float x, float &r) {
+    const float t = x + kMagic;
+    r = t - kMagic;
+    return __float_as_int(t) - kMagicBits;
+}
+// floorf(x) for 0 <= |x| < 2^22, as a float and an integer
+__device__ __forceinline__ int floor_small(float x, float &fl) {
+    float r;
+    const int k = rint_small(x, r);
+    const bool over = r > x;
+    fl = over ? r - 1.0f : r;
+    return over ? k - 1 : k;
 }
 
-// B | G << 8 | R << 16 of one flow vector
+// B | G << 8 | R << 16 of one flow vector.  Every byte is the 8-bit saturating
+// round-to-nearest-even conversion of the reference; the operands are known to
+// lie in [0, 255] (V after its clamp, the colour channels) or in [-91, 91]
+// (the hue), so rint_small replaces rintf and the float<->int conversions.
 __device__ __forceinline__ uint32_t flow_bgr(float fu, float fv) {
     const float hue_scale = (float)(180.0 / 3.14159265358979323846 / 2.0);
     const float mag = sqrtf(fu * fu + fv * fv);
     float m = mag * 10.0f;
     if (m > 255.0f) m = 255.0f;
-    const uint32_t V = sat_u8(m);
+    float vr;  // the V byte as a float
+    rint_small(m, vr);
+    if (!(m == m)) vr = 0.0f;  // NaN converts to 0
     // hue byte = rint(RN(RN(atan2) * scale)) with atan2 correctly rounded to
     // float.  atan2f is within 3 ulp (CUDA's documented bound), which moves
     // the scaled angle (|.| <= 90) by less than 3.5e-5 including the product's
     // rounding; only when that lies within 1e-4 of a rounding boundary k + 1/2
     // can the byte differ, and then the double-precision atan2 decides.
     float hf = atan2f(fv, fu) * hue_scale;
-    if (fabsf(hf - (floorf(hf) + 0.5f)) < 1e-4f || !(fabsf(hf) <= 91.0f))
+    float fl;
+    floor_small(hf, fl);
+    if (fabsf(hf - (fl + 0.5f)) < 1e-4f || !(fabsf(hf) <= 91.0f))
         hf = (float)atan2((double)fv, (double)fu) * hue_scale;
-    const uint32_t H = sat_u8(hf);
-    const float hh = (float)H * (6.0f / 180.0f);
-    int sector = (int)floorf(hh);
-    float f = hh - (float)sector;
+    float hr;  // the H byte as a float
+    if (rint_small(hf, hr) < 0 || !(hf == hf)) hr = 0.0f;  // negative angles and NaN saturate to 0
+    const float hh = hr * (6.0f / 180.0f);
+    float sf;
+    int sector = floor_small(hh, sf);
+    float f = hh - sf;
     if (sector < 0 || sector > 5) {
         sector = 0;
         f = 0.0f;
     }
     const float s = 255.0f * (1.0f / 255.0f);
-    const float vv = (float)V * (1.0f / 255.0f);
+    const float vv = vr * (1.0f / 255.0f);
     const float p = vv * (1.0f - s), q = vv * (1.0f - s * f), t = vv * (1.0f - s * (1.0f - f));
     float r, g, b;
     switch (sector) {
@@ -69,7 +89,11 @@ __device__ __forceinline__ uint32_t flow_bgr(float fu, float fv) {
         case 4: r = t; g = p; b = vv; break;
         default: r = vv; g = p; b = q; break;
     }
-    return sat_u8(b * 255.0f) | (sat_u8(g * 255.0f) << 8) | (sat_u8(r * 255.0f) << 16);
+    float unused;
+    const uint32_t B8 = (uint32_t)rint_small(b * 255.0f, unused);
+    const uint32_t G8 = (uint32_t)rint_small(g * 255.0f, unused);
+    const uint32_t R8 = (uint32_t)rint_small(r * 255.0f, unused);
+    return B8 | (G8 << 8) | (R8 << 16);
 }
 
 __global__ void __launch_bounds__(kColorNT) k_flow_to_color(ColorJobs jobs) {
