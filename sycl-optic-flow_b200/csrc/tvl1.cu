@@ -362,7 +362,10 @@ __global__ void k_grad_pack(const float *__restrict__ pyr, size_t pyr_stride, in
 // With first_warp, p is zeroed (tvl1.cpp:190-193).
 enum { kWarpFromU = 0, kWarpFromUz = 1, kWarpZero = 2 };
 
-__global__ void k_warp(const float *__restrict__ pyr, size_t pyr_stride, const float4 *I1g,
+// 6 blocks of 256 per SM (40 registers, a few spilled): the 16-tap gathers
+// need the warps to hide their latency.  The 25 warps of the 1024x436 workload
+// took 3.74 ms at 3 blocks (66 registers), 3.14 at 5, 3.05 at 6, 3.75 at 8.
+__global__ void __launch_bounds__(256, 6) k_warp(const float *__restrict__ pyr, size_t pyr_stride, const float4 *I1g,
                        float4 *WR, float2 *U0, float2 *U1, const float2 *Uz, float4 *P0,
                        float4 *P1, size_t stride, int nx, int ny, int mode, int first_warp,
                        TvCtrl *ctrl) {
