@@ -1,6 +1,6 @@
 """TV-L1 on the GPU through the C ABI against the oracle and the reference.
 
-Tolerances (north star): max |du|,|dv| <= 1e-3 px and |dEPE| <= 1e-4 px after
+Tolerances against the compiled reference: max |du|,|dv| <= 1e-3 px and |dEPE| <= 1e-4 px after
 the full solve; per-iteration energy within 1e-5 relative.  Against the C
 restatement with the same error-sum rounding (one rounding of a double sum)
 the kernels are bit-identical, and that is asserted where it holds by
