@@ -27,6 +27,7 @@
 #include "ptx.cuh"
 #include "tvl1.hpp"
 
+#include <cooperative_groups.h>
 #include <cudaTypedefs.h>
 
 #include <cmath>
@@ -49,7 +50,16 @@ constexpr int kTbNumCfgs = 4;
 // Configuration 4: the whole level of a pair in one block (k_tvl1_level), for
 // levels of at most kLvMaxPx pixels.
 constexpr int kLevelCfg = 4;
-constexpr int kNumIterCfgs = 5;
+// Configuration 5: the whole level of a pair in row bands over a cluster of
+// kClC blocks (k_tvl1_cluster), for levels whose band fits shared memory.
+constexpr int kClusterCfg = 5;
+constexpr int kNumIterCfgs = 6;
+constexpr int kClC = 4, kClNT = 512;
+constexpr size_t kClMaxSmem = 200 * 1024;
+__host__ __device__ inline int cl_band_rows(int ny) { return (ny + kClC - 1) / kClC; }
+inline bool cluster_fits(int nx, int ny) {
+    return ny >= 2 * kClC && (size_t)cl_band_rows(ny) * nx * 24 <= kClMaxSmem;
+}
 constexpr int kLvNT = 1024;
 constexpr int kLvMaxPx = 9216;  // u (8 B) + p (16 B) per pixel: 221,184 B of shared memory
 inline bool level_fits(int nx, int ny) { return (long long)nx * ny <= kLvMaxPx; }
@@ -996,6 +1006,107 @@ __global__ void __launch_bounds__(kLvNT) k_tvl1_level(TbArgs a) {
     }
 }
 
+// ---------------------------------------------------------------- level per cluster
+// A level split into row bands over a cluster of kClC blocks, one cluster per
+// pair: for levels that one block runs too slowly and tiles leave most SMs
+// idle.  Each block keeps its band's u and p in shared memory and reads the one
+// neighbouring row it needs -- p of the row above its band, u of the row below
+// it -- from the adjacent block's shared memory (distributed shared memory).
+// Per inner iteration the cluster synchronises twice: after the TH step and u
+// update (u new everywhere, the bands' squared-change sums posted) and after
+// the dual update (p new everywhere).  Every block adds the bands' sums in rank
+// order from the others' shared memory, so all take the same stopping decision
+// (tvl1.cpp:216) and run the same number of cluster barriers.  The per-pixel
+// arithmetic is th_u_update and dual_update, as in the tiled kernels.
+__global__ void __cluster_dims__(kClC, 1, 1) __launch_bounds__(kClNT) k_tvl1_cluster(TbArgs a) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int c = (int)cluster.block_rank();
+    extern __shared__ float4 cl_smem[];
+    __shared__ double sred[kClNT / 32];
+    __shared__ double s_part;
+    const int nx = a.nx, ny = a.ny, tid = threadIdx.x;
+    const int r0 = c * ny / kClC, r1 = (c + 1) * ny / kClC, nb = r1 - r0;
+    float4 *sP = cl_smem;
+    float2 *sU = reinterpret_cast<float2 *>(sP + (size_t)cl_band_rows(ny) * nx);
+    const int b = blockIdx.y;
+    TvCtrl *ctrl = a.ctrl + b;
+    const int cur = *((volatile int *)&ctrl->cur);
+    const int fin = cur == 0 ? 1 : 0;
+    const size_t off = (size_t)b * a.stride;
+    const float2 *__restrict__ Uin = state_buf(a.U0, a.U1, cur) + off + (size_t)r0 * nx;
+    const float4 *__restrict__ Pin = state_buf(a.P0, a.P1, cur) + off + (size_t)r0 * nx;
+    const float4 *__restrict__ Wg = a.WR + off;
+    const int N = nb * nx;
+    for (int i = tid; i < N; i += kClNT) {
+        sU[i] = Uin[i];
+        sP[i] = Pin[i];
+    }
+    // the neighbours' rows: p of the band above (its last row), u of the band below (its first)
+    const int nb_up = c > 0 ? r0 - (c - 1) * ny / kClC : 0;
+    const float4 *upP = c > 0 ? cluster.map_shared_rank(sP, c - 1) + (size_t)(nb_up - 1) * nx : nullptr;
+    const float2 *dnU = c + 1 < kClC ? cluster.map_shared_rank(sU, c + 1) : nullptr;
+    cluster.sync();
+    int n = *((volatile int *)&ctrl->n);
+    bool done = n >= a.max_it;
+    while (!done) {
+        double err = 0.0;
+        for (int i = tid; i < N; i += kClNT) {
+            const int ly = i / nx, x = i - ly * nx, y = r0 + ly;
+            const float2 u = sU[i];
+            const float4 pc = sP[i];
+            const float4 pl = x > 0 ? sP[i - 1] : pc;  // unused on the left border
+            const float4 pu = y == 0 ? pc : (ly > 0 ? sP[i - nx] : upP[x]);  // unused on the top border
+            const float2 un = th_u_update(u, __ldg(Wg + (size_t)y * nx + x), pc, pl, pu, x == 0,
+                                          x == nx - 1, y == 0, y == ny - 1, a.l_t, a.theta);
+            sU[i] = un;
+            const float e1 = un.x - u.x, e2 = un.y - u.y;
+            const float term = e1 * e1 + e2 * e2;
+            err += (double)term;
+        }
+        const double bs = block_sum_double<kClNT>(err, sred);
+        if (tid == 0) s_part = bs;
+        cluster.sync();  // u new in every band, the bands' sums posted
+        double tot = 0.0;
+#pragma unroll
+        for (int k = 0; k < kClC; k++) tot += *cluster.map_shared_rank(&s_part, k);
+        n++;
+        float e = (float)tot;
+        e = e / (float)(nx * ny);
+        const bool stop = !(e > a.eps2) || n >= a.max_it;
+        for (int i = tid; i < N; i += kClNT) {
+            const int ly = i / nx, x = i - ly * nx, y = r0 + ly;
+            const float2 uc = sU[i];
+            float f1x = 0.0f, f2x = 0.0f, f1y = 0.0f, f2y = 0.0f;
+            if (x < nx - 1) {
+                const float2 ur = sU[i + 1];
+                f1x = ur.x - uc.x;
+                f2x = ur.y - uc.y;
+            }
+            if (y < ny - 1) {
+                const float2 ud = ly + 1 < nb ? sU[i + nx] : dnU[x];
+                f1y = ud.x - uc.x;
+                f2y = ud.y - uc.y;
+            }
+            sP[i] = dual_update(sP[i], f1x, f1y, f2x, f2y, a.taut);
+        }
+        cluster.sync();  // p new in every band; the sums may be overwritten
+        done = stop;
+    }
+    float2 *__restrict__ Uout = state_buf(a.U0, a.U1, fin) + off + (size_t)r0 * nx;
+    float4 *__restrict__ Pout = state_buf(a.P0, a.P1, fin) + off + (size_t)r0 * nx;
+    for (int i = tid; i < N; i += kClNT) {
+        Uout[i] = sU[i];
+        Pout[i] = sP[i];
+    }
+    if (c == 0 && tid == 0) {
+        ctrl->n = n;
+        ctrl->cur = fin;
+        ctrl->stop = 1;
+        a.iters[(size_t)b * a.iter_stride + a.stage] = n;
+    }
+}
+
 // ---------------------------------------------------------------- energy
 // E = sum |grad u1| + |grad u2| (forward differences, double) + lambda *
 // sum |rho(u)| with rho linearised at the current warp.  Last block of a pair
@@ -1181,6 +1292,11 @@ static void tb_launch(dim3 g, cudaStream_t st, const TbArgs &ta) {
 }
 
 static void tb_launch_cfg(int cfg, dim3 g, cudaStream_t st, const TbArgs &ta) {
+    if (cfg == kClusterCfg) {
+        const size_t smem = (size_t)cl_band_rows(ta.ny) * ta.nx * (sizeof(float4) + sizeof(float2));
+        k_tvl1_cluster<<<dim3(kClC, g.z), kClNT, smem, st>>>(ta);
+        return;
+    }
     if (cfg == kLevelCfg) {
         const size_t smem = (size_t)ta.nx * ta.ny * (sizeof(float4) + sizeof(float2));
         k_tvl1_level<<<g.z, kLvNT, smem, st>>>(ta);
@@ -1201,10 +1317,12 @@ static void tb_set_smem_attrs() {
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tb_smem_bytes(64, 16)));
     OF_CUDA(cudaFuncSetAttribute(k_tvl1_level, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  kLvMaxPx * (int)(sizeof(float4) + sizeof(float2))));
+    OF_CUDA(cudaFuncSetAttribute(k_tvl1_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kClMaxSmem));
 }
 
 static int tb_tiles(int cfg, int nx, int ny) {
-    if (cfg == kLevelCfg) return 1;
+    if (cfg == kLevelCfg || cfg == kClusterCfg) return 1;
     return div_up(nx, kTbCfgs[cfg].tw) * div_up(ny, kTbCfgs[cfg].th);
 }
 
@@ -1216,6 +1334,7 @@ static int tb_pick(int nx, int ny, int B) {
         const int c = atoi(e);
         if (c >= 0 && c < kTbNumCfgs) return c;
         if (c == kLevelCfg && level_fits(nx, ny)) return c;
+        if (c == kClusterCfg && cluster_fits(nx, ny)) return c;
     }
     if (level_fits(nx, ny)) return kLevelCfg;
     for (int c = 0; c < kTbNumCfgs; c++)
@@ -1225,7 +1344,8 @@ static int tb_pick(int nx, int ny, int B) {
 
 // a configuration from a tuning table, if it is valid for this level
 static bool cfg_valid(int c, int nx, int ny) {
-    return (c >= 0 && c < kTbNumCfgs) || (c == kLevelCfg && level_fits(nx, ny));
+    return (c >= 0 && c < kTbNumCfgs) || (c == kLevelCfg && level_fits(nx, ny)) ||
+           (c == kClusterCfg && cluster_fits(nx, ny));
 }
 
 TvPlan::TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, bool trace,
@@ -1429,9 +1549,10 @@ void TvPlan::record(cudaStream_t st) {
                           prm_.theta, taut, eps2, ctrl, part, max_blocks_ / kTbK, iters,
                           iter_stride_, ia.stage};
                 tb_maps(ta, cfg, nx, ny, B, N0, P0, U0, WR, err_.device());
-                dim3 tg(div_up(nx, kTbCfgs[cfg].tw), div_up(ny, kTbCfgs[cfg].th), B);
+                const dim3 tg = cfg < kTbNumCfgs ? dim3(div_up(nx, kTbCfgs[cfg].tw), div_up(ny, kTbCfgs[cfg].th), B)
+                                                 : dim3(1, 1, B);
                 const int nl = iter_launches_per_stage();
-                if (cfg == kLevelCfg) {
+                if (cfg == kLevelCfg || cfg == kClusterCfg) {
                     // the whole stage in one launch; the profile keeps one
                     // (empty) event pair for each slot of the tiled schedule
                     for (int it = 0; it < nl; it++) {
@@ -1563,14 +1684,16 @@ void TvPlan::autotune(cudaStream_t st, TuneTable *table, int reps) {
                 if (!cfg_valid(c, nx, ny)) continue;
                 // per-iteration time: a tiled launch runs K iterations (no
                 // stop); the whole-level kernel is given 2K
-                const int iters_run = c == kLevelCfg ? 2 * kTbK : kTbK;
+                const bool whole = c == kLevelCfg || c == kClusterCfg;
+                const int iters_run = whole ? 2 * kTbK : kTbK;
                 TbArgs ta{ar_.at<float4>(o_WR_), ubuf(0), ubuf(1), pbuf(0),
                           pbuf(1), N0,
-                          nx, ny, c == kLevelCfg ? iters_run : 1 << 30, l_t, prm_.theta, taut, -1.0f,
+                          nx, ny, whole ? iters_run : 1 << 30, l_t, prm_.theta, taut, -1.0f,
                           ctrl, ar_.at<double>(o_part_), max_blocks_ / kTbK, ar_.at<int>(o_iters_),
                           iter_stride_, 0};
                 tb_maps(ta, c, nx, ny, B_, N0, pbuf(0), ubuf(0), ar_.at<float4>(o_WR_), err_.device());
-                dim3 tg(div_up(nx, kTbCfgs[c].tw), div_up(ny, kTbCfgs[c].th), B_);
+                const dim3 tg = c < kTbNumCfgs ? dim3(div_up(nx, kTbCfgs[c].tw), div_up(ny, kTbCfgs[c].th), B_)
+                                               : dim3(1, 1, B_);
                 float ms_min = 1e30f;
                 for (int r = 0; r <= reps; r++) {  // first launch warms up
                     k_ctrl_rearm<<<div_up(B_, 128), 128, 0, st>>>(ctrl, B_);

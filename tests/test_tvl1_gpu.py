@@ -214,12 +214,13 @@ def test_full_size_workload_against_oracle_and_reference(of, orc, ctx):
     assert synth.epe(u, v, p.u, p.v, p.valid, 8) < 0.5
 
 
-@pytest.mark.parametrize("cfg", [None, "3"])
+@pytest.mark.parametrize("cfg", [None, "3", "5"])
 def test_repeated_full_size_solves_match_the_oracle(of, orc, monkeypatch, cfg):
     """Five solves of the 1024x436 pair, each on a fresh context (new plan,
-    new graph, reused device memory), with the tile shapes the plan picks and
-    with the smallest tile forced everywhere: every solve equals the oracle.
-    Catches order-dependent faults that a single solve can miss."""
+    new graph, reused device memory), with the tile shapes the plan picks,
+    with the smallest tile forced everywhere, and with the cluster kernel on
+    every level whose band fits (the three coarsest): every solve equals the
+    oracle.  Catches order-dependent faults that a single solve can miss."""
     if cfg:
         monkeypatch.setenv("OFLOW_TB_CFG", cfg)
     p, a, b = _pair(0, 1024, 436, radius=80.0)
@@ -284,7 +285,7 @@ def test_autotune_keeps_results_and_roundtrips(of, tmp_path):
     prm = of.TVL1Params(nscales=3, max_iterations=12)
     before = of.tvl1_batch(pairs, prm, ctx)
     cfg = of.tvl1_autotune(pairs, prm, ctx)
-    assert len(cfg) == 3 and all(0 <= c < 5 for c in cfg)  # 4: whole level per block
+    assert len(cfg) == 3 and all(0 <= c < 6 for c in cfg)  # 4, 5: whole level per block, per cluster
     after = of.tvl1_batch(pairs, prm, ctx)
     for (u0, v0), (u1, v1) in zip(before, after):
         assert np.array_equal(u0, u1) and np.array_equal(v0, v1)
