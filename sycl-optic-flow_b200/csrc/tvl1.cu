@@ -57,8 +57,9 @@ constexpr int kNumIterCfgs = 6;
 constexpr int kClC = 4, kClNT = 512;
 constexpr size_t kClMaxSmem = 200 * 1024;
 __host__ __device__ inline int cl_band_rows(int ny) { return (ny + kClC - 1) / kClC; }
+// u (8 B), p (16 B) and the warp data (16 B) of a band in shared memory
 inline bool cluster_fits(int nx, int ny) {
-    return ny >= 2 * kClC && (size_t)cl_band_rows(ny) * nx * 24 <= kClMaxSmem;
+    return ny >= 2 * kClC && (size_t)cl_band_rows(ny) * nx * 40 <= kClMaxSmem;
 }
 constexpr int kLvNT = 1024;
 constexpr int kLvMaxPx = 9216;  // u (8 B) + p (16 B) per pixel: 221,184 B of shared memory
@@ -1009,7 +1010,7 @@ __global__ void __launch_bounds__(kLvNT) k_tvl1_level(TbArgs a) {
 // ---------------------------------------------------------------- level per cluster
 // A level split into row bands over a cluster of kClC blocks, one cluster per
 // pair: for levels that one block runs too slowly and tiles leave most SMs
-// idle.  Each block keeps its band's u and p in shared memory and reads the one
+// idle.  Each block keeps its band's u, p and warp data in shared memory and reads the one
 // neighbouring row it needs -- p of the row above its band, u of the row below
 // it -- from the adjacent block's shared memory (distributed shared memory).
 // Per inner iteration the cluster synchronises twice: after the TH step and u
@@ -1027,8 +1028,10 @@ __global__ void __cluster_dims__(kClC, 1, 1) __launch_bounds__(kClNT) k_tvl1_clu
     __shared__ double s_part;
     const int nx = a.nx, ny = a.ny, tid = threadIdx.x;
     const int r0 = c * ny / kClC, r1 = (c + 1) * ny / kClC, nb = r1 - r0;
+    const size_t cap = (size_t)cl_band_rows(ny) * nx;
     float4 *sP = cl_smem;
-    float2 *sU = reinterpret_cast<float2 *>(sP + (size_t)cl_band_rows(ny) * nx);
+    float4 *sW = sP + cap;
+    float2 *sU = reinterpret_cast<float2 *>(sW + cap);
     const int b = blockIdx.y;
     TvCtrl *ctrl = a.ctrl + b;
     const int cur = *((volatile int *)&ctrl->cur);
@@ -1036,11 +1039,12 @@ __global__ void __cluster_dims__(kClC, 1, 1) __launch_bounds__(kClNT) k_tvl1_clu
     const size_t off = (size_t)b * a.stride;
     const float2 *__restrict__ Uin = state_buf(a.U0, a.U1, cur) + off + (size_t)r0 * nx;
     const float4 *__restrict__ Pin = state_buf(a.P0, a.P1, cur) + off + (size_t)r0 * nx;
-    const float4 *__restrict__ Wg = a.WR + off;
+    const float4 *__restrict__ Wg = a.WR + off + (size_t)r0 * nx;
     const int N = nb * nx;
     for (int i = tid; i < N; i += kClNT) {
         sU[i] = Uin[i];
         sP[i] = Pin[i];
+        sW[i] = Wg[i];
     }
     // the neighbours' rows: p of the band above (its last row), u of the band below (its first)
     const int nb_up = c > 0 ? r0 - (c - 1) * ny / kClC : 0;
@@ -1057,8 +1061,8 @@ __global__ void __cluster_dims__(kClC, 1, 1) __launch_bounds__(kClNT) k_tvl1_clu
             const float4 pc = sP[i];
             const float4 pl = x > 0 ? sP[i - 1] : pc;  // unused on the left border
             const float4 pu = y == 0 ? pc : (ly > 0 ? sP[i - nx] : upP[x]);  // unused on the top border
-            const float2 un = th_u_update(u, __ldg(Wg + (size_t)y * nx + x), pc, pl, pu, x == 0,
-                                          x == nx - 1, y == 0, y == ny - 1, a.l_t, a.theta);
+            const float2 un = th_u_update(u, sW[i], pc, pl, pu, x == 0, x == nx - 1, y == 0,
+                                          y == ny - 1, a.l_t, a.theta);
             sU[i] = un;
             const float e1 = un.x - u.x, e2 = un.y - u.y;
             const float term = e1 * e1 + e2 * e2;
@@ -1293,7 +1297,7 @@ static void tb_launch(dim3 g, cudaStream_t st, const TbArgs &ta) {
 
 static void tb_launch_cfg(int cfg, dim3 g, cudaStream_t st, const TbArgs &ta) {
     if (cfg == kClusterCfg) {
-        const size_t smem = (size_t)cl_band_rows(ta.ny) * ta.nx * (sizeof(float4) + sizeof(float2));
+        const size_t smem = (size_t)cl_band_rows(ta.ny) * ta.nx * (2 * sizeof(float4) + sizeof(float2));
         k_tvl1_cluster<<<dim3(kClC, g.z), kClNT, smem, st>>>(ta);
         return;
     }

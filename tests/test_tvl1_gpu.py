@@ -219,7 +219,7 @@ def test_repeated_full_size_solves_match_the_oracle(of, orc, monkeypatch, cfg):
     """Five solves of the 1024x436 pair, each on a fresh context (new plan,
     new graph, reused device memory), with the tile shapes the plan picks,
     with the smallest tile forced everywhere, and with the cluster kernel on
-    every level whose band fits (the three coarsest): every solve equals the
+    every level whose band fits (the two coarsest): every solve equals the
     oracle.  Catches order-dependent faults that a single solve can miss."""
     if cfg:
         monkeypatch.setenv("OFLOW_TB_CFG", cfg)
