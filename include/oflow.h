@@ -155,7 +155,7 @@ oflow_status oflow_tvl1_batch_profile(oflow_ctx *ctx, int n, const oflow_image *
  * inner-iteration configuration at every scale on the device and keeps the
  * fastest for plans of this size and batch: 0 = 64x32 tiles, 1 = 64x16,
  * 2 = 32x16, 3 = 16x8 (up to 4 iterations per launch), 4 = the whole level of
- * a pair in one block, 5 = the whole level in row bands over a cluster of 4
+ * a pair in one block, 5 = the whole level in row bands over a cluster of 8
  * blocks (4 and 5 where the level fits shared memory).
  * cfg_per_scale (OFLOW_MAX_SCALES ints, may be NULL) receives the choice per
  * scale, -1 past the last scale.  The table lives in the context; it can be

@@ -54,7 +54,7 @@ constexpr int kLevelCfg = 4;
 // kClC blocks (k_tvl1_cluster), for levels whose band fits shared memory.
 constexpr int kClusterCfg = 5;
 constexpr int kNumIterCfgs = 6;
-constexpr int kClC = 4, kClNT = 512;
+constexpr int kClC = 8, kClNT = 512;
 constexpr size_t kClMaxSmem = 200 * 1024;
 __host__ __device__ inline int cl_band_rows(int ny) { return (ny + kClC - 1) / kClC; }
 // u (8 B), p (16 B) and the warp data (16 B) of a band in shared memory
