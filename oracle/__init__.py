@@ -8,6 +8,10 @@ the CPU-baseline leg of bench.py (never by the product path):
   (src/tvl1/sequential) compiled from its sources in place by
   ``build_ref.sh``.  Present only where the reference checkout was available
   at build time (it travels with the tree as a built file).
+* ``_ref/libhslk_ref.so`` / ``_ref/libhslk_ref_stock.so`` -- the reference's
+  Horn-Schunck and Lucas-Kanade CUDA kernels (src/hs/cuda/kernels,
+  src/lk/cuda) behind ``ref_gpu_harness.cu``, built by ``build_ref.sh`` with
+  -fmad=false and with the reference's own flags.  They need a GPU.
 
 Arrays are numpy, row-major, C-contiguous float32 / uint8.
 """
@@ -23,6 +27,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libtvl1_ref.so")
+REFG_SO = {False: os.path.join(HERE, "_ref", "libhslk_ref.so"),
+           True: os.path.join(HERE, "_ref", "libhslk_ref_stock.so")}
 
 _f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
@@ -66,6 +72,7 @@ class TVL1Params:
 
 _orc = None
 _ref = None
+_refg = {}
 
 
 def orc_lib():
@@ -225,6 +232,61 @@ def hs(I0, I1, alpha=15.0, nlevels=1, nwarp=1, nsolver=200):
     return u, v
 
 
+def hs_downscale(src):
+    """2x2 box to (h//2, w//2), every pixel (D-H1)."""
+    src = _f32(src)
+    h, w = src.shape
+    out = np.zeros((h // 2, w // 2), np.float32)
+    orc_lib().orc_hs_downscale(src, w, h, out)
+    return out
+
+
+def hs_warp(src, u, v):
+    """Bilinear clamp-to-edge sample of src at (x+u, y+v) (D-H2)."""
+    src = _f32(src)
+    h, w = src.shape
+    out = np.zeros_like(src)
+    orc_lib().orc_hs_warp(src, _f32(u), _f32(v), w, h, out)
+    return out
+
+
+def hs_derivatives(I0, I1w):
+    """(Ix, Iy, Iz) with clamped 5-tap stencils (D-H3)."""
+    I0 = _f32(I0)
+    h, w = I0.shape
+    Ix, Iy, Iz = (np.zeros_like(I0) for _ in range(3))
+    orc_lib().orc_hs_derivatives(I0, _f32(I1w), w, h, Ix, Iy, Iz)
+    return Ix, Iy, Iz
+
+
+def hs_jacobi(du0, dv0, Ix, Iy, Iz, alpha):
+    """One Jacobi sweep; returns (du1, dv1)."""
+    du0 = _f32(du0)
+    h, w = du0.shape
+    du1 = np.zeros_like(du0)
+    dv1 = np.zeros_like(du0)
+    orc_lib().orc_hs_jacobi(du0, _f32(dv0), _f32(Ix), _f32(Iy), _f32(Iz), w, h, alpha, du1, dv1)
+    return du1, dv1
+
+
+def upscale(src, nw, nh, scale):
+    """Centre-aligned bilinear x2 upsample times `scale` (D-H4)."""
+    src = _f32(src)
+    h, w = src.shape
+    out = np.zeros((nh, nw), np.float32)
+    orc_lib().orc_upscale(src, w, h, nw, nh, scale, out)
+    return out
+
+
+def lk_filters(spac, temp):
+    """(spatial taps, temporal taps) of the restatement."""
+    fs = np.zeros(9, np.float32)
+    ft = np.zeros(9, np.float32)
+    if orc_lib().orc_lk_filters(spac, temp, fs, ft) != 0:
+        raise ValueError("oracle lk_filters: size without a tap table")
+    return fs[:spac], ft[:temp]
+
+
 def lk_ring(frames, iframe, spac=3, temp=2, window=5):
     """Single-step LK over a ring of `temp` uint8 frames (slot k = frames[k])."""
     fr = [np.ascontiguousarray(f, dtype=np.uint8) for f in frames]
@@ -286,3 +348,86 @@ def flow_to_color(u, v):
     out = np.zeros((h, w, 3), np.uint8)
     orc_lib().orc_flow_to_color(u, v, w, h, out.ctypes.data_as(C.c_void_p))
     return out
+
+
+# ------------------------------------------------- reference HS/LK CUDA kernels
+def refg_available(stock: bool = False) -> bool:
+    return os.path.exists(REFG_SO[stock])
+
+
+def refg_lib(stock: bool = False):
+    """The reference's HS/LK CUDA kernels behind ref_gpu_harness.cu.
+    stock=False: built with -fmad=false; stock=True: the reference's flags."""
+    if stock not in _refg:
+        path = REFG_SO[stock]
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        lib = C.CDLL(path)
+        lib.refg_device_count.restype = C.c_int
+        lib.refg_hs_downscale.argtypes = [_f32p, C.c_int, C.c_int, _f32p]
+        lib.refg_hs_jacobi.argtypes = [_f32p, _f32p, _f32p, C.c_int, C.c_int, C.c_int, C.c_float,
+                                       C.c_int, _f32p, _f32p]
+        lib.refg_hs_add.argtypes = [_f32p, _f32p, C.c_int, _f32p]
+        lib.refg_lk_filters.argtypes = [C.c_int, C.c_int, _f32p, _f32p, _f32p]
+        for fn in (lib.refg_lk_class, lib.refg_lk_parts):
+            fn.argtypes = [_u8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                           _f32p, _f32p, _f32p, _f32p, _f32p]
+        for fn in (lib.refg_hs_downscale, lib.refg_hs_jacobi, lib.refg_hs_add,
+                   lib.refg_lk_filters, lib.refg_lk_class, lib.refg_lk_parts):
+            fn.restype = C.c_int
+        _refg[stock] = lib
+    return _refg[stock]
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise RuntimeError(f"reference {what}: status {rc}")
+
+
+def refg_hs_downscale(src, stock=False):
+    """DownscaleKernel output (h//2, w//2); the last row and column, which the
+    kernel does not write, are NaN."""
+    src = _f32(src)
+    h, w = src.shape
+    out = np.full((h // 2, w // 2), np.nan, np.float32)
+    _check(refg_lib(stock).refg_hs_downscale(src, w, h, out), "Downscale")
+    return out
+
+
+def refg_hs_jacobi(Ix, Iy, Iz, alpha, nsweeps, stride=None, stock=False):
+    """nsweeps JacobiIteration<32,6> sweeps from zero; returns (du, dv)."""
+    Ix, Iy, Iz = _f32(Ix), _f32(Iy), _f32(Iz)
+    h, w = Ix.shape
+    du = np.zeros_like(Ix)
+    dv = np.zeros_like(Ix)
+    _check(refg_lib(stock).refg_hs_jacobi(Ix, Iy, Iz, w, h, stride or w, alpha, nsweeps, du, dv),
+           "SolveForUpdate")
+    return du, dv
+
+
+def refg_hs_add(a, b, stock=False):
+    a, b = _f32(a), _f32(b)
+    out = np.zeros_like(a)
+    _check(refg_lib(stock).refg_hs_add(a.ravel(), b.ravel(), a.size, out.ravel()), "Add")
+    return out
+
+
+def refg_lk_filters(spac, temp, stock=False):
+    fx = np.zeros(9, np.float32)
+    fy = np.zeros(9, np.float32)
+    ft = np.zeros(9, np.float32)
+    _check(refg_lib(stock).refg_lk_filters(spac, temp, fx, fy, ft), "getfilters")
+    return fx[:spac], fy[:spac], ft[:temp]
+
+
+def refg_lk(frames, iframe, spac=3, temp=2, window=5, whole_class=False, stock=False):
+    """The reference LK on a ring of `temp` uint8 frames (slot k = frames[k]).
+    whole_class=True runs LucasKanade::lucas_kanade (square frames only);
+    otherwise the kernel wrappers with the y-filter taken through the x-filter
+    on the transposed frame.  Returns (Vx, Vy, Ix, Iy, It)."""
+    ring = np.ascontiguousarray(np.stack([np.asarray(f, np.uint8) for f in frames]))
+    _, h, w = ring.shape
+    outs = [np.zeros((h, w), np.float32) for _ in range(5)]
+    fn = refg_lib(stock).refg_lk_class if whole_class else refg_lib(stock).refg_lk_parts
+    _check(fn(ring.ravel(), w, h, spac, temp, window, iframe, *outs), "lucas_kanade")
+    return tuple(outs)
