@@ -143,8 +143,8 @@ def algorithmic_bytes(stats_list, nx, ny):
     return tot
 
 
-def level_sizes(ns):
-    nx, ny = [W], [H]
+def level_sizes(ns, w=W, h=H):
+    nx, ny = [w], [h]
     for _ in range(1, ns):
         nx.append(int(float(nx[-1]) * 0.5 + 0.5))
         ny.append(int(float(ny[-1]) * 0.5 + 0.5))
@@ -152,40 +152,61 @@ def level_sizes(ns):
 
 
 # ------------------------------------------------------------- CPU baseline
-def cpu_worker(args):
-    """Runs in a subprocess: the reference's sequential TV-L1 (oracle/_ref,
-    OpenMP over all host threads) or, without it, the oracle port (one
-    thread), on up to --cpu-pairs pairs or --cpu-seconds of work."""
+BENCH_SEED0 = 10_000  # rank r solves seeds BENCH_SEED0 + r*P ... (multigpu.rank_seeds)
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def cpu_runner(threads):
+    """(kind, run(a, b)) for the reference's sequential TV-L1 (oracle/_ref,
+    OpenMP over `threads` threads) or, without it, the oracle port (one
+    thread)."""
     import numpy as np
     import oracle
-    pairs = make_pairs(1, 1000)
-    a, b, _ = pairs[0]
     prm = oracle.TVL1Params(**PARAMS)
     if oracle.ref_available():
-        kind, cores = "reference", int(os.environ.get("OMP_NUM_THREADS", "1"))
-        run = lambda: oracle.ref_tvl1(a, b, prm)
-    else:
-        kind, cores = "port", 1
-        run = lambda: oracle.tvl1(a.astype(np.float32), b.astype(np.float32), prm)
-    run()  # warm-up
+        return "reference", threads, lambda a, b: oracle.ref_tvl1(a, b, prm)
+    return "port", 1, lambda a, b: oracle.tvl1(a.astype(np.float32), b.astype(np.float32), prm)
+
+
+def cpu_worker(args):
+    """Runs in a subprocess (OMP_NUM_THREADS set by the parent): the CPU
+    implementation on the benchmark's own pairs (seeds BENCH_SEED0, +1, ...,
+    the pairs rank 0 of the GPU arm solves), one after another, up to
+    --cpu-pairs pairs or --cpu-seconds of work."""
+    threads = int(os.environ.get("OMP_NUM_THREADS", "1"))
+    kind, cores, run = cpu_runner(threads)
+    pairs = make_pairs(min(args.cpu_pairs, args.batch), BENCH_SEED0)
+    run(*pairs[0][:2])  # warm-up
     n, t0 = 0, time.perf_counter()
     times = []
     while n < args.cpu_pairs and (time.perf_counter() - t0) < args.cpu_seconds:
+        a, b, _ = pairs[n % len(pairs)]
         t = time.perf_counter()
-        run()
+        run(a, b)
         times.append(time.perf_counter() - t)
         n += 1
     el = time.perf_counter() - t0
     print(json.dumps({"value": n / el, "unit": "pairs/s", "cores": cores, "kind": kind,
-                      "sample": f"{n} pairs of the 1024x436 workload, {el:.1f} s, "
-                                f"median {1e3 * sorted(times)[len(times) // 2]:.0f} ms/pair"}))
+                      "sample": f"{n} pairs of the 1024x436 workload (generator seeds "
+                                f"{BENCH_SEED0}..{BENCH_SEED0 + min(n, len(pairs)) - 1}, the "
+                                f"GPU arm's first pairs), {el:.1f} s, median "
+                                f"{1e3 * sorted(times)[len(times) // 2]:.0f} ms/pair"}))
 
 
-def cpu_baseline(pairs=30, seconds=20.0, threads=None):
+def cpu_baseline(pairs=30, seconds=20.0, threads=None, batch=32):
     threads = threads or os.cpu_count() or 1
     env = dict(os.environ, OMP_NUM_THREADS=str(threads))
     cmd = [sys.executable, os.path.abspath(__file__), "--cpu-worker", "--cpu-pairs", str(pairs),
-           "--cpu-seconds", str(seconds)]
+           "--cpu-seconds", str(seconds), "--batch", str(batch)]
     out = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=600)
     if out.returncode != 0:
         log(out.stderr[-2000:])
@@ -195,27 +216,25 @@ def cpu_baseline(pairs=30, seconds=20.0, threads=None):
 
 # ------------------------------------------------------------- reference arm
 def reference_arm(args, rank):
+    """The reference's sequential TV-L1 on all host threads.  Step k solves
+    the benchmark pair k mod --batch (seeds BENCH_SEED0 ...): the same pairs,
+    in the same order, that rank 0 of the GPU arm solves in every step."""
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
     os.environ["OMP_NUM_THREADS"] = str(threads)
-    import numpy as np
-    import oracle
-    a, b, _ = make_pairs(1, 1000)[0]
-    prm = oracle.TVL1Params(**PARAMS)
-    if oracle.ref_available():
-        kind = "reference"
-        run = lambda: oracle.ref_tvl1(a, b, prm)
-    else:
-        kind, threads = "port", 1
-        run = lambda: oracle.tvl1(a.astype(np.float32), b.astype(np.float32), prm)
-    for _ in range(args.warmup):
-        run()
+    kind, threads, run = cpu_runner(threads)
+    n_pairs = min(args.batch, max(args.steps, args.warmup, 1))
+    pairs = make_pairs(n_pairs, BENCH_SEED0)
+    for k in range(args.warmup):
+        run(*pairs[k % n_pairs][:2])
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        run()
+    for k in range(args.steps):
+        run(*pairs[k % n_pairs][:2])
     el = time.perf_counter() - t0
     v = args.steps / el
+    sample = (f"{args.steps} pairs, one per step: generator seeds {BENCH_SEED0}.."
+              f"{BENCH_SEED0 + min(args.steps, n_pairs) - 1} (the GPU arm's pairs)")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "pairs/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
@@ -223,9 +242,10 @@ def reference_arm(args, rank):
         "data": "synthetic",
         "config": {"workload": "tvl1 1024x436, 5 scales x 5 warps x <=50 inner iterations, "
                                "1 uint8 pair per step", "solver": "reference sequential C++ "
-                               "(src/tvl1/sequential, OpenMP)"},
+                               "(src/tvl1/sequential, OpenMP)",
+                   "pairs": f"seeds {BENCH_SEED0}+k mod {args.batch}, as the GPU arm"},
         "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": threads, "kind": kind,
-                         "sample": f"{args.steps} pairs, one per step"},
+                         "sample": sample, "cpu_model": cpu_model()},
         "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -342,7 +362,7 @@ def our_arm(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     P = args.batch
     log(f"[rank {rank}] generating {P} pairs ...")
-    seeds = multigpu.rank_seeds(rank, world, P, base=10_000)
+    seeds = multigpu.rank_seeds(rank, world, P, base=BENCH_SEED0)
     pairs = make_pairs_seeds(seeds)
     prm = oflow.TVL1Params(**PARAMS)
     ctx = oflow.Context(local_rank)
@@ -460,9 +480,22 @@ def our_arm(args, rank, world, local_rank):
     # --- the other two solvers on their configurations (device-resident)
     solvers = solver_measure(oflow, synth, np, torch, ctx, stream, dev, measured_peak()[0])
 
+    # --- the mixed batch workload (256 pairs, HS and TV-L1, five sizes)
+    mixed = None
+    if not args.no_mixed:
+        mixed = batch_measure(ctx, dev, stream, args.mixed_steps, 3, args.batch_pairs, rank,
+                              max_over_ranks, barrier, measured_peak()[0])
+        mixed["value"] *= world
+        mixed["e2e"]["value"] *= world
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args.cpu_pairs, args.cpu_seconds)
+        cpu = cpu_baseline(args.cpu_pairs, args.cpu_seconds, batch=P)
+        if cpu:
+            one = cpu_baseline(8, args.cpu_seconds / 2, threads=1, batch=P)
+            cpu["cpu_model"] = cpu_model()
+            cpu["single_thread"] = one and {"value": one["value"], "unit": one["unit"],
+                                            "cores": 1, "sample": one["sample"]}
 
     if world > 1:
         dist.destroy_process_group()
@@ -508,6 +541,8 @@ def our_arm(args, rank, world, local_rank):
         line["warm_start"] = warm
     line["flow_to_color"] = color
     line["solvers"] = solvers
+    if mixed:
+        line["mixed_batch"] = dict(mixed, metric=METRIC_BATCH)
     print(json.dumps(line), flush=True)
     return 0
 
@@ -536,56 +571,69 @@ def once(args):
 
 
 METRIC_BATCH = "mixed batch pairs/s: 256 pairs, half HS half TV-L1, 5 sizes up to 1920x1080"
+HS_SWEEP_BYTES = 28  # per px per Jacobi sweep: read du, dv, Ix, Iy, Iz; write du, dv
+HS_WARP_BYTES = 24   # per px per warp: warp + derivatives
+TV_WARP_BYTES = 32   # per px per warp stage: warp of I1, I1x, I1y + rho_c / grad
+TV_LEVEL_BYTES = 40  # per px per level: pyramid, gradients, zoom of the flow
 
 
-def batch_arm(args, rank, world, local_rank):
-    """The batched uneven workload: 256 pairs with sizes uniform over
+def batch_measure(ctx, dev, stream, steps, warmup, n_pairs, seed, max_over_ranks, barrier,
+                  peak):
+    """The batched uneven workload: n_pairs pairs with sizes uniform over
     {320x240, 640x480, 1024x436, 1280x720, 1920x1080}, half Horn-Schunck
     (alpha 15, 200 sweeps) and half TV-L1 (5 scales x 5 warps x <= 50),
-    solved as one oflow_batch schedule (one graph, a branch per group)."""
+    solved as one oflow_batch schedule (one graph, a branch per group).
+    Returns the measurement: pairs/s device-resident and end to end, and the
+    whole step's algorithmic bytes against the HBM peak."""
     import torch
     import oflow
-    from oflow import multigpu, synth, synth_gpu
+    from oflow import synth, synth_gpu
 
-    torch.cuda.set_device(local_rank)
-    dev = torch.device("cuda", local_rank)
-    specs = multigpu.shard(synth.batch_specs(args.batch_pairs, seed=rank), 0, 1)
+    specs = synth.batch_specs(n_pairs, seed=seed)
     tp = oflow.TVL1Params(nscales=5, max_iterations=50)
     hp = oflow.HSParams(15.0, 1, 1, 200)
     groups = {}
-    for i, (solver, w, h, seed) in enumerate(specs):
+    for i, (solver, w, h, _) in enumerate(specs):
         groups.setdefault((solver, w, h), []).append(i)
     frames = [None] * len(specs)
     for (solver, w, h), idx in groups.items():
-        if solver == "tvl1":
-            a, b, *_ = synth_gpu.tvl1_pairs(len(idx), w, h, seed=hash((w, h)) & 0xffff, device=dev)
-        else:
-            a, b, *_ = synth_gpu.hs_pairs(len(idx), w, h, seed=hash((w, h)) & 0xffff, device=dev)
+        gen = synth_gpu.tvl1_pairs if solver == "tvl1" else synth_gpu.hs_pairs
+        a, b, *_ = gen(len(idx), w, h, seed=(seed * 7919 + w * 31 + h) & 0xffff, device=dev)
         for k, i in enumerate(idx):
             frames[i] = (a[k].contiguous(), b[k].contiguous())
     jobs = [(solver, frames[i][0], frames[i][1], tp if solver == "tvl1" else hp)
-            for i, (solver, w, h, seed) in enumerate(specs)]
+            for i, (solver, w, h, _) in enumerate(specs)]
     outs = [(torch.empty((h, w), dtype=torch.float32, device=dev),
              torch.empty((h, w), dtype=torch.float32, device=dev)) for (_, w, h, _) in specs]
-    ctx = oflow.Context(local_rank)
-    stream = torch.cuda.current_stream(dev)
-    ctx.set_stream(stream.cuda_stream)
-    for (solver, w, h), idx in groups.items():  # tile shapes per group (untimed)
+    # tile shapes per group (untimed), and the TV-L1 iteration counts that
+    # set the algorithmic bytes (same kernels and inputs as the timed batch)
+    alg = 0
+    for (solver, w, h), idx in groups.items():
+        grp = [frames[i] for i in idx]
         if solver == "tvl1":
-            oflow.tvl1_autotune([frames[i] for i in idx], tp, ctx)
+            oflow.tvl1_autotune(grp, tp, ctx)
+            _, st = oflow.tvl1_batch(grp, tp, ctx, stats=True)
+            nx, ny = level_sizes(st[0]["nscales"], w, h)
+            for sti in st:
+                its = sti["iterations"]
+                for sc in range(its.shape[0]):
+                    px = nx[sc] * ny[sc]
+                    alg += px * (int(its[sc].sum()) * BYTES_PER_PX_ITER
+                                 + its.shape[1] * TV_WARP_BYTES + TV_LEVEL_BYTES)
         else:
-            oflow.hs_autotune([frames[i] for i in idx], hp, ctx)
-    for _ in range(args.warmup):
+            oflow.hs_autotune(grp, hp, ctx)
+            alg += len(idx) * w * h * (hp.nsolver * HS_SWEEP_BYTES + HS_WARP_BYTES)
+    for _ in range(warmup):
         oflow.batch(jobs, ctx, out=outs)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(local_rank) as clk:
-        e0.record(stream)
-        for _ in range(args.steps):
-            oflow.batch(jobs, ctx, out=outs)
-        e1.record(stream)
-        torch.cuda.synchronize()
-    t = e0.elapsed_time(e1) / 1e3
+    barrier()
+    e0.record(stream)
+    for _ in range(steps):
+        oflow.batch(jobs, ctx, out=outs)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = max_over_ranks(e0.elapsed_time(e1) / 1e3)
     # end to end: pinned host frames in, host flows out
     h_jobs = [(s_, f0.cpu().pin_memory().numpy(), f1.cpu().pin_memory().numpy(), p_)
               for (s_, f0, f1, p_) in jobs]
@@ -593,27 +641,64 @@ def batch_arm(args, rank, world, local_rank):
                torch.empty(o[0].shape).pin_memory().numpy()) for o in outs]
     oflow.batch(h_jobs, ctx, out=h_outs)
     torch.cuda.synchronize()
+    barrier()
     e0.record(stream)
-    e2e_steps = max(2, args.steps // 2)
+    e2e_steps = max(2, steps // 2)
     for _ in range(e2e_steps):
         oflow.batch(h_jobs, ctx, out=h_outs)
     e1.record(stream)
     torch.cuda.synchronize()
-    t_e2e = e0.elapsed_time(e1) / 1e3
+    t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3)
     n = len(specs)
     px = sum(w * h for (_, w, h, _) in specs)
-    line = {"metric": METRIC_BATCH, "value": n * args.steps / t, "unit": "pairs/s", "n_gpus": 1,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic",
-            "config": {"workload": "mixed batch (HS alpha 15, 200 sweeps; TV-L1 5x5x<=50)",
+    ach = alg * steps / t / 1e9
+    return {"value": n * steps / t, "unit": "pairs/s", "ms_per_step": 1e3 * t / steps,
+            "steps": steps,
+            "config": {"workload": "mixed batch (HS alpha 15, 1 level, 1 warp, 200 sweeps; "
+                                   "TV-L1 5 scales x 5 warps x <=50)",
                        "pairs": n, "groups": len(groups), "megapixels_per_step": px / 1e6,
+                       "tvl1_pairs": sum(1 for sp in specs if sp[0] == "tvl1"),
                        "l2": "inputs larger than L2"},
             "e2e": {"value": n * e2e_steps / t_e2e, "unit": "pairs/s",
-                    "h2d_bytes_per_step": sum(f[0].nbytes + f[1].nbytes for (_, f0, f1, _) in h_jobs
-                                              for f in [(f0, f1)]),
+                    "h2d_bytes_per_step": sum(f0.nbytes + f1.nbytes for (_, f0, f1, _) in h_jobs),
                     "d2h_bytes_per_step": 2 * 4 * px},
-            "clocks": clk.summary()}
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": ach / peak, "algorithmic_bytes_per_step": alg,
+                         "bytes_basis": "whole step: TV-L1 per px 60 B x inner iterations + "
+                                        "32 B per warp stage + 40 B per level; HS per px "
+                                        "28 B x sweeps + 24 B per warp"}}
+
+
+def batch_arm(args, rank, world, local_rank):
+    """--workload batch: the mixed workload alone, as its own JSON line."""
+    import torch
+    import torch.distributed as dist
+    import oflow
+    from oflow import multigpu
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180),
+                                device_id=torch.device("cuda", local_rank))
+    dev = torch.device("cuda", local_rank)
+    ctx = oflow.Context(local_rank)
+    stream = torch.cuda.current_stream(dev)
+    ctx.set_stream(stream.cuda_stream)
+    with Clocks(local_rank) as clk:
+        m = batch_measure(ctx, dev, stream, args.steps, args.warmup, args.batch_pairs, rank,
+                          lambda x: multigpu.max_over_ranks(x, dev),
+                          (lambda: dist.barrier()) if world > 1 else (lambda: None),
+                          measured_peak()[0])
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC_BATCH, "value": world * m["value"], "unit": "pairs/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": m["config"],
+            "e2e": dict(m["e2e"], value=world * m["e2e"]["value"]),
+            "roofline": m["roofline"], "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -634,6 +719,10 @@ def main():
                     help="tvl1: the 1024x436 TV-L1 workload (default); batch: the 256-pair "
                          "mixed HS/TV-L1 workload")
     ap.add_argument("--batch-pairs", type=int, default=256)
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="skip the mixed batch workload in the default run")
+    ap.add_argument("--mixed-steps", type=int, default=5,
+                    help="timed steps of the mixed batch workload in the default run")
     ap.add_argument("--cpu-pairs", type=int, default=30)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--cpu-worker", action="store_true", help=argparse.SUPPRESS)

@@ -69,6 +69,18 @@ def test_hs_autotune_keeps_results_and_roundtrips(of, tmp_path):
     ctx2.close()
 
 
+def test_hs_1920x1080_against_oracle(of, orc, ctx):
+    """The largest frame of the mixed batch workload with the HS parameters
+    it uses (alpha 15, one level, one warp, 200 sweeps), and a 3-level
+    pyramid at the same size: bit-identical to the oracle."""
+    from oflow import synth
+    q = synth.hs_pair(seed=33, w=1920, h=1080)
+    for prm in (of.HSParams(15.0, 1, 1, 200), of.HSParams(0.2, 3, 2, 20)):
+        u, v = of.hs(q.I0, q.I1, prm, ctx)
+        ou, ov = orc.hs(q.I0, q.I1, prm.alpha, prm.nlevels, prm.nwarp, prm.nsolver)
+        assert _same(u, ou) and _same(v, ov)
+
+
 def test_hs_golden(of, ctx):
     d = dict(np.load(os.path.join(GOLDEN, "hs_64x48.npz")))
     u, v = of.hs(d["I0"], d["I1"], of.HSParams(15.0, 1, 1, 50), ctx)

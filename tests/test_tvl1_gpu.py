@@ -304,3 +304,56 @@ def test_autotune_keeps_results_and_roundtrips(of, tmp_path):
         ctx2.load_tuning(str(bad))
     ctx.close()
     ctx2.close()
+
+
+@pytest.mark.parametrize("w,h,seed", [(1920, 1080, 31), (1280, 720, 32)])
+def test_largest_batch_sizes_against_oracle_and_reference(of, orc, ctx, w, h, seed):
+    """The two largest frame sizes of the mixed batch workload (1920x1080,
+    1280x720), 5 scales x 5 warps x 50 iterations: bit-identical to the
+    oracle (flow and iteration counts), within the stated tolerances of the
+    compiled reference."""
+    from oflow import synth
+    p, a, b = _pair(seed, w, h, radius=min(w, h) / 5.0)
+    prm = of.TVL1Params(nscales=5, max_iterations=50)
+    u, v, st = of.tvl1(a, b, prm, ctx, stats=True)
+    ou, ov, its, _ = _oracle(orc, a, b, prm, mode=1)
+    assert np.array_equal(st["iterations"], its)
+    assert np.array_equal(u, ou) and np.array_equal(v, ov)
+    if orc.ref_available():
+        ru, rv = orc.ref_tvl1(a, b, orc.TVL1Params(nscales=5, max_iterations=50))
+        assert max(np.abs(u - ru).max(), np.abs(v - rv).max()) <= TOL_FLOW
+        assert abs(synth.epe(u, v, p.u, p.v, p.valid, 8) -
+                   synth.epe(ru, rv, p.u, p.v, p.valid, 8)) <= TOL_EPE
+
+
+def test_benchmark_pairs_against_reference(of, orc, ctx):
+    """The first 8 pairs the benchmark solves (generator seeds 10000-10007 at
+    1024x436), solved as one batch: each bit-identical to the oracle with the
+    GPU's error-sum rounding; each within max |du|,|dv| <= 1e-3 px and
+    |dEPE| <= 1e-4 px of the compiled reference.  The iteration counts per
+    (scale, warp) are also compared with the oracle in the reference's own
+    summation order (left to right in float): a stage whose count differs is
+    a stopping-decision flip, printed, and the flow tolerances above still
+    hold."""
+    from oflow import synth
+    seeds = list(range(10_000, 10_008))
+    pairs = []
+    for s in seeds:
+        p = synth.tvl1_pair(seed=s, w=1024, h=436)
+        pairs.append((p, synth.quantize(p.I0), synth.quantize(p.I1)))
+    prm = of.TVL1Params(nscales=5, max_iterations=50)
+    res, stats = of.tvl1_batch([(a, b) for _, a, b in pairs], prm, ctx, stats=True)
+    flips = []
+    for s, (p, a, b), (u, v), st in zip(seeds, pairs, res, stats):
+        ou, ov, its, _ = _oracle(orc, a, b, prm, mode=1)
+        assert np.array_equal(st["iterations"], its), s
+        assert np.array_equal(u, ou) and np.array_equal(v, ov), s
+        _, _, its0, _ = _oracle(orc, a, b, prm, mode=0)
+        flips += [(s, int(k), int(w_), int(its[k, w_]), int(its0[k, w_]))
+                  for k, w_ in zip(*np.nonzero(its != its0))]
+        if orc.ref_available():
+            ru, rv = orc.ref_tvl1(a, b, orc.TVL1Params(nscales=5, max_iterations=50))
+            assert max(np.abs(u - ru).max(), np.abs(v - rv).max()) <= TOL_FLOW, s
+            assert abs(synth.epe(u, v, p.u, p.v, p.valid, 8) -
+                       synth.epe(ru, rv, p.u, p.v, p.valid, 8)) <= TOL_EPE, s
+    print(f"iteration-count flips (seed, scale, warp, gpu, reference order): {flips}")
