@@ -172,6 +172,22 @@ oflow_status oflow_ctx_save_tuning(oflow_ctx *ctx, const char *path);
 oflow_status oflow_ctx_last_launches(oflow_ctx *ctx, long long *launches);
 oflow_status oflow_ctx_load_tuning(oflow_ctx *ctx, const char *path);
 
+/* Device check of the arithmetic behind the exact fast forms (no counterpart
+ * in the reference; a diagnostic for tests and for new GPUs).  The TV-L1
+ * kernels round exactly as IEEE single precision by refining the hardware's
+ * square-root and reciprocal estimates; this runs those refinements on the
+ * device and counts operands that break their contracts:
+ *   which 0: sqrt_near within one ulp of sqrtf, float bit patterns [lo, hi)
+ *   which 1: the refined reciprocal equal to __frcp_rn, bit patterns [lo, hi)
+ *   which 2: the fast hypot equal to (float)sqrt(double a^2 + double b^2),
+ *            seeded pseudo-random operands, indices [lo, hi)
+ *   which 3: Markstein's quotient from the refined reciprocal equal to IEEE
+ *            division, seeded pseudo-random operands, indices [lo, hi)
+ * Synchronous on the default stream of the current device; *mismatches
+ * receives the count (0 means the contract held on every operand). */
+oflow_status oflow_selftest_math(int which, uint32_t lo, uint32_t hi, unsigned long long seed,
+                                 unsigned long long *mismatches);
+
 /* ------------------------------------------------------------ Horn-Schunck */
 /* Parameters of ComputeFlow (src/hs/cuda/flow.cuh:21-31).  nlevels pyramid
  * levels (2x2 box downscale), nwarp warps per level, nsolver Jacobi sweeps. */

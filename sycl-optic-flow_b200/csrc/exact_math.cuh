@@ -35,10 +35,60 @@ __host__ __device__ __forceinline__ float hypot_ref(float a, float b) {
 #define OF_RCP(x) (1.0f / (x))
 #endif
 
+// Hardware estimates (PTX rsqrt.approx / rcp.approx), refined below by one
+// Newton step each.  On the host the refined forms are the plain correctly
+// rounded operations, which satisfy the same contracts.
+#ifdef __CUDA_ARCH__
+__device__ __forceinline__ float rsqrt_est(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float rcp_est(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+#endif
+
+// sqrt(x) within one ulp (not necessarily correctly rounded) for positive
+// normal x: y = x*r from the reciprocal square-root estimate r, then one
+// Newton step y + (r/2)(x - y^2).  The device tests check every positive
+// normal float against the correctly rounded sqrtf.
+__host__ __device__ __forceinline__ float sqrt_near(float x) {
+#ifdef __CUDA_ARCH__
+    const float r = rsqrt_est(x);
+    const float y = x * r;
+    const float e = __fmaf_rn(-y, y, x);
+    return __fmaf_rn(0.5f * r, e, y);
+#else
+    return sqrtf(x);
+#endif
+}
+
+// RN(1/g) for g in [kRcpLo, kRcpHi): the reciprocal estimate r, then one
+// Newton step r + r(1 - g r) with the residual formed exactly by a fused
+// multiply-add.  The device tests check every float of the range against the
+// correctly rounded reciprocal; rcp_in_range says whether g lies in it.
+constexpr float kRcpLo = 0x1p-40f, kRcpHi = 0x1p24f;
+__host__ __device__ __forceinline__ bool rcp_in_range(float g) { return g >= kRcpLo && g < kRcpHi; }
+__host__ __device__ __forceinline__ float rcp_near_rn(float g) {
+#ifdef __CUDA_ARCH__
+    const float r = rcp_est(g);
+    const float e = __fmaf_rn(-g, r, 1.0f);
+    return __fmaf_rn(r, e, r);
+#else
+    return 1.0f / g;
+#endif
+}
+
 // hypot_ref without double arithmetic on the common path.  With S = a^2+b^2
-// held exactly as float pairs, y0 = sqrt(RN(ah+bh)) is within one ulp of the
-// result.  The residual e = S - y0^2 (error < 2^-46 S) places sqrt(S) relative
-// to the midpoints y0 +- ulp/2 (at |e| = y0*ulp to first order).  When it is
+// held exactly as float pairs, y0 = sqrt_near(RN(bh+sh)) is within 1.5 ulp of
+// sqrt(S) (one ulp from sqrt_near, half an ulp from rounding the sum), so the
+// correctly rounded result is y0 or one of its neighbours.  The residual
+// e = S - y0^2 (error < 2^-46 S) places sqrt(S) relative to the midpoints
+// y0 +- ulp/2 (at |e| = y0*ulp to first order, the second-order term far
+// below the margin even with y0 an ulp off).  When it is
 // more than 2^-20 of that distance away, single rounding of sqrt(S) and the
 // reference's double-then-single rounding agree, and the fast answer is
 // certain; otherwise (and for tiny, huge or non-finite input) the double
@@ -53,7 +103,7 @@ __host__ __device__ __forceinline__ float hypot_try(float a, float b, bool &ok) 
     const float big = fmaxf(a, b), small = fminf(a, b);
     const float bh = big * big, bl = OF_FMAF(big, big, -bh);
     const float sh = small * small, sl = OF_FMAF(small, small, -sh);
-    const float y0 = sqrtf(bh + sh);
+    const float y0 = sqrt_near(bh + sh);
     const float yh = y0 * y0, yl = OF_FMAF(y0, y0, -yh);
     // (bh - yh) and the following add are exact (Sterbenz); the low parts
     // carry errors far below the threshold
@@ -91,9 +141,9 @@ __host__ __device__ __forceinline__ void hypot2_fast(float a1, float b1, float a
 
 // p / g correctly rounded (IEEE division) from y = RN(1/g): q0 = RN(p*y),
 // r = p - q0*g (exact by FMA), q = RN(q0 + r*y) (Markstein).  Valid while
-// neither the quotient nor p underflows (|p| > 2^-100 for the g >= 1 of the
-// dual update) and for p = +0; markstein_safe says so.  Other p take the
-// plain division.
+// neither the quotient nor p underflows: |p| > 2^-100 with g < 2^24 keeps the
+// quotient above 2^-124; and for p = +0.  markstein_safe says so for p; other
+// p take the plain division.
 __host__ __device__ __forceinline__ float markstein(float p, float g, float y) {
     const float q0 = p * y;
     const float r = OF_FMAF(-q0, g, p);

@@ -54,6 +54,15 @@ constexpr int kLevelCfg = 4;
 // kClC blocks (k_tvl1_cluster), for levels whose band fits shared memory.
 constexpr int kClusterCfg = 5;
 constexpr int kNumIterCfgs = 6;
+// tile of a tiled configuration (false for the whole-level ones)
+inline bool cfg_tile(int c, int &tw, int &th) {
+    if (c >= 0 && c < kTbNumCfgs) {
+        tw = kTbCfgs[c].tw;
+        th = kTbCfgs[c].th;
+        return true;
+    }
+    return false;
+}
 constexpr int kClC = 8, kClNT = 512;
 constexpr size_t kClMaxSmem = 200 * 1024;
 __host__ __device__ inline int cl_band_rows(int ny) { return (ny + kClC - 1) / kClC; }
@@ -453,7 +462,9 @@ __device__ __forceinline__ float div_border(float a1c, float a1l, float a2c, flo
 // coefficient of (I1wx, I1wy): l_t where rho < -l_t*grad, -l_t where rho >
 // l_t*grad, 0 where the gradient vanishes, else -rho/grad; the products are
 // the reference's, so the result is identical.  The quotient is formed for
-// every pixel (most need it) rather than behind a branch.
+// every pixel (most need it) by Markstein's correction from RN(1/grad), which
+// equals IEEE division inside the ranges rcp_in_range and markstein_safe
+// cover; a pixel that needs the quotient outside them takes the division.
 __device__ __forceinline__ float2 th_u_update(float2 u, float4 wr, float4 pc, float4 pl, float4 pu,
                                               bool L, bool R, bool T, bool B, float l_t,
                                               float theta) {
@@ -461,10 +472,12 @@ __device__ __forceinline__ float2 th_u_update(float2 u, float4 wr, float4 pc, fl
     const float rho = wr.z + (wr.x * u.x + wr.y * u.y);
     const float lg = l_t * grad;
     const bool c1 = rho >= -lg, c2 = rho > lg, c3 = grad < 1E-10f;
-    const float fi = -rho / grad;
+    const float nrho = -rho;
+    float fi = markstein(nrho, grad, rcp_near_rn(grad));
+    if (c1 && !c2 && !c3 && !(rcp_in_range(grad) && markstein_safe(nrho))) fi = nrho / grad;
     const float k = !c1 ? l_t : (c2 ? -l_t : fi);
-    float d1 = k * wr.x, d2 = k * wr.y;
-    if (c1 && !c2 && c3) d1 = d2 = 0.0f;
+    const bool flat = c1 && !c2 && c3;  // the reference's d = 0, by selection
+    const float d1 = flat ? 0.0f : k * wr.x, d2 = flat ? 0.0f : k * wr.y;
     const float v1 = u.x + d1, v2 = u.y + d2;
     const float div1 = div_border(pc.x, pl.x, pc.y, pu.y, L, R, T, B);
     const float div2 = div_border(pc.z, pl.z, pc.w, pu.w, L, R, T, B);
@@ -473,15 +486,17 @@ __device__ __forceinline__ float2 th_u_update(float2 u, float4 wr, float4 pc, fl
 
 // Dual update (tvl1.cpp:268-291) from the forward differences of u(new):
 // g = 1 + tau/theta*hypot(grad u), p = (p + tau/theta*grad u) / g, with the
-// hypot and the divisions in their exact fast forms (exact_math.cuh); the
-// rare inputs those forms do not cover share one branch per kind.
+// hypot and the divisions in their exact fast forms (exact_math.cuh).  Every
+// condition those forms need is checked without branching; a pixel outside
+// any of them takes the reference formulas in one shared branch.
 __device__ __forceinline__ float4 dual_update(float4 po, float f1x, float f1y, float f2x,
                                               float f2y, float taut) {
-    float h1, h2;
-    hypot2_fast(f1x, f1y, f2x, f2y, h1, h2);
-    const float g1 = 1.0f + taut * h1;
-    const float g2 = 1.0f + taut * h2;
-    const float r1 = OF_RCP(g1), r2 = OF_RCP(g2);
+    bool ok1, ok2;
+    float h1 = hypot_try(f1x, f1y, ok1);
+    float h2 = hypot_try(f2x, f2y, ok2);
+    float g1 = 1.0f + taut * h1;
+    float g2 = 1.0f + taut * h2;
+    const float r1 = rcp_near_rn(g1), r2 = rcp_near_rn(g2);
     const float n1 = taut * f1x + po.x, n2 = taut * f1y + po.y;
     const float n3 = taut * f2x + po.z, n4 = taut * f2y + po.w;
     float4 pn;
@@ -489,7 +504,13 @@ __device__ __forceinline__ float4 dual_update(float4 po, float f1x, float f1y, f
     pn.y = markstein(n2, g1, r1);
     pn.z = markstein(n3, g2, r2);
     pn.w = markstein(n4, g2, r2);
-    if (!(markstein_safe(n1) && markstein_safe(n2) && markstein_safe(n3) && markstein_safe(n4))) {
+    const bool fast = ok1 && ok2 && rcp_in_range(g1) && rcp_in_range(g2) && markstein_safe(n1) &&
+                      markstein_safe(n2) && markstein_safe(n3) && markstein_safe(n4);
+    if (!fast) {
+        if (!ok1) h1 = hypot_ref(f1x, f1y);
+        if (!ok2) h2 = hypot_ref(f2x, f2y);
+        g1 = 1.0f + taut * h1;
+        g2 = 1.0f + taut * h2;
         pn.x = n1 / g1;
         pn.y = n2 / g1;
         pn.z = n3 / g2;
@@ -1326,8 +1347,15 @@ static void tb_set_smem_attrs() {
 }
 
 static int tb_tiles(int cfg, int nx, int ny) {
-    if (cfg == kLevelCfg || cfg == kClusterCfg) return 1;
-    return div_up(nx, kTbCfgs[cfg].tw) * div_up(ny, kTbCfgs[cfg].th);
+    int tw, th;
+    if (!cfg_tile(cfg, tw, th)) return 1;
+    return div_up(nx, tw) * div_up(ny, th);
+}
+
+static dim3 tb_grid(int cfg, int nx, int ny, int B) {
+    int tw, th;
+    if (!cfg_tile(cfg, tw, th)) return dim3(1, 1, B);
+    return dim3(div_up(nx, tw), div_up(ny, th), B);
 }
 
 // Largest tile whose grid still gives every SM two blocks; small scales get
@@ -1386,7 +1414,7 @@ TvPlan::TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, boo
         tb_cfg_[s] = (tuned && it != tuned->end() && cfg_valid(it->second, nx_[s], ny_[s]))
                          ? it->second
                          : tb_pick(nx_[s], ny_[s], B);
-        for (int c = 0; c < kTbNumCfgs; c++)  // any configuration may run while tuning
+        for (int c = 0; c < kNumIterCfgs; c++)  // any configuration may run while tuning
             iter_blocks_ = imax(iter_blocks_, tb_tiles(c, nx_[s], ny_[s]) * kTbK);
     }
     ingest_blocks_ = imin(div_up((int)N0, kIngestNT * kIngestPPT), 1024);
@@ -1553,8 +1581,7 @@ void TvPlan::record(cudaStream_t st) {
                           prm_.theta, taut, eps2, ctrl, part, max_blocks_ / kTbK, iters,
                           iter_stride_, ia.stage};
                 tb_maps(ta, cfg, nx, ny, B, N0, P0, U0, WR, err_.device());
-                const dim3 tg = cfg < kTbNumCfgs ? dim3(div_up(nx, kTbCfgs[cfg].tw), div_up(ny, kTbCfgs[cfg].th), B)
-                                                 : dim3(1, 1, B);
+                const dim3 tg = tb_grid(cfg, nx, ny, B);
                 const int nl = iter_launches_per_stage();
                 if (cfg == kLevelCfg || cfg == kClusterCfg) {
                     // the whole stage in one launch; the profile keeps one
@@ -1696,8 +1723,7 @@ void TvPlan::autotune(cudaStream_t st, TuneTable *table, int reps) {
                           ctrl, ar_.at<double>(o_part_), max_blocks_ / kTbK, ar_.at<int>(o_iters_),
                           iter_stride_, 0};
                 tb_maps(ta, c, nx, ny, B_, N0, pbuf(0), ubuf(0), ar_.at<float4>(o_WR_), err_.device());
-                const dim3 tg = c < kTbNumCfgs ? dim3(div_up(nx, kTbCfgs[c].tw), div_up(ny, kTbCfgs[c].th), B_)
-                                               : dim3(1, 1, B_);
+                const dim3 tg = tb_grid(c, nx, ny, B_);
                 float ms_min = 1e30f;
                 for (int r = 0; r <= reps; r++) {  // first launch warms up
                     k_ctrl_rearm<<<div_up(B_, 128), 128, 0, st>>>(ctrl, B_);

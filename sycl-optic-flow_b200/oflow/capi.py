@@ -125,6 +125,8 @@ SIGNATURES = {
     "oflow_stream_push": (_I, [_VP, C.POINTER(Image), C.POINTER(Flow), C.POINTER(Tvl1Stats)]),
     "oflow_stream_frames": (C.c_longlong, [_VP]),
     "oflow_ctx_last_launches": (_I, [_VP, C.POINTER(C.c_longlong)]),
+    "oflow_selftest_math": (_I, [_I, C.c_uint32, C.c_uint32, C.c_ulonglong,
+                                 C.POINTER(C.c_ulonglong)]),
     "oflow_flow_to_color": (_I, [_VP, _I, _I, _I, C.POINTER(Flow), C.POINTER(BgrImage)]),
     "oflow_conv3x3": (_I, [_I, _I, _I, _I, _I, _I, _I, _I, _I, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "oflow_lk_default_params": (None, [C.POINTER(LkParams)]),

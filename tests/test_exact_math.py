@@ -85,6 +85,13 @@ int main(int argc, char **argv) {
         if (!same(div_by_rcp(p, g, y), p / g)) bad_d++;
         if (markstein_safe(p) && !same(markstein(p, g, y), p / g)) bad_d++;
     }
+    // the TH step's quotient -rho/grad: g over the whole refined-reciprocal range
+    for (long i = 0; i < n; i++) {
+        const float g = ldexpf((float)unit(rng), (int)(rng() % 64) - 40);
+        const float p = rnd(-99, 30);
+        const float y = 1.0f / g;
+        if (rcp_in_range(g) && markstein_safe(p) && !same(markstein(p, g, y), p / g)) bad_d++;
+    }
     printf("%ld %ld %ld %ld %ld\n", bad_h, bad_h2, bad_d, mids, cases);
     return 0;
 }
