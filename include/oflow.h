@@ -283,19 +283,26 @@ oflow_status oflow_net_train_step(oflow_net *net, const void *frames, int dtype,
 oflow_status oflow_net_predict(oflow_net *net, const void *frames, int dtype, float *flow);
 
 /* TV-L1 warm-started by the network: the network's flow initialises scale 3
- * and the solve runs scales 3..0 with `warm` (e.g. 2 warps x 20 iterations).
+ * and the solve runs scales 3..0 with `warm` (e.g. 2 warps x 20 iterations),
+ * or per scale with warps_per_scale[s] (in [1, warm->warps]) and
+ * iters_per_scale[s] (index 0 = finest; either array may be NULL for the
+ * uniform value of `warm`).
  * With `plain` non-NULL the plain solve also runs and is the judge: a pair's
- * warm result is kept only if its TV-L1 energy (non-linearised: sum |grad u|
- * + lambda * sum |I1(x+u) - I0(x)|, bicubic warp with border zeroing) is at
- * most 1.01 times the plain solve's; otherwise the plain result is returned.
+ * warm result is kept only if (a) its TV-L1 energy (non-linearised: sum
+ * |grad u| + lambda * sum |I1(x+u) - I0(x)|, bicubic warp with border zeroing)
+ * is at most 1.01 times the plain solve's, and (b) its end-point difference
+ * from the plain flow, summed over the pixels, is at most 1 % of the plain
+ * flow's summed magnitude; otherwise the plain result is returned.
  * n must equal the network's batch and all frames its size.  energy_warm,
- * energy_plain, accepted and stats (arrays of n; stats = the warm solve's
- * iterations per (scale, warp), 0 for the scales above 3) may be NULL. */
+ * energy_plain, epe_vs_plain (the ratio of (b)), accepted and stats (arrays
+ * of n; stats = the warm solve's iterations per (scale, warp), 0 for the
+ * scales above 3) may be NULL. */
 oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_image *I0,
                              const oflow_image *I1, const oflow_tvl1_params *warm,
+                             const int *warps_per_scale, const int *iters_per_scale,
                              const oflow_tvl1_params *plain, const oflow_flow *out,
-                             double *energy_warm, double *energy_plain, int *accepted,
-                             oflow_tvl1_stats *stats);
+                             double *energy_warm, double *energy_plain, double *epe_vs_plain,
+                             int *accepted, oflow_tvl1_stats *stats);
 
 /* ---------------------------------------------------------------- streaming */
 /* Frame streams: the streaming form of the reference's CUDA TV-L1
@@ -383,6 +390,14 @@ oflow_status oflow_lk(oflow_ctx *ctx, const oflow_image *frames, int iframe,
  * warp-and-solve refinements per level, temporal taps (-1, 1)). */
 oflow_status oflow_pyrlk(oflow_ctx *ctx, const oflow_image *I0, const oflow_image *I1,
                          const oflow_lk_params *p, const oflow_flow *out);
+
+/* n pairs in one call (no reference entry point; the batched form of
+ * oflow_pyrlk for many small frames, which one pair cannot spread over the
+ * GPU).  Pairs of one size and dtype share one plan and one CUDA graph; each
+ * flow equals oflow_pyrlk's on the same pair. */
+oflow_status oflow_pyrlk_batch(oflow_ctx *ctx, int n, const oflow_image *I0,
+                               const oflow_image *I1, const oflow_lk_params *p,
+                               const oflow_flow *out);
 
 #ifdef __cplusplus
 }

@@ -183,6 +183,9 @@ TvPlan &side_plan(oflow_ctx *ctx, int c, int w, int h, int B, int dtype, const o
             same(pl->params(), p))
             return *pl;
     v.emplace_back(new TvPlan(w, h, B, dtype, p, false, &ctx->tune));
+    // chunks share the GPU: launches per block of iterations interleave with
+    // the other chunks' kernels, where persistent blocks would hold the SMs
+    v.back()->use_queue(false);
     if (v.size() > kMaxPlans) ctx->last_tv.clear();  // an evicted plan may be listed
     keep_recent(v);
     return *v.back();
@@ -532,6 +535,7 @@ oflow_status oflow_batch(oflow_ctx *ctx, int n, const oflow_job *jobs) {
                     m->slot.push_back((int)m->tv.size());
                     m->tv.emplace_back(new TvPlan(j.I0.width, j.I0.height, B, j.I0.dtype, *j.tvl1,
                                                   false, &ctx->tune));
+                    m->tv.back()->use_queue(false);  // groups run concurrently, as chunks do
                 } else {
                     m->slot.push_back((int)m->hs.size());
                     m->hs.emplace_back(new HsPlan(j.I0.width, j.I0.height, B, j.I0.dtype, *j.hs,
@@ -780,32 +784,47 @@ oflow_status oflow_lk(oflow_ctx *ctx, const oflow_image *frames, int iframe,
     });
 }
 
-oflow_status oflow_pyrlk(oflow_ctx *ctx, const oflow_image *I0, const oflow_image *I1,
-                         const oflow_lk_params *p, const oflow_flow *out) {
+oflow_status oflow_pyrlk_batch(oflow_ctx *ctx, int n, const oflow_image *I0,
+                               const oflow_image *I1, const oflow_lk_params *p,
+                               const oflow_flow *out) {
     return guard(ctx, [&] {
         OF_CHECK(ctx != nullptr && p != nullptr, "pyrlk: null argument");
+        OF_CHECK(n >= 1 && I0 && I1 && out, "pyrlk: empty batch or null arrays");
         OF_CHECK(p->temp == 2, "pyrlk: temporal filter must be the 2-tap difference");
-        check_flow(out, I0 ? I0->width : 0);
+        for (int i = 0; i < n; i++) check_flow(&out[i], I0[i].width);
         const cudaStream_t st = ctx->stream();
-        for (const Group &g : group_pairs(1, I0, I1)) {
+        bool device_only = true;
+        for (const Group &g : group_pairs(n, I0, I1)) {
+            const int B = (int)g.idx.size();
             PyrLkPlan *pl = nullptr;
             for (auto &q : ctx->pyrlk)
-                if (q->width() == g.w && q->height() == g.h && q->batch() == 1 &&
+                if (q->width() == g.w && q->height() == g.h && q->batch() == B &&
                     q->dtype() == g.dtype && same(q->params(), *p))
                     pl = q.get();
             if (!pl) {
-                ctx->pyrlk.emplace_back(new PyrLkPlan(g.w, g.h, 1, g.dtype, *p));
+                ctx->pyrlk.emplace_back(new PyrLkPlan(g.w, g.h, B, g.dtype, *p));
                 keep_recent(ctx->pyrlk);
                 pl = ctx->pyrlk.back().get();
             }
-            stage_image(*I0, pl->raw_input(0, 0), dtype_size(g.dtype), st);
-            stage_image(*I1, pl->raw_input(0, 1), dtype_size(g.dtype), st);
+            for (int b = 0; b < B; b++) {
+                stage_image(I0[g.idx[b]], pl->raw_input(b, 0), dtype_size(g.dtype), st);
+                stage_image(I1[g.idx[b]], pl->raw_input(b, 1), dtype_size(g.dtype), st);
+            }
             pl->run(st);
-            unstage_plane(pl->out_u(0), g.w, g.h, out->u, out->pitch, out->location, st);
-            unstage_plane(pl->out_v(0), g.w, g.h, out->v, out->pitch, out->location, st);
+            for (int b = 0; b < B; b++) {
+                const oflow_flow &o = out[g.idx[b]];
+                unstage_plane(pl->out_u(b), g.w, g.h, o.u, o.pitch, o.location, st);
+                unstage_plane(pl->out_v(b), g.w, g.h, o.v, o.pitch, o.location, st);
+                if (o.location == OFLOW_HOST) device_only = false;
+            }
         }
-        finish(ctx, out->location == OFLOW_DEVICE);
+        finish(ctx, device_only);
     });
+}
+
+oflow_status oflow_pyrlk(oflow_ctx *ctx, const oflow_image *I0, const oflow_image *I1,
+                         const oflow_lk_params *p, const oflow_flow *out) {
+    return oflow_pyrlk_batch(ctx, 1, I0, I1, p, out);
 }
 
 }  // extern "C"
@@ -885,9 +904,10 @@ oflow_status oflow_net_predict(oflow_net *net, const void *frames, int dtype, fl
 
 oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_image *I0,
                              const oflow_image *I1, const oflow_tvl1_params *warm,
+                             const int *warps_per_scale, const int *iters_per_scale,
                              const oflow_tvl1_params *plain, const oflow_flow *out,
-                             double *energy_warm, double *energy_plain, int *accepted,
-                             oflow_tvl1_stats *stats) {
+                             double *energy_warm, double *energy_plain, double *epe_vs_plain,
+                             int *accepted, oflow_tvl1_stats *stats) {
     return guard(ctx, [&] {
         OF_CHECK(ctx != nullptr && net != nullptr && I0 && I1 && out, "tvl1 warm: null argument");
         OF_CHECK(net->ctx != nullptr, "tvl1 warm: the network's context was destroyed");
@@ -904,10 +924,12 @@ oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_
         TvPlan *wp = nullptr;
         for (auto &q : ctx->tv_warm)
             if (q->width() == g.w && q->height() == g.h && q->batch() == n && q->dtype() == g.dtype &&
-                same(q->params(), *warm))
+                same(q->params(), *warm) && q->same_schedule(warps_per_scale, iters_per_scale))
                 wp = q.get();
         if (!wp) {
-            ctx->tv_warm.emplace_back(new TvPlan(g.w, g.h, n, g.dtype, *warm, false, &ctx->tune, 3));
+            std::unique_ptr<TvPlan> np(new TvPlan(g.w, g.h, n, g.dtype, *warm, false, &ctx->tune, 3));
+            np->set_schedule(warps_per_scale, iters_per_scale);
+            ctx->tv_warm.emplace_back(std::move(np));
             keep_recent(ctx->tv_warm);
             wp = ctx->tv_warm.back().get();
         }
@@ -917,7 +939,7 @@ oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_
         net->net->forward(wp->raw_input(0, 0), g.dtype, wp->plane_stride(), st);
         net->net->flow_to(wp->uz(), wp->plane_stride(), nullptr, st);
         wp->run(st);
-        std::vector<double> ew(n), ep(n, 0.0);
+        std::vector<double> ew(n), ep(n, 0.0), er(n, 0.0);
         std::vector<int> acc(n, 1);
         wp->true_energy(ew.data(), st);  // synchronises
         wp->check_device_error();
@@ -930,7 +952,10 @@ oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_
             pp->run(st);
             pp->true_energy(ep.data(), st);
             pp->check_device_error();
-            for (int b = 0; b < n; b++) acc[b] = ew[b] <= 1.01 * ep[b] ? 1 : 0;
+            wp->rel_epe_against(*pp, er.data(), st);
+            // both within 1 %: energy, and the end-point difference from the
+            // plain flow relative to the plain flow's magnitude
+            for (int b = 0; b < n; b++) acc[b] = (ew[b] <= 1.01 * ep[b] && er[b] <= 0.01) ? 1 : 0;
         }
         for (int b = 0; b < n; b++) {
             const TvPlan *src = acc[b] ? wp : pp;
@@ -938,6 +963,7 @@ oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_
             unstage_plane(src->out_v(b), g.w, g.h, out[b].v, out[b].pitch, out[b].location, st);
             if (energy_warm) energy_warm[b] = ew[b];
             if (energy_plain) energy_plain[b] = ep[b];
+            if (epe_vs_plain) epe_vs_plain[b] = er[b];
             if (accepted) accepted[b] = acc[b];
         }
     });

@@ -94,6 +94,8 @@ class HostFlag {
     HostFlag(const HostFlag &) = delete;
     HostFlag &operator=(const HostFlag &) = delete;
     int *device() const { return d_; }
+    // sets the flag from the host, as a kernel would (failure injection)
+    void raise() { *reinterpret_cast<volatile int *>(h_) = 1; }
     // the flag's value, cleared
     int take() {
         const int v = *reinterpret_cast<volatile int *>(h_);

@@ -279,9 +279,8 @@ void PyrLkPlan::record(cudaStream_t st) {
         k_to_float<float><<<nb, 256, 0, st>>>(ar_.at<float>(o_raw_), pyr, 2 * B * N_);
     for (int l = 1; l < L_; l++) {
         const size_t sp = (size_t)W_[l - 1] * H_[l - 1], dp = (size_t)W_[l] * H_[l];
-        launch_gauss(pyr + pyr_off_[l - 1], T, W_[l - 1], H_[l - 1], sp, taps_, 2 * B, st);
-        launch_resample(T, sp, W_[l - 1], H_[l - 1], pyr + pyr_off_[l], dp, W_[l], H_[l], 0.5f,
-                        0.5f, 2 * B, st);
+        launch_zoom_out(pyr + pyr_off_[l - 1], sp, W_[l - 1], H_[l - 1], T, pyr + pyr_off_[l], dp,
+                        W_[l], H_[l], 0.5f, taps_, 2 * B, st);
     }
     int cur = 0;
     OF_CUDA(cudaMemsetAsync(U[cur], 0, B * N_ * 8, st));

@@ -37,6 +37,12 @@ void launch_gauss(const float *src, float *dst, int nx, int ny, size_t stride,
 void launch_resample(const float *src, size_t sstride, int nx, int ny, float *dst,
                      size_t dstride, int nxx, int nyy, float dx, float dy, int planes,
                      cudaStream_t st);
+// zoom_out of `planes` planes (zoom.cpp:20-53): blur with `t` then resample by
+// zfactor.  At zfactor 1/2 one fused pass (T unused), otherwise blur into the
+// scratch planes T (stride sstride) and resample.  Returns the launch count.
+int launch_zoom_out(const float *src, size_t sstride, int nx, int ny, float *T, float *dst,
+                    size_t dstride, int nxx, int nyy, float zfactor, const GaussTaps &t,
+                    int planes, cudaStream_t st);
 
 // Where a plan reads one input frame: a device pointer of the plan's dtype and
 // its row pitch in elements.
@@ -58,10 +64,26 @@ class TvPlan {
     // Non-linearised TV-L1 energy of the last result, per pair (see
     // k_energy_true): sum |grad u1| + |grad u2| + lambda * sum |I1(x+u) - I0(x)|.
     void true_energy(double *host_out, cudaStream_t st);
+    // Per pair: sum of end-point differences of this plan's last flows against
+    // `other`'s (same shape), over the sum of `other`'s flow magnitudes.
+    // Synchronises.
+    void rel_epe_against(const TvPlan &other, double *host_out, cudaStream_t st);
     // Times each blocked-iteration configuration per scale on the current
     // buffers, keeps the fastest and records it in `table`.
     void autotune(cudaStream_t st, TuneTable *table, int reps = 3);
     int tb_config(int s) const { return tb_cfg_[s]; }
+    // Per-scale schedule (index 0 = finest): warps in [1, params.warps] and
+    // iteration caps; nullptr keeps the parameters' uniform value.  Rebuilds
+    // the graph on change.  Not for traced plans.
+    void set_schedule(const int *warps, const int *iters);
+    bool same_schedule(const int *warps, const int *iters) const;
+    // Tiled warp stages as one persistent work-queue launch each (default) or
+    // as one launch per block of K iterations (for plans that share the GPU
+    // with concurrent kernels).  Same results either way.
+    void use_queue(bool on) {
+        if (on != queue_) graph_.reset();
+        queue_ = on && !queue_off_env_;
+    }
     // Device destination of input frame k (0: I0, 1: I1) of pair b: a dense
     // w*h plane of the plan's dtype.
     void *raw_input(int b, int k) const;
@@ -117,7 +139,8 @@ class TvPlan {
     int iter_stride_ = 0, energy_slots_ = 0;
     GaussTaps taps0_{}, tapsz_{};
     struct Prof {
-        std::vector<cudaEvent_t> ev;
+        std::vector<cudaEvent_t> ev;  // begin/end pairs
+        std::vector<int> tag;         // per pair: -1 warp launch, else the scale
         int n_ev = 0;
     };
     Prof *prof_ = nullptr;
@@ -127,7 +150,7 @@ class TvPlan {
     int s0_ = 0;
     bool warm_ = false;
     size_t o_tarr_ = 0, o_tout_ = 0;
-    int iter_launches_per_stage() const;
+    int sw_[OFLOW_MAX_SCALES] = {}, si_[OFLOW_MAX_SCALES] = {};  // warps, iterations per scale
     size_t o_WR_ = 0;
     size_t o_raw_ = 0, o_T_ = 0, o_pyr_ = 0, o_I1g_ = 0, o_U0_ = 0, o_Uz_ = 0, o_P0_ = 0,
            o_out_ = 0, o_ctrl_ = 0, o_part_ = 0, o_recs_ = 0, o_iters_ = 0, o_energy_ = 0;
@@ -138,6 +161,10 @@ class TvPlan {
     std::vector<FrameRef> frames_;  // [B][2], host copy of the device table
     HostFlag err_;
     size_t o_frames_ = 0;
+    size_t o_queue_ = 0, o_left_ = 0;
+    bool queue_ = true;  // tiled stages as one persistent launch each
+    bool queue_off_env_ = false;
+    int warp_cap_ = 0;   // samples k_warp may stage in shared memory
     void upload_frames(cudaStream_t st);
 };
 

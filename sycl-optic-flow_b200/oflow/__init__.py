@@ -23,11 +23,11 @@ from dataclasses import dataclass
 import numpy as np
 
 from .capi import (LIB_PATH, SOLVER_HS, SOLVER_TVL1, BgrImage, Flow, StreamDesc, HsParams, Image, Job, LkParams,
-                   OflowError, Tvl1Params, Tvl1Profile, Tvl1Stats, lib, status_string)
+                   MAX_SCALES, OflowError, Tvl1Params, Tvl1Profile, Tvl1Stats, lib, status_string)
 
 __all__ = [
     "Context", "OflowError", "TVL1Params", "HSParams", "LKParams", "tvl1", "tvl1_batch",
-    "tvl1_energy_trace", "hs", "hs_batch", "lk", "pyrlk", "TV_L1", "initFlow", "ComputeFlow",
+    "tvl1_energy_trace", "hs", "hs_batch", "lk", "pyrlk", "pyrlk_batch", "TV_L1", "initFlow", "ComputeFlow",
     "deleteFlow_mem", "LucasKanade", "nscales", "LIB_PATH", "flow_to_color", "flow_to_color_batch",
     "save_ppm", "FrameStream",
 ]
@@ -435,10 +435,11 @@ class WarmNet:
 
 
 def tvl1_warm(pairs, net: WarmNet, warm: TVL1Params, plain: TVL1Params | None = None,
-              ctx: Context | None = None, out=None):
-    """Warm-started TV-L1 (oflow_tvl1_warm).  Returns (results, info) with
-    info = {energy_warm, energy_plain, accepted} arrays and "stats", the warm
-    solve's per-pair iteration dicts."""
+              ctx: Context | None = None, out=None, warps_per_scale=None, iters_per_scale=None):
+    """Warm-started TV-L1 (oflow_tvl1_warm).  warps_per_scale /
+    iters_per_scale: optional per-scale schedule (index 0 = finest).  Returns
+    (results, info) with info = {energy_warm, energy_plain, epe_vs_plain,
+    accepted} arrays and "stats", the warm solve's per-pair iteration dicts."""
     n = len(pairs)
     I0 = (Image * n)()
     I1 = (Image * n)()
@@ -452,17 +453,29 @@ def tvl1_warm(pairs, net: WarmNet, warm: TVL1Params, plain: TVL1Params | None = 
         res.append(uv)
     ew = np.zeros(n, np.float64)
     ep = np.zeros(n, np.float64)
+    er = np.zeros(n, np.float64)
     acc = np.zeros(n, np.int32)
     st = (Tvl1Stats * n)()
     wp = warm.c()
     pp = plain.c() if plain is not None else None
+
+    def sched(a):
+        if a is None:
+            return None, None
+        arr = np.zeros(MAX_SCALES, np.int32)
+        arr[:len(a)] = a
+        return arr, arr.ctypes.data_as(C.c_void_p)
+
+    ws, wsp = sched(warps_per_scale)
+    its, itp = sched(iters_per_scale)
     h = (ctx or net.ctx).handle
-    _check(lib().oflow_tvl1_warm(h, net.handle, n, I0, I1, C.byref(wp),
+    _check(lib().oflow_tvl1_warm(h, net.handle, n, I0, I1, C.byref(wp), wsp, itp,
                                  C.byref(pp) if pp is not None else None, O,
                                  ew.ctypes.data_as(C.c_void_p), ep.ctypes.data_as(C.c_void_p),
+                                 er.ctypes.data_as(C.c_void_p),
                                  acc.ctypes.data_as(C.c_void_p), st), h)
-    return res, {"energy_warm": ew, "energy_plain": ep, "accepted": acc.astype(bool),
-                 "stats": [_stats_dict(s) for s in st]}
+    return res, {"energy_warm": ew, "energy_plain": ep, "epe_vs_plain": er,
+                 "accepted": acc.astype(bool), "stats": [_stats_dict(s) for s in st]}
 
 
 def conv3x3(mode, N, H, W, C_, K, stride, relu, out_f32, a, y_act, b, out, bias=None, gbias=None):
@@ -501,6 +514,25 @@ def pyrlk(I0, I1, params: LKParams | None = None, ctx: Context | None = None, ou
     h = _ctx(ctx)
     _check(lib().oflow_pyrlk(h, C.byref(a), C.byref(b), C.byref(p), C.byref(f)), h)
     return uv
+
+
+def pyrlk_batch(pairs, params: LKParams | None = None, ctx: Context | None = None, out=None):
+    """oflow_pyrlk_batch: pyramidal LK of many pairs in one call."""
+    p = (params or LKParams()).c()
+    n = len(pairs)
+    I0 = (Image * n)()
+    I1 = (Image * n)()
+    O = (Flow * n)()
+    keep, res = [], []
+    for i, (a, b) in enumerate(pairs):
+        I0[i], ka = _image(a)
+        I1[i], kb = _image(b)
+        keep += [ka, kb]
+        O[i], uv = _outputs(a, I0[i].height, I0[i].width, None if out is None else out[i])
+        res.append(uv)
+    h = _ctx(ctx)
+    _check(lib().oflow_pyrlk_batch(h, n, I0, I1, C.byref(p), O), h)
+    return res
 
 
 # ------------------------------------------------------------------ streams

@@ -118,8 +118,8 @@ SIGNATURES = {
     "oflow_net_train_step": (_I, [_VP, _VP, _I, _VP, C.c_float, C.POINTER(C.c_double)]),
     "oflow_net_predict": (_I, [_VP, _VP, _I, _VP]),
     "oflow_tvl1_warm": (_I, [_VP, _VP, _I, C.POINTER(Image), C.POINTER(Image),
-                             C.POINTER(Tvl1Params), C.POINTER(Tvl1Params), C.POINTER(Flow),
-                             _VP, _VP, _VP, C.POINTER(Tvl1Stats)]),
+                             C.POINTER(Tvl1Params), _VP, _VP, C.POINTER(Tvl1Params),
+                             C.POINTER(Flow), _VP, _VP, _VP, _VP, C.POINTER(Tvl1Stats)]),
     "oflow_stream_create": (_I, [_VP, C.POINTER(StreamDesc), C.POINTER(_VP)]),
     "oflow_stream_destroy": (_I, [_VP]),
     "oflow_stream_push": (_I, [_VP, C.POINTER(Image), C.POINTER(Flow), C.POINTER(Tvl1Stats)]),
@@ -133,6 +133,8 @@ SIGNATURES = {
     "oflow_lk": (_I, [_VP, C.POINTER(Image), _I, C.POINTER(LkParams), C.POINTER(Flow)]),
     "oflow_pyrlk": (_I, [_VP, C.POINTER(Image), C.POINTER(Image), C.POINTER(LkParams),
                          C.POINTER(Flow)]),
+    "oflow_pyrlk_batch": (_I, [_VP, _I, C.POINTER(Image), C.POINTER(Image),
+                               C.POINTER(LkParams), C.POINTER(Flow)]),
 }
 
 _lib = None

@@ -108,13 +108,47 @@ def test_warm_start_judge(of):
     warm = of.TVL1Params(nscales=5, warps=2, max_iterations=20)
     plain = of.TVL1Params(nscales=5, max_iterations=50)
     res, info = of.tvl1_warm(pairs, net, warm, plain)
-    for (a, b), (u, v), acc, ew, ep in zip(pairs, res, info["accepted"], info["energy_warm"],
-                                          info["energy_plain"]):
+    warm_only, _ = of.tvl1_warm(pairs, net, warm, None)
+    for (a, b), (u, v), (wu, wv), acc, ew, ep, er in zip(
+            pairs, res, warm_only, info["accepted"], info["energy_warm"], info["energy_plain"],
+            info["epe_vs_plain"]):
         assert np.isfinite(ew) and np.isfinite(ep) and ep > 0
-        assert acc == (ew <= 1.01 * ep)
-        if not acc:
-            pu, pv = of.tvl1(a, b, plain)
+        pu, pv = of.tvl1(a, b, plain)
+        # the end-point criterion: sum |warm - plain| / sum |plain| (double)
+        d = np.hypot(wu.astype(np.float64) - pu, wv.astype(np.float64) - pv).sum()
+        m = np.hypot(pu.astype(np.float64), pv.astype(np.float64)).sum()
+        assert abs(er - d / m) <= 1e-9 * max(1.0, d / m)
+        assert acc == (ew <= 1.01 * ep and er <= 0.01)
+        if acc:
+            assert np.array_equal(u, wu) and np.array_equal(v, wv)
+        else:
             assert np.array_equal(u, pu) and np.array_equal(v, pv)
+
+
+def test_warm_start_per_scale_schedule(of):
+    """A per-scale schedule: the uniform values given per scale reproduce the
+    uniform solve bit for bit, and a mixed schedule respects every scale's
+    warp count and iteration cap."""
+    from oflow import synth
+    pairs = []
+    for s in range(2):
+        p = synth.tvl1_pair(seed=310 + s, w=256, h=128, radius=25.0)
+        pairs.append((synth.quantize(p.I0), synth.quantize(p.I1)))
+    net = of.WarmNet(256, 128, 2)
+    net.set_params(_init_params(of, 2))
+    warm = of.TVL1Params(nscales=5, warps=3, max_iterations=20)
+    r0, i0 = of.tvl1_warm(pairs, net, warm)
+    r1, i1 = of.tvl1_warm(pairs, net, warm, warps_per_scale=[3, 3, 3, 3],
+                          iters_per_scale=[20, 20, 20, 20])
+    for (u0, v0), (u1, v1) in zip(r0, r1):
+        assert np.array_equal(u0, u1) and np.array_equal(v0, v1)
+    ws, its = [3, 1, 2, 1], [12, 5, 7, 3]
+    _, i2 = of.tvl1_warm(pairs, net, warm, warps_per_scale=ws, iters_per_scale=its)
+    for st in i2["stats"]:
+        it = st["iterations"]  # [scale][warp]
+        for s in range(4):
+            assert np.all(it[s, :ws[s]] >= 1) and np.all(it[s, :ws[s]] <= its[s])
+            assert np.all(it[s, ws[s]:] == 0)
 
 
 def test_trained_network_gains_over_no_network(of):

@@ -145,6 +145,21 @@ def test_pyrlk_bit_identical(of, orc, ctx, levels, iters, window, w, h):
     assert _same(u, ou) and _same(v, ov)
 
 
+def test_pyrlk_batch_matches_single_pairs(of, orc, ctx):
+    """oflow_pyrlk_batch: pairs of two sizes (one plan per size) give each
+    pair's oflow_pyrlk flow, which is the oracle's."""
+    from oflow import synth
+    pairs = [synth.lk_pair(seed=s, w=w, h=h) for s, (w, h) in
+             enumerate([(160, 120), (97, 61), (160, 120), (160, 120), (97, 61)])]
+    prm = of.LKParams(3, 2, 5, 3, 2)
+    res = of.pyrlk_batch([(l.I0, l.I1) for l in pairs], prm, ctx)
+    for l, (u, v) in zip(pairs, res):
+        su, sv = of.pyrlk(l.I0, l.I1, prm, ctx)
+        assert np.array_equal(u, su) and np.array_equal(v, sv)
+        ou, ov = orc.pyrlk(l.I0, l.I1, 3, 2, 3, 5)
+        assert _same(u, ou) and _same(v, ov)
+
+
 def test_pyrlk_golden_and_accuracy(of, ctx):
     from oflow import synth
     d = dict(np.load(os.path.join(GOLDEN, "lk_80x60.npz")))

@@ -174,12 +174,18 @@ def test_host_batch_in_chunks_matches_device_batch(of, ctx):
         assert all(s["energy"] > 0 for s in st_h)
 
 
-def test_launch_count_of_the_schedule(of):
+@pytest.mark.parametrize("queue", [True, False])
+def test_launch_count_of_the_schedule(of, monkeypatch, queue):
     """oflow_ctx_last_launches reports the captured schedule: per warp stage
-    one warp launch and, for levels larger than 9216 pixels, ceil(50/4)+1
-    tiled inner-iteration launches (one for a re-run after a stop inside a
-    launch that wrote no snapshots); a smaller level runs its whole stage in
-    one launch.  Plus the ingest, pyramid, gradient, zoom and output launches."""
+    one warp launch and one persistent work-queue launch (k_tvl1_q) for the
+    tiled levels; with the queue off (OFLOW_TB_QUEUE=0), for levels larger
+    than 9216 pixels, ceil(50/4)+1 tiled inner-iteration launches (one for a
+    re-run after a stop inside a launch that wrote no snapshots).  A smaller
+    level runs its whole stage in one launch either way.  Plus the ingest,
+    pyramid (one fused blur-and-decimate launch per level), gradient, zoom
+    and output launches."""
+    if not queue:
+        monkeypatch.setenv("OFLOW_TB_QUEUE", "0")
     ctx = of.Context(0)
     pairs = [_pair(700 + i, 128, 96)[1:] for i in range(3)]
     prm = of.TVL1Params(nscales=5, max_iterations=50)
@@ -189,10 +195,11 @@ def test_launch_count_of_the_schedule(of):
     for _ in range(ns - 1):
         w, h = sizes[-1]
         sizes.append((int(w * 0.5 + 0.5), int(h * 0.5 + 0.5)))
-    per_stage = [1 + (1 if w * h <= 9216 else 14) for w, h in sizes]
+    per_stage = [1 + (1 if (w * h <= 9216 or queue) else 14) for w, h in sizes]
     expect = 5 * sum(per_stage)
     n = ctx.last_launches()
-    assert expect < n < expect + 4 * ns + 8
+    # ingest 2, level-0 blur 1, pyramid ns-1, gradients ns, zooms ns-1, energy and output 2
+    assert n == expect + 3 * ns + 3
     ctx.close()
 
 
@@ -232,6 +239,48 @@ def test_repeated_full_size_solves_match_the_oracle(of, orc, monkeypatch, cfg):
         c.close()
         assert np.array_equal(st["iterations"], its)
         assert np.array_equal(u, ou) and np.array_equal(v, ov)
+
+
+@pytest.mark.parametrize("env", [{"OFLOW_TB_QUEUE": "0"}, {"OFLOW_WARP_STAGED": "0"},
+                                 {"OFLOW_TB_QUEUE": "0", "OFLOW_WARP_STAGED": "0"}])
+@pytest.mark.parametrize("w,h,ns", [(1024, 436, 5), (131, 77, 4), (333, 201, 5)])
+def test_alternative_kernel_forms_match_the_oracle(of, orc, monkeypatch, env, w, h, ns):
+    """The tiled stages as one launch per block of iterations (k_tvl1_tb)
+    instead of the persistent work queue, and the warp reading its samples
+    per pixel instead of through shared memory: the same bits as the oracle
+    (and so as the default forms).  Odd widths take the plain region loads."""
+    for k, v in env.items():
+        monkeypatch.setenv(k, v)
+    _, a, b = _pair(w + h, w, h, radius=min(w, h) / 5.0)
+    prm = of.TVL1Params(nscales=ns, warps=2, max_iterations=30)
+    ou, ov, its, _ = _oracle(orc, a, b, prm, mode=1)
+    c = of.Context(0)
+    u, v, st = of.tvl1(a, b, prm, c, stats=True)
+    c.close()
+    assert np.array_equal(st["iterations"], its)
+    assert np.array_equal(u, ou) and np.array_equal(v, ov)
+
+
+def test_timeout_is_reported_and_the_context_recovers(of, orc, monkeypatch):
+    """A kernel that gives up a bounded wait sets the plan's error flag; the
+    call then returns OFLOW_ERR_TIMEOUT (3).  The flag is raised from the
+    host here (OFLOW_INJECT_TIMEOUT), so no GPU wait runs out.  The next call
+    on the same context, reusing the same plan and graph, equals the oracle."""
+    _, a, b = _pair(41, 200, 150)
+    prm = of.TVL1Params(nscales=4, max_iterations=30)
+    ou, ov, its, _ = _oracle(orc, a, b, prm)
+    c = of.Context(0)
+    of.tvl1(a, b, prm, c)
+    monkeypatch.setenv("OFLOW_INJECT_TIMEOUT", "1")
+    with pytest.raises(of.OflowError) as e:
+        of.tvl1(a, b, prm, c)
+    assert e.value.status == 3
+    monkeypatch.delenv("OFLOW_INJECT_TIMEOUT")
+    for _ in range(2):
+        u, v, st = of.tvl1(a, b, prm, c, stats=True)
+        assert np.array_equal(st["iterations"], its)
+        assert np.array_equal(u, ou) and np.array_equal(v, ov)
+    c.close()
 
 
 def test_known_answers_on_gpu(of, ctx):
