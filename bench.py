@@ -605,8 +605,50 @@ def our_arm(args, rank, world, local_rank):
     return 0
 
 
+def once_other(args):
+    """Profiling cases of the other kernels (--once-solver): hs: --batch pairs
+    of the 320x240 HS configuration (alpha 15, 200 sweeps); pyrlk: --batch
+    pairs of the 640x480 pyramidal LK configuration; color: flowToColor of
+    --batch 1024x436 flows; conv: the warm-start network's forward pass on
+    --batch 1024x436 pairs."""
+    import numpy as np
+    import torch
+    import oflow
+    from oflow import synth
+    dev = torch.device("cuda", 0)
+    ctx = oflow.Context(0)
+    n = args.batch
+    if args.once_solver == "hs":
+        gen = [synth.hs_pair(seed=40_000 + i) for i in range(n)]
+        d = [(torch.from_numpy(g.I0).to(dev), torch.from_numpy(g.I1).to(dev)) for g in gen]
+        oflow.hs_batch(d, oflow.HSParams(15.0, 1, 1, 200), ctx)
+    elif args.once_solver == "pyrlk":
+        gen = [synth.lk_pair(seed=41_000 + i) for i in range(n)]
+        d = [(torch.from_numpy(g.I0).to(dev), torch.from_numpy(g.I1).to(dev)) for g in gen]
+        oflow.pyrlk_batch(d, oflow.LKParams(3, 2, 5, 3, 3), ctx)
+    elif args.once_solver == "color":
+        rng = np.random.default_rng(5)
+        flows = [(torch.from_numpy(rng.normal(0, 4, (H, W)).astype(np.float32)).to(dev),
+                  torch.from_numpy(rng.normal(0, 4, (H, W)).astype(np.float32)).to(dev))
+                 for _ in range(n)]
+        oflow.flow_to_color_batch(flows, ctx)
+    else:
+        from oflow import warmstart
+        params, _ = warmstart.load()
+        net = oflow.WarmNet(W, H, n, ctx)
+        net.set_params(params)
+        pairs = make_pairs(n, 0)
+        fr = torch.from_numpy(np.stack([np.stack([a, b]) for a, b, _ in pairs])).to(dev)
+        net.predict(fr)
+    torch.cuda.synchronize()
+    log("done:", args.once_solver, n)
+    return 0
+
+
 def once(args):
     """Profiling case: one solve of --batch pairs with --nscales / --iters."""
+    if args.once_solver != "tvl1":
+        return once_other(args)
     import torch
     import oflow
     pairs = make_pairs(args.batch, 0)
@@ -788,6 +830,8 @@ def main():
     ap.add_argument("--cpu-worker", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--once", action="store_true",
                     help="one solve of --batch device-resident pairs and exit (profiling case)")
+    ap.add_argument("--once-solver", choices=["tvl1", "hs", "pyrlk", "color", "conv"],
+                    default="tvl1", help="kernel family of the --once profiling case")
     ap.add_argument("--nscales", type=int, default=PARAMS["nscales"])
     ap.add_argument("--iters", type=int, default=PARAMS["max_iterations"])
     ap.add_argument("--tuning", default=None,

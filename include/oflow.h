@@ -175,14 +175,12 @@ oflow_status oflow_ctx_load_tuning(oflow_ctx *ctx, const char *path);
 /* Device check of the arithmetic behind the exact fast forms (no counterpart
  * in the reference; a diagnostic for tests and for new GPUs).  The TV-L1
  * kernels round exactly as IEEE single precision by refining the hardware's
- * square-root and reciprocal estimates; this runs those refinements on the
- * device and counts operands that break their contracts:
- *   which 0: sqrt_near within one ulp of sqrtf, float bit patterns [lo, hi)
+ * reciprocal estimate; this runs that refinement on the device and counts
+ * operands that break its contract:
  *   which 1: the refined reciprocal equal to __frcp_rn, bit patterns [lo, hi)
- *   which 2: the fast hypot equal to (float)sqrt(double a^2 + double b^2),
- *            seeded pseudo-random operands, indices [lo, hi)
  *   which 3: Markstein's quotient from the refined reciprocal equal to IEEE
  *            division, seeded pseudo-random operands, indices [lo, hi)
+ * (other values of which: OFLOW_ERR_BAD_ARG)
  * Synchronous on the default stream of the current device; *mismatches
  * receives the count (0 means the contract held on every operand). */
 oflow_status oflow_selftest_math(int which, uint32_t lo, uint32_t hi, unsigned long long seed,
@@ -217,25 +215,30 @@ oflow_status oflow_hs_autotune(oflow_ctx *ctx, int n, const oflow_image *I0,
                                const oflow_image *I1, const oflow_hs_params *p,
                                int *cfg_per_level);
 
-/* Horn-Schunck for callers that cannot allocate device memory: code running
- * while a CUDA graph is captured, real-time frame loops that cannot afford the
- * synchronisation of cudaMalloc/cudaFree, hosts with a fixed memory budget.
- * This entry point has no counterpart in the reference.
+/* Horn-Schunck for callers that cannot allocate device memory: real-time
+ * frame loops that cannot afford the device-wide synchronisation that
+ * cudaMalloc/cudaFree may imply, and hosts that hand the library a fixed
+ * memory budget up front.  This entry point has no counterpart in the
+ * reference.
  *
  * It allocates nothing and needs no context.  Its scratch is one static
  * device array of 8 MiB, held by every GPU that loads the library until the
- * process exits.  With nlevels = 1 that covers frames up to about 125,000
- * pixels (320x240 uses 5.2 MB); larger requests return OFLOW_ERR_BAD_ARG.
+ * process exits.  With nlevels = 1 a frame needs 64 B per pixel (320x240:
+ * 4.9 MB), so frames up to about 131,000 pixels fit; more levels add up to
+ * 8/3 B per pixel for the pyramid.  Larger requests return OFLOW_ERR_BAD_ARG.
  * I0, I1 are device float frames, u and v device float planes; pitches are in
  * elements (0 means width).  The work is enqueued on `stream` (a
  * cudaStream_t; NULL is the default stream) and the call returns without
  * waiting.  The result equals oflow_hs with the same parameters.
  *
  * The first call on a device looks up the array's device address (with that
- * device current) and caches it; make that first call before any stream
- * capture.  All calls share the one array: calls that overlap on the GPU (on
- * different streams, or from several threads without ordering) race and give
- * wrong results.  Order them on one stream. */
+ * device current) and caches it for the process; make that first call before
+ * any stream capture.  The cached address does not survive a device reset
+ * (cudaDeviceReset, or the primary context being destroyed and recreated):
+ * do not call this entry point on a device after such a reset.  All calls
+ * share the one array, which keeps the last call's contents: calls that
+ * overlap on the GPU (on different streams, or from several threads without
+ * ordering) race and give wrong results.  Order them on one stream. */
 oflow_status oflow_hs_noalloc(const float *I0, const float *I1, int width, int height,
                               int pitch, const oflow_hs_params *p, float *u, float *v,
                               int out_pitch, void *stream);
@@ -285,8 +288,8 @@ oflow_status oflow_net_predict(oflow_net *net, const void *frames, int dtype, fl
 /* TV-L1 warm-started by the network: the network's flow initialises scale 3
  * and the solve runs scales 3..0 with `warm` (e.g. 2 warps x 20 iterations),
  * or per scale with warps_per_scale[s] (in [1, warm->warps]) and
- * iters_per_scale[s] (index 0 = finest; either array may be NULL for the
- * uniform value of `warm`).
+ * iters_per_scale[s] for s = 0 (finest) .. 3; either array may be NULL for
+ * the uniform value of `warm`, and entries beyond scale 3 are ignored.
  * With `plain` non-NULL the plain solve also runs and is the judge: a pair's
  * warm result is kept only if (a) its TV-L1 energy (non-linearised: sum
  * |grad u| + lambda * sum |I1(x+u) - I0(x)|, bicubic warp with border zeroing)

@@ -626,6 +626,7 @@ oflow_status oflow_batch(oflow_ctx *ctx, int n, const oflow_job *jobs) {
         }
         finish(ctx, device_only);
         for (auto &t : mb->tv) t->check_device_error();
+        for (auto &t : mb->hs) t->check_device_error();
     });
 }
 
@@ -696,8 +697,10 @@ oflow_status oflow_hs_batch(oflow_ctx *ctx, int n, const oflow_image *I0,
         for (int i = 0; i < n; i++) check_flow(&out[i], I0[i].width);
         const cudaStream_t st = ctx->stream();
         bool device_only = true;
+        std::vector<HsPlan *> ran;
         for (const Group &g : group_pairs(n, I0, I1)) {
             HsPlan *pl = &hs_plan(ctx, g.w, g.h, (int)g.idx.size(), g.dtype, *p);
+            ran.push_back(pl);
             for (size_t b = 0; b < g.idx.size(); b++) {
                 stage_image(I0[g.idx[b]], pl->raw_input((int)b, 0), dtype_size(g.dtype), st);
                 stage_image(I1[g.idx[b]], pl->raw_input((int)b, 1), dtype_size(g.dtype), st);
@@ -711,6 +714,7 @@ oflow_status oflow_hs_batch(oflow_ctx *ctx, int n, const oflow_image *I0,
             }
         }
         finish(ctx, device_only);
+        for (HsPlan *pl : ran) pl->check_device_error();
     });
 }
 
@@ -1106,6 +1110,7 @@ oflow_status oflow_stream_push(oflow_stream *s, const oflow_image *frames, const
         s->frames++;
         finish(s->ctx, device_only);
         if (s->tv) s->tv->check_device_error();
+        if (s->hs) s->hs->check_device_error();
     });
 }
 

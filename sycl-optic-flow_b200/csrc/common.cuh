@@ -62,24 +62,6 @@ __device__ __forceinline__ float cubic_cell(float v0, float v1, float v2, float 
     return (float)r;
 }
 
-// cubic_cell with the samples' double conversions given: v0..v3 are the
-// samples as doubles, d20 = v2 - v0 and d12 = v1 - v2 their single-precision
-// differences.  The same operations in the same order, so the same result.
-__device__ __forceinline__ float cubic_cell_d(double v0, double v1, double v2, double v3,
-                                              float d20, float d12, double xd) {
-    double c3 = 3.0 * (double)d12;
-    c3 = c3 + v3;
-    c3 = c3 - v0;
-    double c2 = 2.0 * v0;
-    c2 = c2 - 5.0 * v1;
-    c2 = c2 + 4.0 * v2;
-    c2 = c2 - v3;
-    c2 = c2 + xd * c3;
-    const double t = (double)d20 + xd * c2;
-    const double r = v1 + (0.5 * xd) * t;
-    return (float)r;
-}
-
 // Stencil of the reference's bicubic sample (bicubic_interpolation.cpp:74-128):
 // columns/rows step away from zero by the coordinate's sign; the row above
 // steps by the x sign (the reference's sx/sy mix-up, :92).  Returns false when

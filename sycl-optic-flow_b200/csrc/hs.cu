@@ -15,9 +15,13 @@
 // a TW x TH tile held in shared memory with a K-pixel halo; the halo shrinks
 // by one pixel per sweep, so after K sweeps the owned tile is exact (clamped
 // neighbours at the image border are exact at every sweep).
+#include <cstring>
+
 #include "common.cuh"
 #include "hs.hpp"
 #include "internal.hpp"
+#include "ptx.cuh"
+#include "tvl1.hpp"
 
 namespace oflow {
 
@@ -88,6 +92,15 @@ __global__ void __launch_bounds__(kDTW *kDTH) k_hs_warp_deriv(
     D[(size_t)b * dstride + (size_t)y * w + x] = make_float4(Ix, Iy, Iz, den);
 }
 
+// Region loads of k_hs_jacobi by TMA: D as (2w, h, pair) and the incoming
+// increments as (w, h, pair), 8-byte elements, zero fill outside the level
+// (pixels outside are never read by a sweep).  use = 0: plain loads.
+struct HsTma {
+    int use;
+    int *err;  // set when a bounded wait gives up
+    CUtensorMap tD, tIn;
+};
+
 // K Jacobi sweeps (solverKernel.cuh:41-153) on a tile with a KH-pixel halo.
 // sweeps <= KH.  first: increments start at 0 (flow.cu:168-171).  last: add
 // the increment to the flow (AddKernel, addKernel.cuh:28-36) instead of
@@ -96,9 +109,10 @@ template <int TW, int TH, int KH, int NT>
 __global__ void __launch_bounds__(NT) k_hs_jacobi(const float4 *__restrict__ D, size_t dstride,
                                                   const float2 *__restrict__ dUin,
                                                   float2 *dUout, float2 *U, size_t stride,
-                                                  int w, int h, int sweeps, int first, int last) {
+                                                  int w, int h, int sweeps, int first, int last,
+                                                  const __grid_constant__ HsTma tma) {
     constexpr int RW = TW + 2 * KH, RH = TH + 2 * KH, RN = RW * RH;
-    extern __shared__ float4 smem[];
+    extern __shared__ __align__(128) float4 smem[];
     float4 *sD = smem;                                   // RN
     float2 *sA = reinterpret_cast<float2 *>(sD + RN);    // RN
     float2 *sB = sA + RN;                                // RN
@@ -106,17 +120,41 @@ __global__ void __launch_bounds__(NT) k_hs_jacobi(const float4 *__restrict__ D, 
     const float4 *Db = D + (size_t)b * dstride;
     const float2 *In = dUin + (size_t)b * stride;
     const int x0 = blockIdx.x * TW - KH, y0 = blockIdx.y * TH - KH;
-    for (int i = threadIdx.x; i < RN; i += NT) {
-        const int x = x0 + i % RW, y = y0 + i / RW;
-        float4 d = make_float4(0.f, 0.f, 0.f, 1.f);
-        float2 a = make_float2(0.f, 0.f);
-        if (x >= 0 && x < w && y >= 0 && y < h) {
-            const size_t p = (size_t)y * w + x;
-            d = Db[p];
-            if (!first) a = In[p];
+    const uint32_t sbase = smem_u32(smem);
+    if (tma.use && (sbase & 127u) == 0) {
+        __shared__ __align__(8) unsigned long long s_bar;
+        const uint32_t bar = smem_u32(&s_bar);
+        if (threadIdx.x == 0) {
+            mbar_init(bar, 1);
+            fence_mbar_init();
+            mbar_arrive_expect_tx(bar, (uint32_t)RN * (first ? 16u : 24u));
+            tma_load_3d(sbase, &tma.tD, 2 * x0, y0, b, bar);
+            if (!first) tma_load_3d(sbase + RN * 16, &tma.tIn, x0, y0, b, bar);
         }
-        sD[i] = d;
-        sA[i] = a;
+        if (first)
+            for (int i = threadIdx.x; i < RN; i += NT) sA[i] = make_float2(0.f, 0.f);
+        __syncthreads();  // the barrier is initialised before anyone waits on it
+        const bool ok = mbar_wait_bounded(bar, 0);
+        if (__syncthreads_or(!ok)) {
+            // report, let the copies land (bounded), leave; the host drops
+            // the plan's results
+            if (threadIdx.x == 0) atomicExch(tma.err, 1);
+            mbar_wait_bounded(bar, 0);
+            return;
+        }
+    } else {
+        for (int i = threadIdx.x; i < RN; i += NT) {
+            const int x = x0 + i % RW, y = y0 + i / RW;
+            float4 d = make_float4(0.f, 0.f, 0.f, 1.f);
+            float2 a = make_float2(0.f, 0.f);
+            if (x >= 0 && x < w && y >= 0 && y < h) {
+                const size_t p = (size_t)y * w + x;
+                d = Db[p];
+                if (!first) a = In[p];
+            }
+            sD[i] = d;
+            sA[i] = a;
+        }
     }
     __syncthreads();
     float2 *src = sA, *dst = sB;
@@ -231,22 +269,44 @@ constexpr size_t hs_smem(const HsJCfg &c) { return (size_t)(c.tw + 2 * c.k) * (c
 template <int TW, int TH, int KH, int NT>
 static void hs_jacobi_launch(dim3 g, cudaStream_t st, const float4 *D, size_t dstride,
                              const float2 *in, float2 *out, float2 *U, size_t stride, int w,
-                             int h, int sweeps, int first, int last) {
+                             int h, int sweeps, int first, int last, const HsTma &tma) {
     const size_t smem = (size_t)(TW + 2 * KH) * (TH + 2 * KH) * 32;
     k_hs_jacobi<TW, TH, KH, NT><<<g, NT, smem, st>>>(D, dstride, in, out, U, stride, w, h, sweeps,
-                                                     first, last);
+                                                     first, last, tma);
 }
 
 static void hs_jacobi_cfg(int c, dim3 g, cudaStream_t st, const float4 *D, size_t dstride,
                           const float2 *in, float2 *out, float2 *U, size_t stride, int w, int h,
-                          int sweeps, int first, int last) {
+                          int sweeps, int first, int last, const HsTma &t) {
     switch (c) {
-        case 1: hs_jacobi_launch<32, 16, 8, 256>(g, st, D, dstride, in, out, U, stride, w, h, sweeps, first, last); break;
-        case 2: hs_jacobi_launch<64, 32, 8, 512>(g, st, D, dstride, in, out, U, stride, w, h, sweeps, first, last); break;
-        case 3: hs_jacobi_launch<64, 16, 4, 256>(g, st, D, dstride, in, out, U, stride, w, h, sweeps, first, last); break;
-        case 4: hs_jacobi_launch<32, 32, 16, 512>(g, st, D, dstride, in, out, U, stride, w, h, sweeps, first, last); break;
-        default: hs_jacobi_launch<32, 16, 4, 256>(g, st, D, dstride, in, out, U, stride, w, h, sweeps, first, last); break;
+        case 1: hs_jacobi_launch<32, 16, 8, 256>(g, st, D, dstride, in, out, U, stride, w, h, sweeps, first, last, t); break;
+        case 2: hs_jacobi_launch<64, 32, 8, 512>(g, st, D, dstride, in, out, U, stride, w, h, sweeps, first, last, t); break;
+        case 3: hs_jacobi_launch<64, 16, 4, 256>(g, st, D, dstride, in, out, U, stride, w, h, sweeps, first, last, t); break;
+        case 4: hs_jacobi_launch<32, 32, 16, 512>(g, st, D, dstride, in, out, U, stride, w, h, sweeps, first, last, t); break;
+        default: hs_jacobi_launch<32, 16, 4, 256>(g, st, D, dstride, in, out, U, stride, w, h, sweeps, first, last, t); break;
     }
+}
+
+// Tensor maps of the Jacobi region loads for configuration c on a level of
+// w x h (pairs N apart, B pairs) reading increments from `in`.  TMA wants
+// 16-byte strides: even w and N, else the kernel loads the region itself.
+static HsTma hs_tma(int c, const float4 *D, const float2 *in, int w, int h, size_t N, int B,
+                    int *err) {
+    HsTma t;
+    memset(&t, 0, sizeof(t));
+    t.err = err;
+    if ((w & 1) || (N & 1) || err == nullptr) return t;
+    const HsJCfg &jc = kHsCfgs[c];
+    const cuuint32_t rw = (cuuint32_t)(jc.tw + 2 * jc.k), rh = (cuuint32_t)(jc.th + 2 * jc.k);
+    const cuuint64_t dd[3] = {2 * (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)B};
+    const cuuint64_t sd[2] = {16 * (cuuint64_t)w, 16 * (cuuint64_t)N};
+    const cuuint32_t bd[3] = {2 * rw, rh, 1};
+    const cuuint64_t di[3] = {(cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)B};
+    const cuuint64_t si[2] = {8 * (cuuint64_t)w, 8 * (cuuint64_t)N};
+    const cuuint32_t bi[3] = {rw, rh, 1};
+    t.use = encode_map8(&t.tD, const_cast<float4 *>(D), 3, dd, sd, bd) &&
+            encode_map8(&t.tIn, const_cast<float2 *>(in), 3, di, si, bi);
+    return t;
 }
 
 static void hs_set_smem_attrs() {
@@ -353,8 +413,9 @@ void HsPlan::record(cudaStream_t st) {
             while (done < prm_.nsolver) {
                 const int k = imin(jc.k, prm_.nsolver - done);
                 const bool first = done == 0, last = done + k == prm_.nsolver;
+                const HsTma tm = hs_tma(jcfg_[l], D, dU[cur], lw, lh, N_, B, err_.device());
                 hs_jacobi_cfg(jcfg_[l], jg, st, D, N_, dU[cur], dU[cur ^ 1], Ubuf[ub], N_, lw, lh, k,
-                              first, last);
+                              first, last, tm);
                 cur ^= 1;
                 done += k;
             }
@@ -402,8 +463,9 @@ void HsPlan::autotune(cudaStream_t st, TuneTable *table, int reps) {
                     int done = 0, cur = 0;
                     while (done < kSweeps) {
                         const int k = imin(jc.k, kSweeps - done);
+                        const HsTma tm = hs_tma(c, D, dU[cur], lw, lh, N_, B_, err_.device());
                         hs_jacobi_cfg(c, jg, st, D, N_, dU[cur], dU[cur ^ 1], U, N_, lw, lh, k,
-                                      done == 0, 0);
+                                      done == 0, 0, tm);
                         cur ^= 1;
                         done += k;
                     }
@@ -463,9 +525,15 @@ size_t hs_scratch_bytes(int w, int h, int nlevels) {
     return off;
 }
 
+void HsPlan::check_device_error() {
+    if (err_.take()) throw Error(OFLOW_ERR_TIMEOUT, "hs: a Jacobi tile's TMA load gave up its bounded wait");
+}
+
 void hs_enqueue_into(void *scratch, const float *I0, const float *I1, int w, int h, int pitch,
                      const oflow_hs_params &prm, float *u, float *v, int out_pitch,
                      cudaStream_t st) {
+    HsTma no_tma;  // this path loads its regions with plain instructions
+    memset(&no_tma, 0, sizeof(no_tma));
     const int L = prm.nlevels;
     int Wl[16], Hl[16];
     Wl[L - 1] = w;
@@ -517,7 +585,7 @@ void hs_enqueue_into(void *scratch, const float *I0, const float *I1, int w, int
                 const int k = imin(kJK, prm.nsolver - done);
                 k_hs_jacobi<kJTW, kJTH, kJK, kJNT><<<jg, kJNT, smem, st>>>(
                     D, N, dU[cur], dU[cur ^ 1], Ubuf[ub], N, lw, lh, k, done == 0,
-                    done + k == prm.nsolver);
+                    done + k == prm.nsolver, no_tma);
                 cur ^= 1;
                 done += k;
             }

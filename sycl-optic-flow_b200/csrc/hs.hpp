@@ -27,6 +27,9 @@ class HsPlan {
     int batch() const { return B_; }
     int dtype() const { return dtype_; }
     const oflow_hs_params &params() const { return prm_; }
+    // Throws OFLOW_ERR_TIMEOUT if a Jacobi launch gave up its bounded TMA
+    // wait since the last check; reads host memory only.
+    void check_device_error();
 
   private:
     int w_, h_, B_, dtype_;
@@ -40,6 +43,7 @@ class HsPlan {
            o_out_ = 0;
     int jcfg_[16] = {};
     Graph graph_;
+    HostFlag err_;
 };
 
 // Bytes of scratch hs_enqueue_into needs for one w x h pair (0: bad sizes).

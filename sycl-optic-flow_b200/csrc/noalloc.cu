@@ -1,13 +1,11 @@
 // Horn-Schunck for callers that cannot allocate device memory.
 //
-// Some callers of this library must not call cudaMalloc: code that runs
-// while a CUDA graph is being captured (a plain cudaMalloc there is not
-// recorded and breaks the capture), real-time frame loops that cannot take
-// the device-wide synchronisation a cudaMalloc/cudaFree may imply, and hosts
-// that hand the library a fixed memory budget up front.  oflow_hs_noalloc
-// serves them: its scratch is one static device array, allocated when the
-// library's device code is loaded and held by every GPU that loads it until
-// the process exits.
+// Some callers of this library must not call cudaMalloc: real-time frame
+// loops that cannot take the device-wide synchronisation a cudaMalloc/cudaFree
+// may imply, and hosts that hand the library a fixed memory budget up front.
+// oflow_hs_noalloc serves them: its scratch is one static device array,
+// allocated when the library's device code is loaded and held by every GPU
+// that loads it until the process exits.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -17,9 +15,9 @@
 
 namespace {
 
-// Capacity of the static scratch: 8 MiB.  With one level this covers frames
-// up to about 125,000 pixels (320x240 needs 5.2 MB); more levels need a little
-// more (the pyramid).
+// Capacity of the static scratch: 8 MiB.  With one level a frame needs 64 B
+// per pixel (320x240: 4.9 MB), so frames up to about 131,000 pixels fit; more
+// levels add up to 8/3 B per pixel (the pyramid).
 constexpr size_t kStaticScratchBytes = size_t(8) << 20;
 __device__ __align__(256) unsigned char g_hs_scratch[kStaticScratchBytes];
 
@@ -29,7 +27,8 @@ void *g_scratch_addr[kMaxDevices] = {};
 
 // Device address of g_hs_scratch on the current device.  In host code the
 // array's name is only a host-side stand-in, so the address is looked up once
-// per device with that device current and cached.
+// per device with that device current and cached for the process (a device
+// reset, after which the array may sit elsewhere, is not followed).
 cudaError_t scratch_address(void **out) {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);

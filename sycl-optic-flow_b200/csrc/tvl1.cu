@@ -74,6 +74,10 @@ constexpr int kLvNT = 1024;
 constexpr int kLvMaxPx = 9216;  // u (8 B) + p (16 B) per pixel: 221,184 B of shared memory
 inline bool level_fits(int nx, int ny) { return (long long)nx * ny <= kLvMaxPx; }
 constexpr size_t tb_smem_bytes(int tw, int th) { return (size_t)(tw + 2 * kTbK) * (th + 2 * kTbK) * 40; }
+// Resident blocks per SM the tiled kernels are compiled for (registers: 64
+// for 512 threads, 85 for fewer), matching what their shared memory allows
+// (64x32: 2, 64x16: 3; the smaller tiles are not limited by it).
+constexpr int tb_min_blocks(int nt) { return nt >= 512 ? 2 : nt >= 256 ? 3 : 6; }
 constexpr int kGaussTW = 32, kGaussTH = 16, kGaussNT = 256, kGaussMaxR = 15;
 constexpr int kIngestNT = 256, kIngestPPT = 8;
 
@@ -446,31 +450,20 @@ __global__ void k_grad_pack(const float *__restrict__ pyr, size_t pyr_stride, in
 // With first_warp, p is zeroed (tvl1.cpp:190-193).
 enum { kWarpFromU = 0, kWarpFromUz = 1, kWarpZero = 2 };
 
-// The Keys cubic of the reference computes in double (double literals on
-// single-precision samples), so each of the 48 samples a pixel reads must be
-// converted to double, and conversions ran the kernel at the rate of the
-// conversion pipe.  Neighbouring pixels read mostly the same samples, so a
-// block of 32 x 8 pixels first finds the rectangle its stencils cover,
-// converts each sample of that rectangle once into shared memory (I1, I1x,
-// I1y as doubles, and as floats for the single-precision differences), and
-// interpolates from there: about 5 conversions of samples per pixel instead
-// of 48.  A block whose rectangle exceeds kWarpCap samples (flow varying by
-// tens of pixels inside the block) reads and converts per pixel, as before
-// (`cap` <= kWarpCap; 0 forces that path, for tests).
-// The arithmetic is the reference's in both cases (cubic_cell_d equals
-// cubic_cell), so the output is identical.
-constexpr int kWarpCap = 1280;
-__global__ void __launch_bounds__(256, 4) k_warp(const float *__restrict__ pyr, size_t pyr_stride, const float4 *I1g,
+// 6 blocks of 256 per SM (40 registers, a few spilled): the 16-tap gathers
+// need the warps to hide their latency.  The 25 warps of the 1024x436 workload
+// took 3.74 ms at 3 blocks (66 registers), 3.14 at 5, 3.05 at 6, 3.75 at 8.
+// A form that staged each block's samples in shared memory as doubles (one
+// conversion per sample and block instead of per pixel) measured slower,
+// 4.35 against 3.80 ms: 64 registers and 46 KB of shared memory left 4 blocks
+// per SM, and the region load before the block barrier stalled.
+__global__ void __launch_bounds__(256, 6) k_warp(const float *__restrict__ pyr, size_t pyr_stride, const float4 *I1g,
                        float4 *WR, float2 *U0, float2 *U1, const float2 *Uz, float4 *P0,
                        float4 *P1, size_t stride, int nx, int ny, int mode, int first_warp,
-                       TvCtrl *ctrl, TbQueue *q, int *left, int cap) {
-    __shared__ double sD[3][kWarpCap];
-    __shared__ float sF[3][kWarpCap];
-    __shared__ int sLim[4][8];
+                       TvCtrl *ctrl, TbQueue *q, int *left) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int b = blockIdx.z;
-    const int lane = threadIdx.x, wid = threadIdx.y;  // blockDim = (32, 8)
     if (x == 0 && y == 0) {
         ctrl[b].n = 0;
         ctrl[b].stop = 0;
@@ -481,107 +474,41 @@ __global__ void __launch_bounds__(256, 4) k_warp(const float *__restrict__ pyr, 
         q[b].ticket = 0;  // the persistent form's work queue, re-armed per stage
         if (b == 0) *left = gridDim.z;
     }
-    const bool inb = x < nx && y < ny;
+    if (x >= nx || y >= ny) return;
+    const int cur = ctrl[b].cur;
     const size_t off = (size_t)b * stride, p = (size_t)y * nx + x;
-    float2 u = make_float2(0.0f, 0.0f);
-    BicubicStencil s;
-    bool valid = false;
-    if (inb) {
-        const int cur = ctrl[b].cur;
-        float2 *U = state_buf(U0, U1, cur) + off;
-        if (mode == kWarpFromU) {
-            u = U[p];
-        } else if (mode == kWarpFromUz) {
-            u = Uz[off + p];
-            U[p] = u;
-        } else {
-            U[p] = u;
-        }
-        if (first_warp) (state_buf(P0, P1, cur) + off)[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        valid = bicubic_stencil((float)x + u.x, (float)y + u.y, nx, ny, true, s);
+    float2 *U = state_buf(U0, U1, cur) + off;
+    float2 u;
+    if (mode == kWarpFromU) {
+        u = U[p];
+    } else if (mode == kWarpFromUz) {
+        u = Uz[off + p];
+        U[p] = u;
+    } else {
+        u = make_float2(0.0f, 0.0f);
+        U[p] = u;
     }
-    // the rectangle of samples the block's stencils read
-    int c0 = INT_MAX, c1 = INT_MIN, r0 = INT_MAX, r1 = INT_MIN;
-    if (valid) {
-        c0 = imin(imin(s.col[0], s.col[1]), imin(s.col[2], s.col[3]));
-        c1 = imax(imax(s.col[0], s.col[1]), imax(s.col[2], s.col[3]));
-        r0 = imin(imin(s.row[0], s.row[1]), imin(s.row[2], s.row[3]));
-        r1 = imax(imax(s.row[0], s.row[1]), imax(s.row[2], s.row[3]));
-    }
-    c0 = __reduce_min_sync(0xffffffffu, c0);
-    c1 = __reduce_max_sync(0xffffffffu, c1);
-    r0 = __reduce_min_sync(0xffffffffu, r0);
-    r1 = __reduce_max_sync(0xffffffffu, r1);
-    if (lane == 0) {
-        sLim[0][wid] = c0;
-        sLim[1][wid] = c1;
-        sLim[2][wid] = r0;
-        sLim[3][wid] = r1;
-    }
-    __syncthreads();
-    c0 = INT_MAX, c1 = INT_MIN, r0 = INT_MAX, r1 = INT_MIN;
-#pragma unroll
-    for (int w = 0; w < 8; w++) {
-        c0 = imin(c0, sLim[0][w]);
-        c1 = imax(c1, sLim[1][w]);
-        r0 = imin(r0, sLim[2][w]);
-        r1 = imax(r1, sLim[3][w]);
-    }
-    const float4 *G = I1g + off;
-    const int rw = c1 - c0 + 1, rh = r1 - r0 + 1;
-    // block-uniform; no valid pixel leaves c0 > c1
-    const bool staged = c0 <= c1 && (long long)rw * rh <= cap;
-    if (staged) {
-        for (int ly = wid; ly < rh; ly += 8) {
-            const float4 *row = G + (size_t)(r0 + ly) * nx + c0;
-            for (int lx = lane; lx < rw; lx += 32) {
-                const float4 t = __ldg(row + lx);
-                const int i = ly * rw + lx;
-                sD[0][i] = (double)t.x;
-                sD[1][i] = (double)t.y;
-                sD[2][i] = (double)t.z;
-                sF[0][i] = t.x;
-                sF[1][i] = t.y;
-                sF[2][i] = t.z;
-            }
-        }
-        __syncthreads();
-    }
-    if (!inb) return;
+    if (first_warp) (state_buf(P0, P1, cur) + off)[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float uu = (float)x + u.x, vv = (float)y + u.y;
     float Iw = 0.0f, Iwx = 0.0f, Iwy = 0.0f;
-    if (valid) {
-        float a[3][4];
-        if (staged) {
-            const double tyd = s.ty;
+    BicubicStencil s;
+    if (bicubic_stencil(uu, vv, nx, ny, true, s)) {
+        const float4 *G = I1g + off;
+        float a[4], bx[4], by[4];
 #pragma unroll
-            for (int c = 0; c < 4; c++) {
-                const int k0 = (s.row[0] - r0) * rw + s.col[c] - c0;
-                const int k1 = (s.row[1] - r0) * rw + s.col[c] - c0;
-                const int k2 = (s.row[2] - r0) * rw + s.col[c] - c0;
-                const int k3 = (s.row[3] - r0) * rw + s.col[c] - c0;
-#pragma unroll
-                for (int ch = 0; ch < 3; ch++) {
-                    const float f0 = sF[ch][k0], f1 = sF[ch][k1], f2 = sF[ch][k2];
-                    a[ch][c] = cubic_cell_d(sD[ch][k0], sD[ch][k1], sD[ch][k2], sD[ch][k3],
-                                            f2 - f0, f1 - f2, tyd);
-                }
-            }
-        } else {
-#pragma unroll
-            for (int c = 0; c < 4; c++) {
-                const float4 *col = G + s.col[c];
-                const float4 t0 = __ldg(col + (size_t)nx * s.row[0]);
-                const float4 t1 = __ldg(col + (size_t)nx * s.row[1]);
-                const float4 t2 = __ldg(col + (size_t)nx * s.row[2]);
-                const float4 t3 = __ldg(col + (size_t)nx * s.row[3]);
-                a[0][c] = cubic_cell(t0.x, t1.x, t2.x, t3.x, s.ty);
-                a[1][c] = cubic_cell(t0.y, t1.y, t2.y, t3.y, s.ty);
-                a[2][c] = cubic_cell(t0.z, t1.z, t2.z, t3.z, s.ty);
-            }
+        for (int c = 0; c < 4; c++) {
+            const float4 *col = G + s.col[c];
+            const float4 t0 = __ldg(col + (size_t)nx * s.row[0]);
+            const float4 t1 = __ldg(col + (size_t)nx * s.row[1]);
+            const float4 t2 = __ldg(col + (size_t)nx * s.row[2]);
+            const float4 t3 = __ldg(col + (size_t)nx * s.row[3]);
+            a[c] = cubic_cell(t0.x, t1.x, t2.x, t3.x, s.ty);
+            bx[c] = cubic_cell(t0.y, t1.y, t2.y, t3.y, s.ty);
+            by[c] = cubic_cell(t0.z, t1.z, t2.z, t3.z, s.ty);
         }
-        Iw = cubic_cell(a[0][0], a[0][1], a[0][2], a[0][3], s.tx);
-        Iwx = cubic_cell(a[1][0], a[1][1], a[1][2], a[1][3], s.tx);
-        Iwy = cubic_cell(a[2][0], a[2][1], a[2][2], a[2][3], s.tx);
+        Iw = cubic_cell(a[0], a[1], a[2], a[3], s.tx);
+        Iwx = cubic_cell(bx[0], bx[1], bx[2], bx[3], s.tx);
+        Iwy = cubic_cell(by[0], by[1], by[2], by[3], s.tx);
     }
     const float I0v = __ldg(pyr + (size_t)(2 * b) * pyr_stride + p);
     const float rho_c = (Iw - Iwx * u.x - Iwy * u.y - I0v);
@@ -633,16 +560,14 @@ __device__ __forceinline__ float2 th_u_update(float2 u, float4 wr, float4 pc, fl
 
 // Dual update (tvl1.cpp:268-291) from the forward differences of u(new):
 // g = 1 + tau/theta*hypot(grad u), p = (p + tau/theta*grad u) / g, with the
-// hypot and the divisions in their exact fast forms (exact_math.cuh).  Every
-// condition those forms need is checked without branching; a pixel outside
-// any of them takes the reference formulas in one shared branch.
+// hypot as glibc computes it (hypot_ref) and the divisions by Markstein's
+// correction from RN(1/g) (exact_math.cuh).  The conditions of the Markstein
+// form are checked without branching; a pixel outside them takes the IEEE
+// divisions in one shared branch.
 __device__ __forceinline__ float4 dual_update(float4 po, float f1x, float f1y, float f2x,
                                               float f2y, float taut) {
-    bool ok1, ok2;
-    float h1 = hypot_try(f1x, f1y, ok1);
-    float h2 = hypot_try(f2x, f2y, ok2);
-    float g1 = 1.0f + taut * h1;
-    float g2 = 1.0f + taut * h2;
+    const float g1 = 1.0f + taut * hypot_ref(f1x, f1y);
+    const float g2 = 1.0f + taut * hypot_ref(f2x, f2y);
     const float r1 = rcp_near_rn(g1), r2 = rcp_near_rn(g2);
     const float n1 = taut * f1x + po.x, n2 = taut * f1y + po.y;
     const float n3 = taut * f2x + po.z, n4 = taut * f2y + po.w;
@@ -651,13 +576,9 @@ __device__ __forceinline__ float4 dual_update(float4 po, float f1x, float f1y, f
     pn.y = markstein(n2, g1, r1);
     pn.z = markstein(n3, g2, r2);
     pn.w = markstein(n4, g2, r2);
-    const bool fast = ok1 && ok2 && rcp_in_range(g1) && rcp_in_range(g2) && markstein_safe(n1) &&
+    const bool fast = rcp_in_range(g1) && rcp_in_range(g2) && markstein_safe(n1) &&
                       markstein_safe(n2) && markstein_safe(n3) && markstein_safe(n4);
     if (!fast) {
-        if (!ok1) h1 = hypot_ref(f1x, f1y);
-        if (!ok2) h2 = hypot_ref(f2x, f2y);
-        g1 = 1.0f + taut * h1;
-        g2 = 1.0f + taut * h2;
         pn.x = n1 / g1;
         pn.y = n2 / g1;
         pn.z = n3 / g2;
@@ -893,23 +814,38 @@ __device__ __forceinline__ void tb_iteration(int j, float4 *sP, const float4 *sW
 // launch re-run exactly that many iterations from the untouched input.  The
 // result is that of one iteration per launch either way.  Partials are summed
 // in a fixed order, so the decision does not depend on block scheduling.
+// Dynamic shared memory the decision may reuse once the tile is stored: K x
+// (NT/32) doubles.  (Static shared memory is kept small: two 64x32 tiles per
+// SM leave it under 512 bytes a block.)
 template <int K, int NT>
 __device__ __forceinline__ bool tb_decide(const TbArgs &a, TvCtrl *ctrl, int b, int tile,
                                           int ntiles, const double (&err)[K], int kk, int fin,
-                                          int snap, int redo, int n0, TbQueue *q, int *left) {
-    __shared__ double sred[NT / 32];
+                                          int snap, int redo, int n0, TbQueue *q, int *left,
+                                          double *scratch) {
+    // The K sums share one block barrier: per warp a fixed shuffle tree, then
+    // thread 0 adds the warps in order (block_sum_double's order, per sum).
+    constexpr int NW = NT / 32;
+    double(*sred)[NW] = reinterpret_cast<double(*)[NW]>(scratch);
     __shared__ double sE[K];
     __shared__ int s_last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     double *part = a.partials + (size_t)b * a.max_tiles * K;
+    __syncthreads();  // every thread has stored its share of the tile (scratch overlays it)
 #pragma unroll
     for (int j = 0; j < K; j++) {
-        if (j < kk) {  // kk is uniform over the block
-            const double s = block_sum_double<NT>(err[j], sred);
-            if (threadIdx.x == 0) part[(size_t)tile * K + j] = s;
-            __syncthreads();
-        }
+        double v = err[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) sred[j][wid] = v;
     }
+    __syncthreads();
     if (threadIdx.x == 0) {
+        for (int j = 0; j < kk; j++) {
+            double r = 0.0;
+#pragma unroll
+            for (int w = 0; w < NW; w++) r += sred[j][w];
+            part[(size_t)tile * K + j] = r;
+        }
         __threadfence();
         const unsigned prev = atomicAdd(&ctrl->arrive, 1u);
         s_last = (prev == (unsigned)ntiles - 1);
@@ -917,12 +853,28 @@ __device__ __forceinline__ bool tb_decide(const TbArgs &a, TvCtrl *ctrl, int b, 
     __syncthreads();
     if (!s_last) return false;
     __threadfence();
-    for (int j = 0; j < kk; j++) {
-        double acc = 0.0;
-        for (int t = threadIdx.x; t < ntiles; t += NT) acc += __ldcg(part + (size_t)t * K + j);
-        const double tot = block_sum_double<NT>(acc, sred);
-        if (threadIdx.x == 0) sE[j] = tot;
+    {
+        double acc[K];
+#pragma unroll
+        for (int j = 0; j < K; j++) acc[j] = 0.0;
+        for (int t = threadIdx.x; t < ntiles; t += NT)
+#pragma unroll
+            for (int j = 0; j < K; j++)
+                if (j < kk) acc[j] += __ldcg(part + (size_t)t * K + j);
+#pragma unroll
+        for (int j = 0; j < K; j++) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc[j] += __shfl_down_sync(0xffffffffu, acc[j], o);
+            if (lane == 0) sred[j][wid] = acc[j];
+        }
         __syncthreads();
+        if (threadIdx.x == 0)
+            for (int j = 0; j < kk; j++) {
+                double r = 0.0;
+#pragma unroll
+                for (int w = 0; w < NW; w++) r += sred[j][w];
+                sE[j] = r;
+            }
     }
     if (threadIdx.x == 0) {
         const float npx = (float)(a.nx * a.ny);
@@ -1098,7 +1050,7 @@ __device__ __forceinline__ bool tb_tile(const TbArgs &a, int b, int tx, int ty, 
 }
 
 template <int TW, int TH, int K, int NT>
-__global__ void __launch_bounds__(NT, 2) k_tvl1_tb(const __grid_constant__ TbArgs a) {
+__global__ void __launch_bounds__(NT, tb_min_blocks(NT)) k_tvl1_tb(const __grid_constant__ TbArgs a) {
     extern __shared__ __align__(128) float4 tb_smem[];
     __shared__ __align__(8) unsigned long long s_bar;
     const int b = blockIdx.z;
@@ -1133,7 +1085,8 @@ __global__ void __launch_bounds__(NT, 2) k_tvl1_tb(const __grid_constant__ TbArg
     const int fin = t.cur == 0 ? 1 : 0;
     const int snap = (t.cur >= 2 && t.cur < 2 + (K - 1)) ? 2 + (K - 1) : 2;
     tb_decide<K, NT>(a, ctrl, b, blockIdx.y * gridDim.x + blockIdx.x, gridDim.x * gridDim.y, err,
-                     t.kk, fin, t.snaps ? snap : -1, t.redo, t.n0, nullptr, nullptr);
+                     t.kk, fin, t.snaps ? snap : -1, t.redo, t.n0, nullptr, nullptr,
+                     reinterpret_cast<double *>(tb_smem));
 }
 
 // Persistent form of k_tvl1_tb: one launch runs a whole warp stage of every
@@ -1148,7 +1101,7 @@ __global__ void __launch_bounds__(NT, 2) k_tvl1_tb(const __grid_constant__ TbArg
 // item, so items always finish; a block with nothing to take sleeps briefly,
 // and gives up with the error flag after kWaitNs without finding work.
 template <int TW, int TH, int K, int NT>
-__global__ void __launch_bounds__(NT, 2) k_tvl1_q(const __grid_constant__ TbArgs a, TbQueue *q,
+__global__ void __launch_bounds__(NT, tb_min_blocks(NT)) k_tvl1_q(const __grid_constant__ TbArgs a, TbQueue *q,
                                                   int *left, int tiles_x, int ntiles, int B) {
     extern __shared__ __align__(128) float4 tb_smem[];
     __shared__ __align__(8) unsigned long long s_bar;
@@ -1237,7 +1190,7 @@ __global__ void __launch_bounds__(NT, 2) k_tvl1_q(const __grid_constant__ TbArgs
         const int fin = t.cur == 0 ? 1 : 0;
         const int snap = (t.cur >= 2 && t.cur < 2 + (K - 1)) ? 2 + (K - 1) : 2;
         tb_decide<K, NT>(a, a.ctrl + b, b, tile, ntiles, err, t.kk, fin, t.snaps ? snap : -1,
-                         t.redo, t.n0, q, left);
+                         t.redo, t.n0, q, left, reinterpret_cast<double *>(tb_smem));
         __syncthreads();  // shared state of this item is dead before the next claim
     }
 }
@@ -1592,8 +1545,8 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 
 // A tiled map of 8-byte elements, zero fill outside; dims innermost first,
 // byte strides of dims 1..rank-1.
-static bool encode_map8(CUtensorMap *m, void *base, int rank, const cuuint64_t *dims,
-                        const cuuint64_t *strides, const cuuint32_t *box) {
+bool encode_map8(CUtensorMap *m, void *base, int rank, const cuuint64_t *dims,
+                 const cuuint64_t *strides, const cuuint32_t *box) {
     const PFN_cuTensorMapEncodeTiled_v12000 fn = tensor_map_encoder();
     if (!fn) return false;
     const cuuint32_t es[5] = {1, 1, 1, 1, 1};
@@ -1819,10 +1772,6 @@ TvPlan::TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, boo
     // iterations (k_tvl1_tb) instead of the persistent work queue (k_tvl1_q)
     if (const char *e = getenv("OFLOW_TB_QUEUE")) queue_off_env_ = atoi(e) == 0;
     queue_ = !queue_off_env_;
-    // OFLOW_WARP_STAGED=0 makes the warp read and convert its samples per
-    // pixel instead of through shared memory (same results; for tests)
-    warp_cap_ = kWarpCap;
-    if (const char *e = getenv("OFLOW_WARP_STAGED")) warp_cap_ = atoi(e) != 0 ? kWarpCap : 0;
     // scales above a warm start's first scale never record a count
     OF_CUDA(cudaMemset(ar_.at<char>(o_iters_), 0, (size_t)B * iter_stride_ * 4));
     tb_set_smem_attrs();
@@ -1948,7 +1897,7 @@ void TvPlan::record(cudaStream_t st) {
                                     : (s == s0_ ? (warm_ ? kWarpFromUz : kWarpZero) : kWarpFromUz);
             mark_begin(-1);
             k_warp<<<gr, blk, 0, st>>>(pyr + pyr_off_[s], lp, I1g, WR, U0, U1, Uz, P0, P1,
-                                       N0, nx, ny, mode, wi == 0, ctrl, queue, left, warp_cap_);
+                                       N0, nx, ny, mode, wi == 0, ctrl, queue, left);
             mark_end();
             launches_ += 1;
             ia.stage = s * prm_.warps + wi;
@@ -2165,7 +2114,7 @@ void TvPlan::true_energy(double *host_out, cudaStream_t st) {
 
 void TvPlan::set_schedule(const int *warps, const int *iters) {
     OF_CHECK(!trace_, "tvl1: a traced plan runs the uniform schedule");
-    for (int s = 0; s < ns_; s++) {
+    for (int s = 0; s <= s0_; s++) {  // the scales this plan solves
         const int w = warps ? warps[s] : prm_.warps, n = iters ? iters[s] : prm_.max_iterations;
         OF_CHECK(w >= 1 && w <= prm_.warps, "tvl1: warps of a scale must be in [1, params.warps]");
         OF_CHECK(n >= 0, "tvl1: iterations of a scale < 0");
@@ -2176,7 +2125,7 @@ void TvPlan::set_schedule(const int *warps, const int *iters) {
 }
 
 bool TvPlan::same_schedule(const int *warps, const int *iters) const {
-    for (int s = 0; s < ns_; s++) {
+    for (int s = 0; s <= s0_; s++) {
         if (sw_[s] != (warps ? warps[s] : prm_.warps)) return false;
         if (si_[s] != (iters ? iters[s] : prm_.max_iterations)) return false;
     }

@@ -3,6 +3,8 @@
 // iterations, output split).
 #pragma once
 
+#include <cuda.h>
+
 #include <map>
 #include <tuple>
 
@@ -44,6 +46,12 @@ int launch_zoom_out(const float *src, size_t sstride, int nx, int ny, float *T, 
                     size_t dstride, int nxx, int nyy, float zfactor, const GaussTaps &t,
                     int planes, cudaStream_t st);
 
+// A tiled TMA map of 8-byte elements with zero fill outside (dims innermost
+// first, byte strides of dims 1..rank-1, box per dim); false if the driver
+// refuses it (the caller then loads with plain instructions).
+bool encode_map8(CUtensorMap *m, void *base, int rank, const cuuint64_t *dims,
+                 const cuuint64_t *strides, const cuuint32_t *box);
+
 // Where a plan reads one input frame: a device pointer of the plan's dtype and
 // its row pitch in elements.
 struct FrameRef {
@@ -72,9 +80,10 @@ class TvPlan {
     // buffers, keeps the fastest and records it in `table`.
     void autotune(cudaStream_t st, TuneTable *table, int reps = 3);
     int tb_config(int s) const { return tb_cfg_[s]; }
-    // Per-scale schedule (index 0 = finest): warps in [1, params.warps] and
-    // iteration caps; nullptr keeps the parameters' uniform value.  Rebuilds
-    // the graph on change.  Not for traced plans.
+    // Per-scale schedule (index 0 = finest) of the scales the plan solves (0
+    // to its start scale; entries above are ignored): warps in [1,
+    // params.warps] and iteration caps; nullptr keeps the parameters' uniform
+    // value.  Rebuilds the graph on change.  Not for traced plans.
     void set_schedule(const int *warps, const int *iters);
     bool same_schedule(const int *warps, const int *iters) const;
     // Tiled warp stages as one persistent work-queue launch each (default) or
@@ -164,7 +173,6 @@ class TvPlan {
     size_t o_queue_ = 0, o_left_ = 0;
     bool queue_ = true;  // tiled stages as one persistent launch each
     bool queue_off_env_ = false;
-    int warp_cap_ = 0;   // samples k_warp may stage in shared memory
     void upload_frames(cudaStream_t st);
 };
 

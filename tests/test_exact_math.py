@@ -1,10 +1,10 @@
 """The exact fast forms of csrc/exact_math.cuh, compiled for the host, against
-the plain expressions they replace: hypot_fast / hypot2_fast against glibc's
-hypotf formula (float)sqrt((double)a^2 + (double)b^2), and the Markstein
-division against IEEE p / g.  Random operands over the whole exponent range,
-the tiny range where low-order product terms would be subnormal, and
-Pythagorean triples whose hypotenuse is exactly a float rounding midpoint
-(where double-then-single rounding and single rounding part ways)."""
+the functions they stand for: hypot_ref ((float)sqrt((double)a^2 +
+(double)b^2)) against this host's hypotf, which the reference's std::hypot
+calls, on random operands and on Pythagorean triples whose hypotenuse is
+exactly a float rounding midpoint; and the Markstein division against IEEE
+p / g on random operands over the whole exponent range, signed zeros and the
+TH step's range of g."""
 import os
 import shutil
 import subprocess
@@ -29,40 +29,21 @@ int main(int argc, char **argv) {
     const long n = atol(argv[1]);
     std::mt19937_64 rng(20240611);
     std::uniform_real_distribution<double> unit(1.0, 2.0);
-    long bad_h = 0, bad_h2 = 0, bad_d = 0, mids = 0, cases = 0;
+    long bad_h = 0, bad_d = 0, mids = 0, cases = 0;
     auto rnd = [&](int emin, int emax) {
         const int e = emin + (int)(rng() % (uint64_t)(emax - emin + 1));
         const float m = (float)unit(rng);
         const float v = ldexpf(m, e);
         return (rng() & 1) ? -v : v;
     };
-    auto check_h = [&](float a, float b) {
-        cases++;
-        if (!same(hypot_fast(a, b), hypot_ref(a, b))) bad_h++;
-    };
-    auto check_h2 = [&](float a1, float b1, float a2, float b2) {
-        float h1, h2;
-        hypot2_fast(a1, b1, a2, b2, h1, h2);
-        if (!same(h1, hypot_ref(a1, b1)) || !same(h2, hypot_ref(a2, b2))) bad_h2++;
-    };
     for (long i = 0; i < n; i++) {
         const float a = rnd(-140, 70), b = rnd(-140, 70);
-        check_h(a, b);
-        const float c = rnd(-30, 10), d = c * (float)unit(rng);  // similar magnitudes
-        check_h(c, d);
-        const float t = rnd(-62, -44), s = rnd(-75, -44);  // low terms near subnormal
-        check_h(t, s);
-        check_h2(a, b, t, s);
-        check_h2(c, d, 0.0f, t);
+        cases++;
+        if (!same(hypot_ref(a, b), hypotf(a, b))) bad_h++;
     }
-    const float sp[] = {0.0f, -0.0f, 1.0f, 3.0f, 4.0f, 1e-45f, 1e-38f, 3e38f, INFINITY, -INFINITY, NAN};
-    for (float a : sp)
-        for (float b : sp) {
-            check_h(a, b);
-            check_h2(a, b, b, a);
-        }
     // primitive triples m^2-n^2, 2mn, m^2+n^2 with an odd 25-bit hypotenuse:
-    // sqrt(a^2+b^2) lies exactly halfway between two floats
+    // sqrt(a^2+b^2) lies exactly halfway between two floats, where double then
+    // single rounding and single rounding part ways
     for (long i = 0; i < n; i++) {
         const uint64_t m = 2900 + rng() % 2900, k = 1 + rng() % (m - 1);
         if (((m ^ k) & 1) == 0) continue;
@@ -71,9 +52,10 @@ int main(int argc, char **argv) {
         const int sc = (int)(rng() % 40) - 20;
         const float fa = ldexpf((float)a, sc), fb = ldexpf((float)b, sc);
         mids++;
-        check_h(fa, fb);
-        check_h(fb, -fa);
-        check_h(nextafterf(fa, 0.0f), fb);
+        for (float x : {fa, nextafterf(fa, 0.0f)}) {
+            cases++;
+            if (!same(hypot_ref(x, fb), hypotf(x, fb))) bad_h++;
+        }
     }
     // Markstein division for the dual update's g >= 1, p of any size and sign
     for (long i = 0; i < n; i++) {
@@ -92,7 +74,7 @@ int main(int argc, char **argv) {
         const float y = 1.0f / g;
         if (rcp_in_range(g) && markstein_safe(p) && !same(markstein(p, g, y), p / g)) bad_d++;
     }
-    printf("%ld %ld %ld %ld %ld\n", bad_h, bad_h2, bad_d, mids, cases);
+    printf("%ld %ld %ld %ld\n", bad_h, bad_d, mids, cases);
     return 0;
 }
 '''
@@ -108,6 +90,6 @@ def test_exact_fast_forms_equal_plain_expressions(tmp_path):
                            "-I", os.path.join(PKG, "csrc"), "-I", cuda_inc, str(src), "-o",
                            str(exe), "-lm"])
     out = subprocess.run([str(exe), "300000"], capture_output=True, text=True, check=True)
-    bad_h, bad_h2, bad_d, mids, cases = map(int, out.stdout.split())
-    assert mids > 1000 and cases > 1_000_000
-    assert (bad_h, bad_h2, bad_d) == (0, 0, 0)
+    bad_h, bad_d, mids, cases = map(int, out.stdout.split())
+    assert mids > 1000 and cases > 300_000
+    assert (bad_h, bad_d) == (0, 0)

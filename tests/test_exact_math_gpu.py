@@ -1,8 +1,8 @@
-"""The hardware-estimate refinements behind the TV-L1 kernels' exact fast
-forms, checked on the device (the host cannot reproduce the estimate
-instructions): every positive normal float for the square root, every float
-of the reciprocal's range, and 2^28 seeded operand pairs each for the hypot
-and the Markstein quotient.  Any mismatch would change the flow's bits."""
+"""The hardware-estimate refinement behind the TV-L1 kernels' exact fast
+division, checked on the device (the host cannot reproduce the estimate
+instruction): every float of the refined reciprocal's range, and 2^28
+seeded operand pairs twice for the Markstein quotient built on it.  Any
+mismatch would change the flow's bits."""
 import ctypes as C
 
 import pytest
@@ -21,17 +21,8 @@ def _bits(f):
     return struct.unpack("<I", struct.pack("<f", f))[0]
 
 
-def test_sqrt_near_within_one_ulp_for_every_normal_float(of):
-    assert _count(of, 0, 0x00800000, 0x7F800000) == 0
-
-
 def test_refined_reciprocal_correctly_rounded_over_its_range(of):
     assert _count(of, 1, _bits(2.0 ** -40), _bits(2.0 ** 24)) == 0
-
-
-@pytest.mark.parametrize("seed", [1, 2])
-def test_fast_hypot_equals_double_formula(of, seed):
-    assert _count(of, 2, 0, 1 << 28, seed) == 0
 
 
 @pytest.mark.parametrize("seed", [3, 4])

@@ -241,14 +241,12 @@ def test_repeated_full_size_solves_match_the_oracle(of, orc, monkeypatch, cfg):
         assert np.array_equal(u, ou) and np.array_equal(v, ov)
 
 
-@pytest.mark.parametrize("env", [{"OFLOW_TB_QUEUE": "0"}, {"OFLOW_WARP_STAGED": "0"},
-                                 {"OFLOW_TB_QUEUE": "0", "OFLOW_WARP_STAGED": "0"}])
+@pytest.mark.parametrize("env", [{"OFLOW_TB_QUEUE": "0"}, {"OFLOW_TB_QUEUE": "1"}])
 @pytest.mark.parametrize("w,h,ns", [(1024, 436, 5), (131, 77, 4), (333, 201, 5)])
 def test_alternative_kernel_forms_match_the_oracle(of, orc, monkeypatch, env, w, h, ns):
     """The tiled stages as one launch per block of iterations (k_tvl1_tb)
-    instead of the persistent work queue, and the warp reading its samples
-    per pixel instead of through shared memory: the same bits as the oracle
-    (and so as the default forms).  Odd widths take the plain region loads."""
+    and as one persistent work-queue launch per stage (k_tvl1_q): the same
+    bits as the oracle.  Odd widths take the plain region loads."""
     for k, v in env.items():
         monkeypatch.setenv(k, v)
     _, a, b = _pair(w + h, w, h, radius=min(w, h) / 5.0)

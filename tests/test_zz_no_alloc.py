@@ -1,5 +1,5 @@
 """oflow_hs_noalloc, the Horn-Schunck entry point for callers that cannot
-allocate device memory (graph capture, real-time loops, fixed budgets): called
+allocate device memory (real-time loops, fixed memory budgets): called
 through the C ABI on device buffers, twice in a row, it must give the same flow
 as the regular oflow_hs entry point, allocate nothing between calls, and reject
 frames beyond its static scratch.  Kept in its own file, collected last."""
