@@ -64,16 +64,16 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "k_tvl1_tb_1024x436.md")
+TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "k_tvl1_q_1024x436.md")
 
 
 def ncu_traffic():
-    """DRAM bytes per pair of one finest-scale inner-iteration launch, from the
-    committed ncu summary (a line 'traffic_bytes_per_pair_per_launch: N'), or
-    None."""
+    """DRAM bytes per pair-iteration of the finest-scale inner iterations, from
+    the committed ncu summary (a line 'traffic_bytes_per_pair_iteration: N'),
+    or None."""
     try:
         for line in open(TRAFFIC_PROFILE):
-            if line.startswith("traffic_bytes_per_pair_per_launch:"):
+            if line.startswith("traffic_bytes_per_pair_iteration:"):
                 return float(line.split(":")[1].split()[0])
     except OSError:
         pass
@@ -470,9 +470,13 @@ def our_arm(args, rank, world, local_rank):
     iters_total = int(sum(int(s["iterations"].sum()) for s in stats))
     peak, peak_kind = measured_peak()
     achieved = alg0 / (ms0 / 1e3) / 1e9 if ms0 > 0 else None
+    # the dominant launch: the persistent stage of the finest scale's first
+    # warp (all pairs' iterations of that stage); its DRAM traffic from the
+    # per-pair-iteration figure of the committed capture
+    it00 = sum(int(s["iterations"][0][0]) for s in stats)
     traffic = ncu_traffic()
     if traffic is not None:
-        traffic *= P  # DRAM traffic of a launch grows with the pairs it processes
+        traffic *= it00
     # the graph replays' launch count (inner iterations run as device-ended
     # while-loops, so it depends on the data); the timed steps replay the same
     # pairs, so each step launched the same kernels
@@ -574,13 +578,14 @@ def our_arm(args, rank, world, local_rank):
         "e2e": {"value": world * P * e2e_steps / t_e2e, "unit": "pairs/s",
                 "h2d_bytes_per_step": P * 2 * W * H, "d2h_bytes_per_step": P * 2 * W * H * 4},
         "gpu_launches": args.steps * launches_per_step,
-        "roofline": {"bound": "hbm", "kernel": "k_tvl1_tb (inner iterations, finest scale)",
+        "roofline": {"bound": "hbm", "kernel": "k_tvl1_q (inner iterations, finest scale)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
                      "traffic": traffic, "peak_source": peak_kind,
                      "bytes_basis": "algorithmic 60 B/px per inner iteration; traffic = DRAM "
-                                    "bytes of one full finest-scale launch (4 iterations)",
-                     "traffic_algorithmic_same_launch": P * nx[0] * ny[0] * 4 * BYTES_PER_PX_ITER,
+                                    "bytes of the finest scale's first-warp stage launch (ncu "
+                                    "bytes per pair-iteration x that stage's iterations)",
+                     "traffic_algorithmic_same_launch": it00 * nx[0] * ny[0] * BYTES_PER_PX_ITER,
                      "finest_scale_ms": round(ms0, 3),
                      "all_scales_achieved": alg_iter / (prof["iter_ms"] / 1e3) / 1e9
                      if prof["iter_ms"] > 0 else None,

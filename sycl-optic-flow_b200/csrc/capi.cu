@@ -236,6 +236,32 @@ std::vector<Group> group_pairs(int n, const oflow_image *I0, const oflow_image *
     return g;
 }
 
+// Points a plan's frame and output tables at one group's pairs: device frames
+// and flows are read and written in place; host frames are staged into the
+// plan's buffers and host flows come from its output buffer (copied after the
+// run by the caller).
+template <typename Plan>
+void bind_pairs(Plan &pl, const Group &g, const oflow_image *I0, const oflow_image *I1,
+                const oflow_flow *out, cudaStream_t s) {
+    for (size_t b = 0; b < g.idx.size(); b++) {
+        const int bi = (int)b;
+        const oflow_image *im[2] = {&I0[g.idx[b]], &I1[g.idx[b]]};
+        for (int k = 0; k < 2; k++) {
+            if (im[k]->location == OFLOW_DEVICE) {
+                pl.bind_frame(bi, k, im[k]->data, im[k]->pitch);
+            } else {
+                stage_image(*im[k], pl.raw_input(bi, k), dtype_size(g.dtype), s);
+                pl.bind_raw(bi, k);
+            }
+        }
+        const oflow_flow &o = out[g.idx[b]];
+        if (o.location == OFLOW_DEVICE)
+            pl.bind_out(bi, o.u, o.v, o.pitch);
+        else
+            pl.bind_own_out(bi);
+    }
+}
+
 void run_tvl1(oflow_ctx *ctx, int n, const oflow_image *I0, const oflow_image *I1,
               const oflow_tvl1_params *p, const oflow_flow *out, oflow_tvl1_stats *stats,
               double *energy_trace, oflow_tvl1_profile *prof = nullptr) {
@@ -701,16 +727,14 @@ oflow_status oflow_hs_batch(oflow_ctx *ctx, int n, const oflow_image *I0,
         for (const Group &g : group_pairs(n, I0, I1)) {
             HsPlan *pl = &hs_plan(ctx, g.w, g.h, (int)g.idx.size(), g.dtype, *p);
             ran.push_back(pl);
-            for (size_t b = 0; b < g.idx.size(); b++) {
-                stage_image(I0[g.idx[b]], pl->raw_input((int)b, 0), dtype_size(g.dtype), st);
-                stage_image(I1[g.idx[b]], pl->raw_input((int)b, 1), dtype_size(g.dtype), st);
-            }
+            bind_pairs(*pl, g, I0, I1, out, st);
             pl->run(st);
             for (size_t b = 0; b < g.idx.size(); b++) {
                 const oflow_flow &o = out[g.idx[b]];
+                if (o.location != OFLOW_HOST) continue;  // written in place
                 unstage_plane(pl->out_u((int)b), g.w, g.h, o.u, o.pitch, o.location, st);
                 unstage_plane(pl->out_v((int)b), g.w, g.h, o.v, o.pitch, o.location, st);
-                if (o.location == OFLOW_HOST) device_only = false;
+                device_only = false;
             }
         }
         finish(ctx, device_only);
@@ -737,6 +761,9 @@ oflow_status oflow_hs_autotune(oflow_ctx *ctx, int n, const oflow_image *I0,
         for (int b = 0; b < n; b++) {
             stage_image(I0[g.idx[b]], pl.raw_input(b, 0), dtype_size(g.dtype), st);
             stage_image(I1[g.idx[b]], pl.raw_input(b, 1), dtype_size(g.dtype), st);
+            pl.bind_raw(b, 0);
+            pl.bind_raw(b, 1);
+            pl.bind_own_out(b);
         }
         pl.run(st);
         pl.autotune(st, &ctx->tune);
@@ -810,16 +837,14 @@ oflow_status oflow_pyrlk_batch(oflow_ctx *ctx, int n, const oflow_image *I0,
                 keep_recent(ctx->pyrlk);
                 pl = ctx->pyrlk.back().get();
             }
-            for (int b = 0; b < B; b++) {
-                stage_image(I0[g.idx[b]], pl->raw_input(b, 0), dtype_size(g.dtype), st);
-                stage_image(I1[g.idx[b]], pl->raw_input(b, 1), dtype_size(g.dtype), st);
-            }
+            bind_pairs(*pl, g, I0, I1, out, st);
             pl->run(st);
             for (int b = 0; b < B; b++) {
                 const oflow_flow &o = out[g.idx[b]];
+                if (o.location != OFLOW_HOST) continue;  // written in place
                 unstage_plane(pl->out_u(b), g.w, g.h, o.u, o.pitch, o.location, st);
                 unstage_plane(pl->out_v(b), g.w, g.h, o.v, o.pitch, o.location, st);
-                if (o.location == OFLOW_HOST) device_only = false;
+                device_only = false;
             }
         }
         finish(ctx, device_only);

@@ -19,19 +19,13 @@
 
 #include "common.cuh"
 #include "hs.hpp"
+#include "pairio.hpp"
 #include "internal.hpp"
 #include "ptx.cuh"
 #include "tvl1.hpp"
 
 namespace oflow {
 
-template <typename In>
-__global__ void k_hs_ingest(const In *__restrict__ raw, float *dst, int N, int planes) {
-    const size_t total = (size_t)N * planes;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-         i += (size_t)gridDim.x * blockDim.x)
-        dst[i] = (float)raw[i];
-}
 
 // 2x2 box average (downscaleKernel.cuh:27-29), every output pixel written.
 __global__ void k_hs_downscale(const float *__restrict__ src, size_t sstride, int w, int h,
@@ -248,6 +242,43 @@ void launch_upscale2(const float2 *src, size_t sstride, int w, int h, float2 *ds
     k_upscale2<<<g, blk, 0, st>>>(src, sstride, w, h, dst, dstride, nw, nh, sx, sy);
 }
 
+template <typename T>
+__global__ void k_ingest_tab(const FrameRef *__restrict__ frames, int w, int h, float *dst,
+                             size_t N) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const FrameRef f = frames[blockIdx.z];
+    dst[(size_t)blockIdx.z * N + (size_t)y * w + x] =
+        (float)__ldg(static_cast<const T *>(f.p) + (size_t)y * f.pitch + x);
+}
+
+void launch_ingest_tab(const FrameRef *frames, int dtype, int w, int h, float *dst, size_t N,
+                       int planes, cudaStream_t st) {
+    dim3 blk(32, 8), g(div_up(w, 32), div_up(h, 8), planes);
+    if (dtype == OFLOW_U8)
+        k_ingest_tab<uint8_t><<<g, blk, 0, st>>>(frames, w, h, dst, N);
+    else
+        k_ingest_tab<float><<<g, blk, 0, st>>>(frames, w, h, dst, N);
+}
+
+__global__ void k_split_tab(const float2 *__restrict__ U, size_t stride, int w, int h,
+                            const OutRef *__restrict__ outs) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const OutRef o = outs[blockIdx.z];
+    const float2 u = U[(size_t)blockIdx.z * stride + (size_t)y * w + x];
+    o.u[(size_t)y * o.pitch + x] = u.x;
+    o.v[(size_t)y * o.pitch + x] = u.y;
+}
+
+void launch_split_tab(const float2 *U, size_t stride, int w, int h, const OutRef *outs, int B,
+                      cudaStream_t st) {
+    dim3 blk(32, 8), g(div_up(w, 32), div_up(h, 8), B);
+    k_split_tab<<<g, blk, 0, st>>>(U, stride, w, h, outs);
+}
+
 void launch_split2(const float2 *U, size_t stride, int N, float *out, int B, cudaStream_t st) {
     k_split2<<<dim3(imin(div_up(N, 1024), 1024), B), 256, 0, st>>>(U, stride, N, out,
                                                                    out + (size_t)B * N, B);
@@ -360,7 +391,18 @@ HsPlan::HsPlan(int w, int h, int B, int dtype, const oflow_hs_params &prm, const
     o_Ua_ = ar_.reserve(B * N_ * 8);
     o_Ub_ = ar_.reserve(B * N_ * 8);
     o_out_ = ar_.reserve(2 * B * N_ * 4);
+    o_ftab_ = ar_.reserve(sizeof(FrameRef) * 2 * B);
+    o_otab_ = ar_.reserve(sizeof(OutRef) * B);
     ar_.commit();
+    io_.init(ar_.at<FrameRef>(o_ftab_), ar_.at<OutRef>(o_otab_), B);
+    for (int b = 0; b < B; b++) {
+        bind_raw(b, 0);
+        bind_raw(b, 1);
+        bind_own_out(b);
+    }
+    // the default tables are valid for schedules recorded into a caller's graph
+    io_.upload(nullptr);
+    OF_CUDA(cudaStreamSynchronize(nullptr));
     hs_set_smem_attrs();
     for (int l = 0; l < L_; l++) {
         const auto it = tuned ? tuned->find(tune_key(W_[l], H_[l], B, kTuneHs)) : TuneTable::const_iterator();
@@ -375,6 +417,13 @@ void *HsPlan::raw_input(int b, int k) const {
 }
 const float *HsPlan::out_u(int b) const { return ar_.at<float>(o_out_) + (size_t)b * N_; }
 const float *HsPlan::out_v(int b) const { return ar_.at<float>(o_out_) + (size_t)(B_ + b) * N_; }
+void HsPlan::bind_frame(int b, int k, const void *p, int pitch) { io_.set_frame(b, k, p, pitch ? pitch : w_); }
+void HsPlan::bind_raw(int b, int k) { io_.set_frame(b, k, raw_input(b, k), w_); }
+void HsPlan::bind_out(int b, float *u, float *v, int pitch) { io_.set_out(b, u, v, pitch ? pitch : w_); }
+void HsPlan::bind_own_out(int b) {
+    float *o = ar_.at<float>(o_out_);
+    io_.set_out(b, o + (size_t)b * N_, o + (size_t)(B_ + b) * N_, w_);
+}
 
 void HsPlan::record(cudaStream_t st) {
     const int B = B_;
@@ -384,13 +433,9 @@ void HsPlan::record(cudaStream_t st) {
     float2 *Ubuf[2] = {ar_.at<float2>(o_Ua_), ar_.at<float2>(o_Ub_)};
     const int top = L_ - 1;
     {
-        const int nb = imin(div_up((int)(2 * B * N_), 1024), 4096);
-        if (dtype_ == OFLOW_U8)
-            k_hs_ingest<uint8_t><<<nb, 256, 0, st>>>(ar_.at<uint8_t>(o_raw_), pyr + pyr_off_[top],
-                                                     (int)N_, 2 * B);
-        else
-            k_hs_ingest<float><<<nb, 256, 0, st>>>(ar_.at<float>(o_raw_), pyr + pyr_off_[top],
-                                                   (int)N_, 2 * B);
+        // frames through the frame table (the caller's device frames in place,
+        // or this plan's staging buffers)
+        launch_ingest_tab(io_.frames(), dtype_, w_, h_, pyr + pyr_off_[top], N_, 2 * B, st);
     }
     for (int l = top; l > 0; l--) {
         dim3 blk(32, 8), g(div_up(W_[l - 1], 32), div_up(H_[l - 1], 8), 2 * B);
@@ -428,11 +473,12 @@ void HsPlan::record(cudaStream_t st) {
             ub ^= 1;
         }
     }
-    launch_split2(Ubuf[ub], N_, (int)N_, ar_.at<float>(o_out_), B, st);
+    launch_split_tab(Ubuf[ub], N_, w_, h_, io_.outs(), B, st);
     OF_CUDA(cudaGetLastError());
 }
 
 void HsPlan::run(cudaStream_t st) {
+    io_.upload(st);
     if (!graph_.ready()) graph_.capture(st, [&](cudaStream_t s) { record(s); });
     graph_.launch(st);
 }

@@ -2,6 +2,7 @@
 #pragma once
 
 #include "internal.hpp"
+#include "pairio.hpp"
 #include "tvl1.hpp"
 
 namespace oflow {
@@ -14,6 +15,14 @@ class HsPlan {
     void *raw_input(int b, int k) const;
     const float *out_u(int b) const;
     const float *out_v(int b) const;
+    // Frame k of pair b: a caller's device frame (read in place on every
+    // run; pitch in elements, 0 = width) or this plan's staging buffer.
+    void bind_frame(int b, int k, const void *p, int pitch);
+    void bind_raw(int b, int k);
+    // Flow of pair b: the caller's device planes (written in place) or this
+    // plan's output buffer (out_u / out_v).
+    void bind_out(int b, float *u, float *v, int pitch);
+    void bind_own_out(int b);
     void run(cudaStream_t st);
     void record(cudaStream_t st);
     // Times every Jacobi configuration (tile shape, sweeps per launch) at every
@@ -44,6 +53,8 @@ class HsPlan {
     int jcfg_[16] = {};
     Graph graph_;
     HostFlag err_;
+    size_t o_ftab_ = 0, o_otab_ = 0;
+    PairIo io_;
 };
 
 // Bytes of scratch hs_enqueue_into needs for one w x h pair (0: bad sizes).

@@ -140,23 +140,54 @@ __global__ void k_lk_grad(const float *__restrict__ src, size_t sstride, int nx,
     G[(size_t)blockIdx.z * gstride + (size_t)y * nx + x] = make_float2(ax, ay);
 }
 
+// lk_window_solve with the window radius known at compile time (the loops
+// unroll; the same sums in the same order).
+template <int C>
+__device__ __forceinline__ void lk_window_solve_c(const float *gx, const float *gy, const float *gt,
+                                                  int RW, int cidx, float &vx, float &vy) {
+    float sxx = 0.0f, sxy = 0.0f, syy = 0.0f, sxt = 0.0f, syt = 0.0f;
+#pragma unroll
+    for (int ii = -C; ii <= C; ii++) {
+        const int row = cidx + ii * RW;
+#pragma unroll
+        for (int jj = -C; jj <= C; jj++) {
+            const int q = row + jj;
+            const float ix = gx[q], iy = gy[q], it = gt[q];
+            sxx += ix * ix;
+            sxy += ix * iy;
+            syy += iy * iy;
+            sxt += ix * it;
+            syt += iy * it;
+        }
+    }
+    const float det = (sxx * syy - sxy * sxy);
+    vx = 0.0f;
+    vy = 0.0f;
+    if (det != 0.0f) {
+        vx = 1.0f / det * (syy * (-sxt) + (-sxy) * (-syt));
+        vy = 1.0f / det * ((-sxy) * (-sxt) + sxx * (-syt));
+    }
+}
+
 // One refinement of pyramidal LK: warp I1 by the current flow (bilinear,
 // clamp-to-edge), It = 0 + (-1)*I0 + 1*I1w, window solve, Uout = Uin + d.
-__global__ void __launch_bounds__(kLNT) k_pyrlk_iter(const float *__restrict__ pyr, size_t lp,
+// Tile 32 x 16 with the window radius C as halo.
+constexpr int kPTW = 32, kPTH = 16, kPNT = kPTW * kPTH;
+template <int C>
+__global__ void __launch_bounds__(kPNT) k_pyrlk_iter(const float *__restrict__ pyr, size_t lp,
                                                      const float2 *__restrict__ G, size_t gstride,
                                                      const float2 *__restrict__ Uin,
                                                      float2 *Uout, size_t ustride, int nx,
-                                                     int ny, int c) {
-    constexpr int RWm = kLTW + 2 * kLMaxC, RHm = kLTH + 2 * kLMaxC;
-    __shared__ float gx[RWm * RHm], gy[RWm * RHm], gt[RWm * RHm];
+                                                     int ny) {
+    constexpr int RW = kPTW + 2 * C, RH = kPTH + 2 * C;
+    __shared__ float gx[RW * RH], gy[RW * RH], gt[RW * RH];
     const int b = blockIdx.z;
     const float *I0 = pyr + (size_t)(2 * b) * lp;
     const float *I1 = pyr + (size_t)(2 * b + 1) * lp;
     const float2 *Gb = G + (size_t)b * gstride;
     const float2 *Ub = Uin + (size_t)b * ustride;
-    const int RW = kLTW + 2 * c, RH = kLTH + 2 * c;
-    const int x0 = blockIdx.x * kLTW - c, y0 = blockIdx.y * kLTH - c;
-    for (int i = threadIdx.x; i < RW * RH; i += kLNT) {
+    const int x0 = blockIdx.x * kPTW - C, y0 = blockIdx.y * kPTH - C;
+    for (int i = threadIdx.x; i < RW * RH; i += kPNT) {
         const int x = x0 + i % RW, y = y0 + i / RW;
         if (x < 0 || x >= nx || y < 0 || y >= ny) continue;
         const size_t p = (size_t)y * nx + x;
@@ -171,22 +202,27 @@ __global__ void __launch_bounds__(kLNT) k_pyrlk_iter(const float *__restrict__ p
         gt[i] = it;
     }
     __syncthreads();
-    const int x = blockIdx.x * kLTW + threadIdx.x % kLTW, y = blockIdx.y * kLTH + threadIdx.x / kLTW;
+    const int tx = threadIdx.x % kPTW, ty = threadIdx.x / kPTW;
+    const int x = blockIdx.x * kPTW + tx, y = blockIdx.y * kPTH + ty;
     if (x >= nx || y >= ny) return;
     float dx = 0.0f, dy = 0.0f;
-    if (x >= c && y >= c && x < nx - c && y < ny - c)
-        lk_window_solve(gx, gy, gt, RW, (threadIdx.x / kLTW + c) * RW + threadIdx.x % kLTW + c, c,
-                        dx, dy);
+    if (x >= C && y >= C && x < nx - C && y < ny - C)
+        lk_window_solve_c<C>(gx, gy, gt, RW, (ty + C) * RW + tx + C, dx, dy);
     const size_t p = (size_t)b * ustride + (size_t)y * nx + x;
     const float2 u = Ub[(size_t)y * nx + x];
     Uout[p] = make_float2(u.x + dx, u.y + dy);
 }
 
-template <typename In>
-__global__ void k_to_float(const In *__restrict__ raw, float *dst, size_t total) {
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-         i += (size_t)gridDim.x * blockDim.x)
-        dst[i] = (float)raw[i];
+static void launch_pyrlk_iter(int c, dim3 g, cudaStream_t st, const float *pyr, size_t lp,
+                              const float2 *G, size_t gstride, const float2 *Uin, float2 *Uout,
+                              size_t ustride, int nx, int ny) {
+    switch (c) {
+        case 0: k_pyrlk_iter<0><<<g, kPNT, 0, st>>>(pyr, lp, G, gstride, Uin, Uout, ustride, nx, ny); break;
+        case 1: k_pyrlk_iter<1><<<g, kPNT, 0, st>>>(pyr, lp, G, gstride, Uin, Uout, ustride, nx, ny); break;
+        case 2: k_pyrlk_iter<2><<<g, kPNT, 0, st>>>(pyr, lp, G, gstride, Uin, Uout, ustride, nx, ny); break;
+        case 3: k_pyrlk_iter<3><<<g, kPNT, 0, st>>>(pyr, lp, G, gstride, Uin, Uout, ustride, nx, ny); break;
+        default: k_pyrlk_iter<4><<<g, kPNT, 0, st>>>(pyr, lp, G, gstride, Uin, Uout, ustride, nx, ny); break;
+    }
 }
 
 // ================================================================ host plans
@@ -255,7 +291,26 @@ PyrLkPlan::PyrLkPlan(int w, int h, int B, int dtype, const oflow_lk_params &prm)
     o_U0_ = ar_.reserve(B * N_ * 8);
     o_U1_ = ar_.reserve(B * N_ * 8);
     o_out_ = ar_.reserve(2 * B * N_ * 4);
+    o_ftab_ = ar_.reserve(sizeof(FrameRef) * 2 * B);
+    o_otab_ = ar_.reserve(sizeof(OutRef) * B);
     ar_.commit();
+    io_.init(ar_.at<FrameRef>(o_ftab_), ar_.at<OutRef>(o_otab_), B);
+    for (int b = 0; b < B; b++) {
+        bind_raw(b, 0);
+        bind_raw(b, 1);
+        bind_own_out(b);
+    }
+    // the default tables are valid for schedules recorded into a caller's graph
+    io_.upload(nullptr);
+    OF_CUDA(cudaStreamSynchronize(nullptr));
+}
+
+void PyrLkPlan::bind_frame(int b, int k, const void *p, int pitch) { io_.set_frame(b, k, p, pitch ? pitch : w_); }
+void PyrLkPlan::bind_raw(int b, int k) { io_.set_frame(b, k, raw_input(b, k), w_); }
+void PyrLkPlan::bind_out(int b, float *u, float *v, int pitch) { io_.set_out(b, u, v, pitch ? pitch : w_); }
+void PyrLkPlan::bind_own_out(int b) {
+    float *o = ar_.at<float>(o_out_);
+    io_.set_out(b, o + (size_t)b * N_, o + (size_t)(B_ + b) * N_, w_);
 }
 
 void *PyrLkPlan::raw_input(int b, int k) const {
@@ -272,11 +327,8 @@ void PyrLkPlan::record(cudaStream_t st) {
     float2 *G = ar_.at<float2>(o_G_);
     float2 *U[2] = {ar_.at<float2>(o_U0_), ar_.at<float2>(o_U1_)};
     const LkTaps taps = make_lk_taps(prm_.spac, 2);
-    const int nb = imin(div_up((int)(2 * B * N_), 1024), 4096);
-    if (dtype_ == OFLOW_U8)
-        k_to_float<uint8_t><<<nb, 256, 0, st>>>(ar_.at<uint8_t>(o_raw_), pyr, 2 * B * N_);
-    else
-        k_to_float<float><<<nb, 256, 0, st>>>(ar_.at<float>(o_raw_), pyr, 2 * B * N_);
+    // frames through the frame table (device frames in place, or staged)
+    launch_ingest_tab(io_.frames(), dtype_, w_, h_, pyr, N_, 2 * B, st);
     for (int l = 1; l < L_; l++) {
         const size_t sp = (size_t)W_[l - 1] * H_[l - 1], dp = (size_t)W_[l] * H_[l];
         launch_zoom_out(pyr + pyr_off_[l - 1], sp, W_[l - 1], H_[l - 1], T, pyr + pyr_off_[l], dp,
@@ -291,10 +343,9 @@ void PyrLkPlan::record(cudaStream_t st) {
         dim3 blk(32, 8), g(div_up(lw, 32), div_up(lh, 8), B);
         // Ix, Iy of I0: plane 2b of the level, so a stride of two planes
         k_lk_grad<<<g, blk, 0, st>>>(pyr + pyr_off_[l], 2 * lp, lw, lh, taps, G, N_);
-        dim3 ig(div_up(lw, kLTW), div_up(lh, kLTH), B);
+        dim3 ig(div_up(lw, kPTW), div_up(lh, kPTH), B);
         for (int r = 0; r < prm_.iters; r++) {
-            k_pyrlk_iter<<<ig, kLNT, 0, st>>>(pyr + pyr_off_[l], lp, G, N_, U[cur], U[cur ^ 1], N_,
-                                              lw, lh, c);
+            launch_pyrlk_iter(c, ig, st, pyr + pyr_off_[l], lp, G, N_, U[cur], U[cur ^ 1], N_, lw, lh);
             cur ^= 1;
         }
         if (l > 0) {
@@ -304,11 +355,12 @@ void PyrLkPlan::record(cudaStream_t st) {
             cur ^= 1;
         }
     }
-    launch_split2(U[cur], N_, (int)N_, ar_.at<float>(o_out_), B, st);
+    launch_split_tab(U[cur], N_, w_, h_, io_.outs(), B, st);
     OF_CUDA(cudaGetLastError());
 }
 
 void PyrLkPlan::run(cudaStream_t st) {
+    io_.upload(st);
     if (!graph_.ready()) graph_.capture(st, [&](cudaStream_t s) { record(s); });
     graph_.launch(st);
 }

@@ -3,6 +3,7 @@
 #pragma once
 
 #include "internal.hpp"
+#include "pairio.hpp"
 #include "tvl1.hpp"
 
 namespace oflow {
@@ -34,6 +35,12 @@ class PyrLkPlan {
     void *raw_input(int b, int k) const;
     const float *out_u(int b) const;
     const float *out_v(int b) const;
+    // frame / flow bindings as in HsPlan (caller's device buffers in place,
+    // or this plan's staging and output buffers)
+    void bind_frame(int b, int k, const void *p, int pitch);
+    void bind_raw(int b, int k);
+    void bind_out(int b, float *u, float *v, int pitch);
+    void bind_own_out(int b);
     void run(cudaStream_t st);
     void record(cudaStream_t st);
     int width() const { return w_; }
@@ -52,6 +59,8 @@ class PyrLkPlan {
     size_t N_ = 0;
     Arena ar_;
     size_t o_raw_ = 0, o_T_ = 0, o_pyr_ = 0, o_G_ = 0, o_U0_ = 0, o_U1_ = 0, o_out_ = 0;
+    size_t o_ftab_ = 0, o_otab_ = 0;
+    PairIo io_;
     Graph graph_;
 };
 

@@ -160,6 +160,49 @@ def test_pyrlk_batch_matches_single_pairs(of, orc, ctx):
         assert _same(u, ou) and _same(v, ov)
 
 
+@pytest.mark.parametrize("solver", ["hs", "pyrlk"])
+def test_device_frames_and_flows_in_place(of, ctx, solver):
+    """Batches of device frames (uint8 with a row pitch, and float) and device
+    flows with a row pitch: read and written in place through the plans'
+    frame and output tables, bit-identical to the same pairs from host
+    memory; padding of the pitched output rows is left untouched."""
+    import torch
+    from oflow import synth
+    w, h = 97, 61
+    gen = [synth.lk_pair(seed=50 + i, w=w, h=h) for i in range(3)]
+    dev = torch.device("cuda", 0)
+    host = [(synth.quantize(g.I0), synth.quantize(g.I1)) for g in gen]
+    pitched = []
+    for a, b in host:  # uint8 frames inside wider device rows
+        pa = torch.zeros((h, w + 13), dtype=torch.uint8, device=dev)
+        pb = torch.zeros((h, w + 13), dtype=torch.uint8, device=dev)
+        pa[:, :w] = torch.from_numpy(a)
+        pb[:, :w] = torch.from_numpy(b)
+        pitched.append((pa[:, :w], pb[:, :w]))
+    outs = [(torch.full((h, w + 5), 7.0, device=dev)[:, :w],
+             torch.full((h, w + 5), 7.0, device=dev)[:, :w]) for _ in gen]
+    if solver == "hs":
+        prm = of.HSParams(2.0, 2, 2, 30)
+        ref = of.hs_batch(host, prm, ctx)
+        res = of.hs_batch(pitched, prm, ctx, out=outs)
+    else:
+        prm = of.LKParams(3, 2, 5, 2, 2)
+        ref = of.pyrlk_batch(host, prm, ctx)
+        res = of.pyrlk_batch(pitched, prm, ctx, out=outs)
+    torch.cuda.synchronize()
+    for (ru, rv), (u, v) in zip(ref, res):
+        assert np.array_equal(u.cpu().numpy(), ru) and np.array_equal(v.cpu().numpy(), rv)
+    for (u, v) in outs:  # the padding columns of the output rows
+        full_u = u.as_strided((h, w + 5), (w + 5, 1))
+        assert torch.all(full_u[:, w:] == 7.0)
+    # float frames on the device, contiguous flows
+    fl = [(torch.from_numpy(a.astype(np.float32)).to(dev),
+           torch.from_numpy(b.astype(np.float32)).to(dev)) for a, b in host]
+    res2 = of.hs_batch(fl, prm, ctx) if solver == "hs" else of.pyrlk_batch(fl, prm, ctx)
+    for (ru, rv), (u, v) in zip(ref, res2):
+        assert np.array_equal(u.cpu().numpy(), ru) and np.array_equal(v.cpu().numpy(), rv)
+
+
 def test_pyrlk_golden_and_accuracy(of, ctx):
     from oflow import synth
     d = dict(np.load(os.path.join(GOLDEN, "lk_80x60.npz")))
