@@ -334,6 +334,22 @@ def warm_measure(oflow, synth, np, torch, pairs, d_in, prm, ctx, stream, args, P
             row["judged_speedup_vs_plain"] = row["judged_sampled_value"] / t_plain
         rows.append(row)
     out = dict(rows[0])
+    # one training step of the network (batch 16, the library's own forward
+    # and backward kernels, Adam), timed over 10 steps
+    tnet = oflow.WarmNet(W, H, 16, ctx)
+    tnet.set_params(params)
+    fr = torch.stack([torch.stack([d_in[i % P][0], d_in[i % P][1]]) for i in range(16)])
+    tg = torch.zeros((16, tnet.out_h, tnet.out_w, 2), dtype=torch.float32, device=dev)
+    for _ in range(3):
+        tnet.train_step(fr, tg, 1e-6)
+    torch.cuda.synchronize()
+    t0 = time.time()
+    for _ in range(10):
+        tnet.train_step(fr, tg, 1e-6)
+    torch.cuda.synchronize()
+    out["training_step_ms"] = (time.time() - t0) * 100.0
+    out["training_step_config"] = ("batch 16 pairs of 1024x436, forward + backward + Adam, "
+                                   "host-timed per synchronous step")
     out["judge"] = ("plain 5x5x50 solve; energy <= 1.01 x plain and sum|warm-plain| <= 0.01 x "
                     "sum|plain|; judged throughput samples every 8th pair")
     out["training"] = meta

@@ -1254,9 +1254,40 @@ oflow_status oflow_conv3x3(int mode, int N, int H, int W, int C, int K, int stri
             conv_forward(d, static_cast<const __nv_bfloat16 *>(a), static_cast<const __nv_bfloat16 *>(b),
                          bias, out, out_f32 != 0, relu != 0, st);
         } else if (mode == 1) {
+            // the tcgen05 kernel; the shape must be one it takes
+            DevBuf err(sizeof(int)), scratch(conv_backward_data_umma_scratch(d));
+            OF_CUDA(cudaMemsetAsync(err.as<int>(), 0, sizeof(int), st));
+            OF_CHECK(conv_backward_data_umma(d, static_cast<const float *>(a),
+                                             static_cast<const __nv_bfloat16 *>(y_act),
+                                             static_cast<const __nv_bfloat16 *>(b),
+                                             static_cast<float *>(out), false, scratch.as<void>(),
+                                             err.as<int>(), st),
+                     "conv3x3: shape outside the tensor-core kernel (C % 16 == 0, K % 16 == 0)");
+            int e = 0;
+            OF_CUDA(cudaMemcpyAsync(&e, err.as<int>(), sizeof(int), cudaMemcpyDeviceToHost, st));
+            OF_CUDA(cudaStreamSynchronize(st));
+            if (e) throw Error(OFLOW_ERR_TIMEOUT, "conv3x3: a bounded wait gave up");
+        } else if (mode == 4) {
+            // the mma.sync backward-data kernel
             conv_backward_data(d, static_cast<const float *>(a), static_cast<const __nv_bfloat16 *>(y_act),
                                static_cast<const __nv_bfloat16 *>(b), static_cast<float *>(out), false, st);
         } else if (mode == 2) {
+            // the tcgen05 kernel; the shape must be one it takes
+            OF_CHECK(gbias != nullptr, "conv3x3: null bias gradient");
+            DevBuf err(sizeof(int)), scratch(conv_backward_data_umma_scratch(d));
+            OF_CUDA(cudaMemsetAsync(err.as<int>(), 0, sizeof(int), st));
+            OF_CHECK(conv_backward_weight_umma(d, static_cast<const float *>(a),
+                                               static_cast<const __nv_bfloat16 *>(y_act),
+                                               static_cast<const __nv_bfloat16 *>(b),
+                                               static_cast<float *>(out), gbias, scratch.as<void>(),
+                                               err.as<int>(), st),
+                     "conv3x3: shape outside the tensor-core kernel (C % 16 == 0, K <= 128)");
+            int e = 0;
+            OF_CUDA(cudaMemcpyAsync(&e, err.as<int>(), sizeof(int), cudaMemcpyDeviceToHost, st));
+            OF_CUDA(cudaStreamSynchronize(st));
+            if (e) throw Error(OFLOW_ERR_TIMEOUT, "conv3x3: a bounded wait gave up");
+        } else if (mode == 5) {
+            // the mma.sync backward-weight kernel
             OF_CHECK(gbias != nullptr, "conv3x3: null bias gradient");
             conv_backward_weight(d, static_cast<const float *>(a),
                                  static_cast<const __nv_bfloat16 *>(y_act),

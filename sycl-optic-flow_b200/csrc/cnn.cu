@@ -194,6 +194,11 @@ void conv_backward_data(const ConvDims &d, const float *g, const __nv_bfloat16 *
                                                    accumulate ? 4 : 0);
 }
 
+void conv_bias_grad(const ConvDims &d, const float *g, const __nv_bfloat16 *y_act, float *gb,
+                    cudaStream_t st) {
+    k_bias_grad<<<d.K, 256, 0, st>>>(g, y_act, d.N * d.P * d.Q, d.K, gb);
+}
+
 void conv_backward_weight(const ConvDims &d, const float *g, const __nv_bfloat16 *y_act,
                           const __nv_bfloat16 *x, float *gw, float *gb, cudaStream_t st) {
     const int KD = d.N * d.P * d.Q;

@@ -38,9 +38,32 @@ inline int conv_out(int n, int stride) { return stride == 1 ? n : (n + 1) / 2; }
 void conv_forward(const ConvDims &d, const __nv_bfloat16 *x, const __nv_bfloat16 *w,
                   const float *bias, void *y, bool y_f32, bool relu, cudaStream_t st,
                   int *err = nullptr);
-// the tcgen05 form alone; false (nothing launched) when the shape is outside it
+// the tcgen05 form alone; false (nothing launched) when the shape is outside it.
+// ldy: elements between output rows (0: K); accumulate: y += (f32 output
+// only); bias may be null.  A negative d.stride (-2) reads the input dilated
+// by 2, the gather of a stride-2 layer's backward-data product.
 bool conv_forward_umma(const ConvDims &d, const __nv_bfloat16 *x, const __nv_bfloat16 *w,
-                       const float *bias, void *y, bool y_f32, bool relu, int *err, cudaStream_t st);
+                       const float *bias, void *y, bool y_f32, bool relu, int *err, cudaStream_t st,
+                       int ldy = 0, bool accumulate = false);
+// backward-data on the tcgen05 kernel: the ReLU-masked gradient rounded to
+// bf16 and the rotated, transposed weights go to `scratch`
+// (conv_backward_data_umma_scratch bytes), then the product runs as forward
+// convolutions of at most 128 output channels each.  false (nothing
+// launched) when K or C is not a multiple of 16 or gin is not 16-byte aligned.
+size_t conv_backward_data_umma_scratch(const ConvDims &d);
+// backward-weight on the tcgen05 kernel (transposing gathers, reduction over
+// output pixels split across CTAs, atomics into gw); gw and gb are
+// overwritten.  scratch: the same size as for backward-data.  false (nothing
+// launched) when K > 128, C is not a multiple of 16 or x is not 16-byte aligned.
+bool conv_backward_weight_umma(const ConvDims &d, const float *g, const __nv_bfloat16 *y_act,
+                               const __nv_bfloat16 *x, float *gw, float *gb, void *scratch,
+                               int *err, cudaStream_t st);
+// bias gradient alone: gb[k] = sum over output pixels of the masked gradient
+void conv_bias_grad(const ConvDims &d, const float *g, const __nv_bfloat16 *y_act, float *gb,
+                    cudaStream_t st);
+bool conv_backward_data_umma(const ConvDims &d, const float *g, const __nv_bfloat16 *y_act,
+                             const __nv_bfloat16 *w, float *gin, bool accumulate, void *scratch,
+                             int *err, cudaStream_t st);
 // backward-data: g f32 [N,P,Q,K] (masked by y_act > 0 when y_act != null,
 // y_act bf16 [N,P,Q,K]) -> gin f32 [N,H,W,C]; accumulate adds to gin.
 void conv_backward_data(const ConvDims &d, const float *g, const __nv_bfloat16 *y_act,

@@ -102,7 +102,7 @@ template <int NP, int CK>
 __global__ void __launch_bounds__(kUmNT) k_conv_fwd_umma(ConvDims d, const __nv_bfloat16 *__restrict__ x,
                                                          const __nv_bfloat16 *__restrict__ w,
                                                          const float *__restrict__ bias, void *y,
-                                                         int flags, int *err) {
+                                                         int flags, int ldy, int *err) {
     static_assert(NP % 16 == 0 && NP >= 16 && NP <= 256, "UMMA M=128 needs N = 16..256, step 16");
     static_assert(CK == 16 || CK == 32, "stage depth is 16 or 32 channels");
     constexpr int A_BYTES = kUmBM * CK * 2;
@@ -150,8 +150,21 @@ __global__ void __launch_bounds__(kUmNT) k_conv_fwd_umma(ConvDims d, const __nv_
     auto gather = [&](int s) {
         const int buf = s % kUmStages;
         const int tap = s / nchunk, c0 = (s % nchunk) * CK;
-        const int yy = pp * d.stride + tap / 3 - 1, xx = pq * d.stride + tap % 3 - 1;
-        const bool ok = mval && yy >= 0 && yy < d.H && xx >= 0 && xx < d.W;
+        int yy, xx;
+        bool ok;
+        if (d.stride > 0) {
+            yy = pp * d.stride + tap / 3 - 1;
+            xx = pq * d.stride + tap % 3 - 1;
+            ok = mval && yy >= 0 && yy < d.H && xx >= 0 && xx < d.W;
+        } else {
+            // input dilated by 2 (the backward-data product of a stride-2
+            // layer): output (p, q) reads input ((p + r - 1)/2, (q + s - 1)/2)
+            // where both are whole
+            const int y2 = pp + tap / 3 - 1, x2 = pq + tap % 3 - 1;
+            yy = y2 >> 1;
+            xx = x2 >> 1;
+            ok = mval && ((y2 | x2) & 1) == 0 && y2 >= 0 && x2 >= 0 && yy < d.H && xx < d.W;
+        }
         const __nv_bfloat16 *src = ok ? x + (((size_t)pn * d.H + yy) * d.W + xx) * d.C + c0 : x;
         const uint32_t a = sbase + buf * STAGE;
 #pragma unroll
@@ -215,8 +228,9 @@ __global__ void __launch_bounds__(kUmNT) k_conv_fwd_umma(ConvDims d, const __nv_
     tc_fence_after();
     if (!timed_out) {
         const int mo = m0 + warp * 32 + lane;
-        const bool relu = flags & 1, f32 = flags & 2;
-        const bool vec = d.K % 8 == 0;  // rows of y start on 16-byte boundaries
+        const bool relu = flags & 1, f32 = flags & 2, accum = flags & 4;
+        const int ld = ldy > 0 ? ldy : d.K;  // elements between output rows
+        const bool vec = d.K % 8 == 0 && ld % 8 == 0;  // rows of y start on 16-byte boundaries
 #pragma unroll 1
         for (int c0 = 0; c0 < NP; c0 += 16) {
             uint32_t r[16];
@@ -226,11 +240,17 @@ __global__ void __launch_bounds__(kUmNT) k_conv_fwd_umma(ConvDims d, const __nv_
 #pragma unroll
             for (int j = 0; j < 16; j++) {
                 const int col = c0 + j;
-                float t = __uint_as_float(r[j]) + (col < d.K ? bias[col] : 0.0f);
+                float t = __uint_as_float(r[j]) + ((bias && col < d.K) ? bias[col] : 0.0f);
                 v[j] = relu ? fmaxf(t, 0.0f) : t;
             }
             if (f32) {
-                float *o = static_cast<float *>(y) + (size_t)mo * d.K + c0;
+                float *o = static_cast<float *>(y) + (size_t)mo * ld + c0;
+                if (accum) {  // each output element belongs to one thread
+#pragma unroll
+                    for (int j = 0; j < 16; j++)
+                        if (c0 + j < d.K) o[j] += v[j];
+                    continue;
+                }
 #pragma unroll
                 for (int j = 0; j < 16; j += 4)
                     if (vec && c0 + j + 3 < d.K)
@@ -239,7 +259,7 @@ __global__ void __launch_bounds__(kUmNT) k_conv_fwd_umma(ConvDims d, const __nv_
                         for (int e = 0; e < 4; e++)
                             if (c0 + j + e < d.K) o[j + e] = v[j + e];
             } else {
-                __nv_bfloat16 *o = static_cast<__nv_bfloat16 *>(y) + (size_t)mo * d.K + c0;
+                __nv_bfloat16 *o = static_cast<__nv_bfloat16 *>(y) + (size_t)mo * ld + c0;
 #pragma unroll
                 for (int j = 0; j < 16; j += 8) {
                     if (vec && c0 + j + 7 < d.K) {
@@ -270,40 +290,284 @@ __global__ void __launch_bounds__(kUmNT) k_conv_fwd_umma(ConvDims d, const __nv_
 
 template <int NP, int CK>
 void launch_umma(const ConvDims &d, const __nv_bfloat16 *x, const __nv_bfloat16 *w, const float *bias,
-                 void *y, int flags, int *err, cudaStream_t st) {
+                 void *y, int flags, int ldy, int *err, cudaStream_t st) {
     constexpr int smem = kUmStages * um_stage_bytes<NP, CK>();
     OF_CUDA(cudaFuncSetAttribute(k_conv_fwd_umma<NP, CK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  smem));
     const int M = d.N * d.P * d.Q;
-    k_conv_fwd_umma<NP, CK><<<div_up(M, kUmBM), kUmNT, smem, st>>>(d, x, w, bias, y, flags, err);
+    k_conv_fwd_umma<NP, CK><<<div_up(M, kUmBM), kUmNT, smem, st>>>(d, x, w, bias, y, flags, ldy, err);
 }
 
 template <int CK>
 bool dispatch_np(int np, const ConvDims &d, const __nv_bfloat16 *x, const __nv_bfloat16 *w,
-                 const float *bias, void *y, int flags, int *err, cudaStream_t st) {
+                 const float *bias, void *y, int flags, int ldy, int *err, cudaStream_t st) {
     switch (np) {
-        case 16: launch_umma<16, CK>(d, x, w, bias, y, flags, err, st); return true;
-        case 32: launch_umma<32, CK>(d, x, w, bias, y, flags, err, st); return true;
-        case 48: launch_umma<48, CK>(d, x, w, bias, y, flags, err, st); return true;
-        case 64: launch_umma<64, CK>(d, x, w, bias, y, flags, err, st); return true;
-        case 96: launch_umma<96, CK>(d, x, w, bias, y, flags, err, st); return true;
-        case 128: launch_umma<128, CK>(d, x, w, bias, y, flags, err, st); return true;
+        case 16: launch_umma<16, CK>(d, x, w, bias, y, flags, ldy, err, st); return true;
+        case 32: launch_umma<32, CK>(d, x, w, bias, y, flags, ldy, err, st); return true;
+        case 48: launch_umma<48, CK>(d, x, w, bias, y, flags, ldy, err, st); return true;
+        case 64: launch_umma<64, CK>(d, x, w, bias, y, flags, ldy, err, st); return true;
+        case 96: launch_umma<96, CK>(d, x, w, bias, y, flags, ldy, err, st); return true;
+        case 128: launch_umma<128, CK>(d, x, w, bias, y, flags, ldy, err, st); return true;
         default: return false;
+    }
+}
+
+// Backward-weight product on the tensor cores:
+//   gw[k][tap][c] += sum_m g[m][k] * x[pixel(m, tap)][c]
+// as a GEMM with M = the layer's output channels k (up to 128 rows), N = NP
+// input channels of one tap, and the reduction over output pixels m, 16 per
+// stage (one 128 x NP x 16 MMA).  The operands are gathered transposed into
+// the same no-swizzle K-major layout as the forward kernel: thread t packs
+// row t of A (the masked bf16 gradient of channel k = t at the stage's 16
+// pixels) and row t of B (channel c0 + t of the tap-shifted input at those
+// pixels) into two 16-byte chunks each.  A CTA reduces a range of pixels and
+// adds its 128 x NP tile to gw with atomics (gridDim.y splits the pixels,
+// gridDim.x runs over (tap, channel chunk)).  Same pipeline and bounded
+// waits as the forward kernel.
+template <int NP>
+__global__ void __launch_bounds__(kUmNT) k_conv_wgrad_umma(ConvDims d, const __nv_bfloat16 *__restrict__ gb,
+                                                           const __nv_bfloat16 *__restrict__ x, float *gw,
+                                                           int pix_per_cta, int *err) {
+    static_assert(NP % 16 == 0 && NP >= 16 && NP <= 128, "N = 16..128, step 16");
+    constexpr int A_BYTES = kUmBM * 16 * 2;
+    constexpr int STAGE = (kUmBM + NP) * 16 * 2;
+    constexpr uint32_t TCOLS = tmem_cols<NP>();
+    constexpr uint32_t IDESC = umma_idesc_bf16(kUmBM, NP);
+    extern __shared__ __align__(1024) uint8_t um_smem[];
+    __shared__ __align__(8) uint64_t mbar[kUmStages];
+    __shared__ uint32_t tmem_base;
+    __shared__ long long s_ga[kUmStages][16], s_xa[kUmStages][16];  // element offsets, -1: zero
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int M = d.N * d.P * d.Q;
+    const int nchunk = d.C / NP;
+    const int tap = blockIdx.x / nchunk, c0 = (blockIdx.x % nchunk) * NP;
+    const int m_lo = blockIdx.y * pix_per_cta;
+    const int m_hi = imin(M, m_lo + pix_per_cta);
+    const int nst = m_hi > m_lo ? div_up(m_hi - m_lo, 16) : 0;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                         smem_u32(&tmem_base)),
+                     "r"(TCOLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int i = 0; i < kUmStages; i++) mbar_init(smem_u32(&mbar[i]), 1);
+        fence_mbar_init();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base;
+    const uint32_t sbase = smem_u32(um_smem);
+
+    // offsets of stage s's 16 pixels: gradient row m*K, input pixel of the tap
+    auto offsets = [&](int s) {
+        if (tid < 16) {
+            const int m = m_lo + s * 16 + tid;
+            long long ga = -1, xa = -1;
+            if (m < m_hi) {
+                const int q = m % d.Q, t = m / d.Q, p = t % d.P, n = t / d.P;
+                ga = (long long)m * d.K;
+                const int yy = p * d.stride + tap / 3 - 1, xx = q * d.stride + tap % 3 - 1;
+                if (yy >= 0 && yy < d.H && xx >= 0 && xx < d.W)
+                    xa = (((long long)n * d.H + yy) * d.W + xx) * d.C + c0;
+            }
+            s_ga[s % kUmStages][tid] = ga;
+            s_xa[s % kUmStages][tid] = xa;
+        }
+    };
+    // rows of A (channel k = tid) and B (channel c0 + tid) of stage s,
+    // transposed into 8-element K-major chunks
+    auto gather = [&](int s) {
+        const int buf = s % kUmStages;
+        const uint32_t a = sbase + buf * STAGE, b = a + A_BYTES;
+        const unsigned short *G = reinterpret_cast<const unsigned short *>(gb);
+        const unsigned short *X = reinterpret_cast<const unsigned short *>(x);
+#pragma unroll
+        for (int kc = 0; kc < 2; kc++) {
+            uint32_t pa[4], pb[4];
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                uint32_t va[2], vb[2];
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int j = kc * 8 + e * 2 + h;
+                    const long long ga = s_ga[buf][j], xa = s_xa[buf][j];
+                    va[h] = (ga >= 0 && tid < d.K) ? G[ga + tid] : 0u;
+                    vb[h] = (xa >= 0 && tid < NP) ? X[xa + tid] : 0u;
+                }
+                pa[e] = va[0] | (va[1] << 16);
+                pb[e] = vb[0] | (vb[1] << 16);
+            }
+            asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};\n" ::"r"(a + kc * (kUmBM * 16) + tid * 16),
+                         "r"(pa[0]), "r"(pa[1]), "r"(pa[2]), "r"(pa[3])
+                         : "memory");
+            if (tid < NP)
+                asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};\n" ::"r"(b + kc * (NP * 16) + tid * 16),
+                             "r"(pb[0]), "r"(pb[1]), "r"(pb[2]), "r"(pb[3])
+                             : "memory");
+        }
+    };
+
+    bool timed_out = false;
+#pragma unroll 1
+    for (int s = 0; s < nst; s++) {
+        // buffer s % 4 last held stage s - 4: its MMA must be done
+        if (s >= kUmStages && !timed_out) {
+            const int so = s - kUmStages;
+            if (!mbar_wait_bounded(smem_u32(&mbar[so % kUmStages]), (so / kUmStages) & 1))
+                timed_out = true;
+        }
+        offsets(s);
+        __syncthreads();
+        gather(s);
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const int buf = s % kUmStages;
+            const uint32_t a = sbase + buf * STAGE, b = a + A_BYTES;
+            const uint64_t ad = umma_desc(a, kUmBM * 16, 128);
+            const uint64_t bd = umma_desc(b, NP * 16, 128);
+            umma_bf16(tmem, ad, bd, IDESC, s > 0 ? 1u : 0u);
+            umma_commit(smem_u32(&mbar[buf]));
+        }
+    }
+    if (nst > 0) {
+        const int sL = nst - 1;
+        if (!timed_out && !mbar_wait_bounded(smem_u32(&mbar[sL % kUmStages]), (sL / kUmStages) & 1))
+            timed_out = true;
+    }
+    timed_out = __syncthreads_or(timed_out);
+    if (timed_out && tid == 0) atomicOr(err, 1);
+    tc_fence_after();
+    if (!timed_out && nst > 0) {
+        const int k = warp * 32 + lane;  // TMEM lane = output channel
+#pragma unroll 1
+        for (int cc = 0; cc < NP; cc += 16) {
+            uint32_t r[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cc, r);
+            if (k >= d.K) continue;
+            float *o = gw + ((size_t)k * 9 + tap) * d.C + c0 + cc;
+#pragma unroll
+            for (int j = 0; j < 16; j++) atomicAdd(o + j, __uint_as_float(r[j]));
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS)
+                     : "memory");
+}
+
+template <int NP>
+void launch_wgrad(const ConvDims &d, const __nv_bfloat16 *gb, const __nv_bfloat16 *x, float *gw,
+                  int *err, cudaStream_t st) {
+    constexpr int smem = kUmStages * (kUmBM + NP) * 16 * 2;
+    OF_CUDA(cudaFuncSetAttribute(k_conv_wgrad_umma<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    const int M = d.N * d.P * d.Q;
+    const int nx = 9 * (d.C / NP);
+    // enough CTAs to fill the GPU a few times over, at least 256 pixels each
+    const int splits = imax(1, imin(div_up(M, 256), div_up(4 * kNumSMs * 8, nx)));
+    const int per = div_up(div_up(M, splits), 16) * 16;
+    k_conv_wgrad_umma<NP><<<dim3(nx, div_up(M, per)), kUmNT, smem, st>>>(d, gb, x, gw, per, err);
+}
+
+// bf16 copy of the output gradient, zero where the layer's ReLU was inactive
+// (the same masking and rounding the mma.sync backward applies on its gather)
+__global__ void k_mask_bf16(const float *__restrict__ g, const __nv_bfloat16 *__restrict__ yact,
+                            __nv_bfloat16 *out, size_t n) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        float v = g[i];
+        if (yact && !(__bfloat162float(yact[i]) > 0.0f)) v = 0.0f;
+        out[i] = __float2bfloat16(v);
+    }
+}
+
+// wt[c][tap][k] = w[k][8 - tap][c]: the weights of the backward-data product
+// seen as a forward convolution (rotated taps, input and output channels
+// exchanged)
+__global__ void k_flip_weights(const __nv_bfloat16 *__restrict__ w, int K, int C,
+                               __nv_bfloat16 *wt) {
+    const int n = K * 9 * C;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int k = i % K, tap = (i / K) % 9, c = i / (9 * K);
+        wt[i] = w[((size_t)k * 9 + (8 - tap)) * C + c];
     }
 }
 
 }  // namespace
 
 bool conv_forward_umma(const ConvDims &d, const __nv_bfloat16 *x, const __nv_bfloat16 *w,
-                       const float *bias, void *y, bool y_f32, bool relu, int *err, cudaStream_t st) {
+                       const float *bias, void *y, bool y_f32, bool relu, int *err, cudaStream_t st,
+                       int ldy, bool accumulate) {
     if (d.C % 16 != 0 || d.K > 128 || d.K < 1) return false;
+    if (accumulate && !y_f32) return false;
     // 16-byte cp.async sources and vector stores
     const auto a16 = [](const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
     if (!a16(x) || !a16(w) || !a16(y)) return false;
     const int np = (d.K + 15) / 16 * 16;
-    const int flags = (relu ? 1 : 0) | (y_f32 ? 2 : 0);
-    if (d.C % 32 == 0) return dispatch_np<32>(np, d, x, w, bias, y, flags, err, st);
-    return dispatch_np<16>(np, d, x, w, bias, y, flags, err, st);
+    const int flags = (relu ? 1 : 0) | (y_f32 ? 2 : 0) | (accumulate ? 4 : 0);
+    if (d.C % 32 == 0) return dispatch_np<32>(np, d, x, w, bias, y, flags, ldy, err, st);
+    return dispatch_np<16>(np, d, x, w, bias, y, flags, ldy, err, st);
+}
+
+bool conv_backward_weight_umma(const ConvDims &d, const float *g, const __nv_bfloat16 *y_act,
+                               const __nv_bfloat16 *x, float *gw, float *gb, void *scratch,
+                               int *err, cudaStream_t st) {
+    if (d.K > 128 || d.C % 16 != 0) return false;
+    int np = 0;  // the widest channel chunk that divides C
+    for (int c : {128, 96, 64, 48, 32, 16})
+        if (d.C % c == 0) {
+            np = c;
+            break;
+        }
+    if (!np || (reinterpret_cast<uintptr_t>(x) & 15u) != 0) return false;
+    const size_t ng = (size_t)d.N * d.P * d.Q * d.K;
+    __nv_bfloat16 *gbf = static_cast<__nv_bfloat16 *>(scratch);
+    k_mask_bf16<<<imin((int)((ng + 255) / 256), 4096), 256, 0, st>>>(g, y_act, gbf, ng);
+    OF_CUDA(cudaMemsetAsync(gw, 0, sizeof(float) * (size_t)d.K * 9 * d.C, st));
+    switch (np) {
+        case 128: launch_wgrad<128>(d, gbf, x, gw, err, st); break;
+        case 96: launch_wgrad<96>(d, gbf, x, gw, err, st); break;
+        case 64: launch_wgrad<64>(d, gbf, x, gw, err, st); break;
+        case 48: launch_wgrad<48>(d, gbf, x, gw, err, st); break;
+        case 32: launch_wgrad<32>(d, gbf, x, gw, err, st); break;
+        default: launch_wgrad<16>(d, gbf, x, gw, err, st); break;
+    }
+    conv_bias_grad(d, g, y_act, gb, st);
+    return true;
+}
+
+size_t conv_backward_data_umma_scratch(const ConvDims &d) {
+    const size_t g = (size_t)d.N * d.P * d.Q * d.K, wt = (size_t)d.K * 9 * d.C;
+    return (g + wt + 64) * sizeof(__nv_bfloat16);
+}
+
+bool conv_backward_data_umma(const ConvDims &d, const float *g, const __nv_bfloat16 *y_act,
+                             const __nv_bfloat16 *w, float *gin, bool accumulate, void *scratch,
+                             int *err, cudaStream_t st) {
+    if (d.K % 16 != 0 || d.C % 16 != 0) return false;
+    if ((reinterpret_cast<uintptr_t>(gin) & 15u) != 0) return false;
+    const size_t ng = (size_t)d.N * d.P * d.Q * d.K;
+    __nv_bfloat16 *gb = static_cast<__nv_bfloat16 *>(scratch);
+    __nv_bfloat16 *wt = gb + (ng + 63) / 64 * 64;  // 128-byte aligned
+    k_mask_bf16<<<imin((int)((ng + 255) / 256), 4096), 256, 0, st>>>(g, y_act, gb, ng);
+    k_flip_weights<<<imin(div_up(d.K * 9 * d.C, 256), 1024), 256, 0, st>>>(w, d.K, d.C, wt);
+    // the product as a forward convolution over the output gradient: input
+    // (N, P, Q, K), output (N, H, W, C); stride 2 layers read a dilated input
+    ConvDims t{d.N, d.P, d.Q, d.K, d.H, d.W, 0, d.stride == 1 ? 1 : -2};
+    for (int c0 = 0; c0 < d.C; c0 += 128) {  // at most 128 output channels a launch
+        t.K = imin(128, d.C - c0);
+        if (!conv_forward_umma(t, gb, wt + (size_t)c0 * 9 * d.K, nullptr, gin + c0, true, false, err,
+                               st, d.C, accumulate))
+            return false;
+    }
+    return true;
 }
 
 }  // namespace oflow

@@ -19,6 +19,9 @@
 #include "internal.hpp"
 #include "warmnet.hpp"
 
+#include <algorithm>
+#include <cstdlib>
+
 namespace oflow {
 
 namespace {
@@ -75,7 +78,11 @@ WarmNet::WarmNet(int w, int h, int B) : w_(w), h_(h), B_(B) {
     o_v_ = ar_.reserve(np_ * 4);
     o_loss_ = ar_.reserve(8);
     o_err_ = ar_.reserve(sizeof(int));
+    size_t bwd = 0;  // scratch of the tensor-core backward products
+    for (int l = 0; l < 10; l++) bwd = std::max(bwd, conv_backward_data_umma_scratch(dims(l)));
+    o_bwd_ = ar_.reserve(bwd);
     ar_.commit();
+    if (const char *e = getenv("OFLOW_CNN_BWD_MMA")) bwd_mma_ = atoi(e) != 0;
     OF_CUDA(cudaMemset(ar_.at<char>(o_err_), 0, sizeof(int)));
     OF_CUDA(cudaMemset(ar_.at<char>(o_m_), 0, np_ * 4));
     OF_CUDA(cudaMemset(ar_.at<char>(o_v_), 0, np_ * 4));
@@ -142,8 +149,14 @@ double WarmNet::train_step(const void *frames, int dtype, size_t pair_stride, co
     auto back = [&](int l, const float *g, int yact_t, int x_t, float *gin, bool acc) {
         const ConvDims d = dims(l);
         const __nv_bfloat16 *yact = yact_t >= 0 ? A(yact_t) : nullptr;
-        conv_backward_weight(d, g, yact, A(x_t), gp + woff_[l], gp + boff_[l], st);
-        if (gin) conv_backward_data(d, g, yact, W + woff_[l], gin, acc, st);
+        // both backward products on the tensor-core kernels where the shape
+        // allows (OFLOW_CNN_BWD_MMA=1 keeps them on the mma.sync kernel, to compare)
+        if (bwd_mma_ || !conv_backward_weight_umma(d, g, yact, A(x_t), gp + woff_[l], gp + boff_[l],
+                                                   ar_.at<char>(o_bwd_), ar_.at<int>(o_err_), st))
+            conv_backward_weight(d, g, yact, A(x_t), gp + woff_[l], gp + boff_[l], st);
+        if (gin && (bwd_mma_ || !conv_backward_data_umma(d, g, yact, W + woff_[l], gin, acc,
+                                                          ar_.at<char>(o_bwd_), ar_.at<int>(o_err_), st)))
+            conv_backward_data(d, g, yact, W + woff_[l], gin, acc, st);
     };
     back(9, ar_.at<float>(o_gout_), -1, 11, G(11), false);  // c10: -> g(c9)
     back(8, G(11), 11, 10, G(10), false);                   // c9 : -> g(cat2)

@@ -44,7 +44,8 @@ class WarmNet {
     Arena ar_;
     size_t aoff_[12] = {}, goff_[12] = {}, gsize_[12] = {};
     size_t o_out_ = 0, o_gout_ = 0, o_p_ = 0, o_pb_ = 0, o_gp_ = 0, o_m_ = 0, o_v_ = 0,
-           o_loss_ = 0, o_err_ = 0;
+           o_loss_ = 0, o_err_ = 0, o_bwd_ = 0;
+    bool bwd_mma_ = false;  // backward products on the mma.sync kernel only
     int step_ = 0;
 };
 

@@ -25,9 +25,9 @@ def _rel(a, b):
                                                    (2, 13, 17, 224, 96, 1, True), (1, 11, 9, 96, 128, 2, True),
                                                    (3, 20, 30, 16, 32, 2, True)])
 def test_conv_products_match_cpu_oracle(of, N, H, W, C, K, stride, relu):
-    """Forward on both tensor-core kernels (mode 0: tcgen05 with the
-    accumulator in tensor memory; mode 3: mma.sync), backward-data and
-    backward-weight, against the float64 oracle."""
+    """Forward, backward-data and backward-weight on both tensor-core kernels
+    (tcgen05 with the accumulator in tensor memory, and mma.sync), against
+    the float64 oracle."""
     import torch
     from oracle import cnn_ref
     g = torch.Generator().manual_seed(N * 1000 + C + K)
@@ -54,10 +54,19 @@ def test_conv_products_match_cpu_oracle(of, N, H, W, C, K, stride, relu):
     gx_ref, gw_ref, gb_ref = cnn_ref.backward(x.float().numpy(), w.float().numpy(), gout_b.numpy(),
                                               stride, yb.float().cpu().numpy() if relu else None)
     gx = torch.empty((N, H, W, C), dtype=torch.float32, device="cuda")
-    of.conv3x3(1, N, H, W, C, K, stride, relu, True, gout.cuda(), yact, wd, gx)
+    if K % 16 == 0:  # mode 1: tcgen05, the backward-data product as a forward convolution
+        of.conv3x3(1, N, H, W, C, K, stride, relu, True, gout.cuda(), yact, wd, gx)
+        assert _rel(gx.cpu().numpy(), gx_ref) < REL
+        gx.fill_(float("nan"))
+    of.conv3x3(4, N, H, W, C, K, stride, relu, True, gout.cuda(), yact, wd, gx)  # mma.sync
     gw = torch.empty((K, 3, 3, C), dtype=torch.float32, device="cuda")
     gb = torch.empty(K, dtype=torch.float32, device="cuda")
+    # mode 2: tcgen05 (transposing gathers, pixels split across CTAs); mode 5: mma.sync
     of.conv3x3(2, N, H, W, C, K, stride, relu, True, gout.cuda(), yact, xd, gw, gbias=gb)
+    torch.cuda.synchronize()
+    assert _rel(gw.cpu().numpy(), gw_ref) < REL
+    gw.fill_(float("nan"))
+    of.conv3x3(5, N, H, W, C, K, stride, relu, True, gout.cuda(), yact, xd, gw, gbias=gb)
     torch.cuda.synchronize()
     assert _rel(gx.cpu().numpy(), gx_ref) < REL
     assert _rel(gw.cpu().numpy(), gw_ref) < REL
