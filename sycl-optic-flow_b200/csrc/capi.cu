@@ -60,12 +60,14 @@ void unstage_plane(const float *src, int w, int h, float *dst, int pitch, int lo
                               s));
 }
 
-// Stages a pair into the plan's own buffers and points its frame table there.
+// Stages a pair into the plan's own buffers and points its frame table there;
+// its flow goes to the plan's own output buffer (the caller reads it there).
 void stage_pair_raw(TvPlan &pl, int b, const oflow_image &I0, const oflow_image &I1, cudaStream_t s) {
     stage_image(I0, pl.raw_input(b, 0), dtype_size(I0.dtype), s);
     stage_image(I1, pl.raw_input(b, 1), dtype_size(I1.dtype), s);
     pl.bind_raw(b, 0);
     pl.bind_raw(b, 1);
+    pl.bind_own_out(b);
 }
 
 }  // namespace oflow
@@ -287,14 +289,22 @@ void run_tvl1(oflow_ctx *ctx, int n, const oflow_image *I0, const oflow_image *I
                     pl.bind_raw(b - b0, k);
                 }
             }
+            // device flows are written in place by the schedule's last kernel
+            const oflow_flow &o = out[g.idx[b]];
+            if (o.location == OFLOW_DEVICE)
+                pl.bind_out(b - b0, o.u, o.v, o.pitch);
+            else
+                pl.bind_own_out(b - b0);
         }
     };
     auto collect = [&](TvPlan &pl, const Group &g, int b0, int b1, cudaStream_t s) {
         for (int b = b0; b < b1; b++) {
             const oflow_flow &o = out[g.idx[b]];
-            unstage_plane(pl.out_u(b - b0), g.w, g.h, o.u, o.pitch, o.location, s);
-            unstage_plane(pl.out_v(b - b0), g.w, g.h, o.v, o.pitch, o.location, s);
-            if (o.location == OFLOW_HOST) device_only = false;
+            if (o.location == OFLOW_HOST) {
+                unstage_plane(pl.out_u(b - b0), g.w, g.h, o.u, o.pitch, o.location, s);
+                unstage_plane(pl.out_v(b - b0), g.w, g.h, o.v, o.pitch, o.location, s);
+                device_only = false;
+            }
             if (stats) pl.read_stats(b - b0, &stats[g.idx[b]], s);
         }
     };
@@ -583,28 +593,44 @@ oflow_status oflow_batch(oflow_ctx *ctx, int n, const oflow_job *jobs) {
         }
         const cudaStream_t st = ctx->stream();
         const size_t G = mb->kind.size();
-        auto stage = [&](size_t g, cudaStream_t s) {
+        // device frames and flows in place through the plans' tables; host
+        // ones through the plans' own buffers
+        auto bind_group = [&](auto &pl, size_t g, cudaStream_t s) {
             for (size_t b = 0; b < mb->members[g].size(); b++) {
                 const oflow_job &j = jobs[mb->members[g][b]];
-                void *d0 = mb->kind[g] == OFLOW_SOLVER_TVL1 ? mb->tv[mb->slot[g]]->raw_input((int)b, 0)
-                                                            : mb->hs[mb->slot[g]]->raw_input((int)b, 0);
-                void *d1 = mb->kind[g] == OFLOW_SOLVER_TVL1 ? mb->tv[mb->slot[g]]->raw_input((int)b, 1)
-                                                            : mb->hs[mb->slot[g]]->raw_input((int)b, 1);
-                stage_image(j.I0, d0, dtype_size(j.I0.dtype), s);
-                stage_image(j.I1, d1, dtype_size(j.I1.dtype), s);
+                const oflow_image *im[2] = {&j.I0, &j.I1};
+                for (int k = 0; k < 2; k++) {
+                    if (im[k]->location == OFLOW_DEVICE) {
+                        pl.bind_frame((int)b, k, im[k]->data, im[k]->pitch ? im[k]->pitch : im[k]->width);
+                    } else {
+                        stage_image(*im[k], pl.raw_input((int)b, k), dtype_size(im[k]->dtype), s);
+                        pl.bind_raw((int)b, k);
+                    }
+                }
+                if (j.out.location == OFLOW_DEVICE)
+                    pl.bind_out((int)b, j.out.u, j.out.v, j.out.pitch);
+                else
+                    pl.bind_own_out((int)b);
             }
+        };
+        auto stage = [&](size_t g, cudaStream_t s) {
+            if (mb->kind[g] == OFLOW_SOLVER_TVL1)
+                bind_group(*mb->tv[mb->slot[g]], g, s);
+            else
+                bind_group(*mb->hs[mb->slot[g]], g, s);
         };
         bool device_only = true;
         auto unstage = [&](size_t g, cudaStream_t s) {
             for (size_t b = 0; b < mb->members[g].size(); b++) {
                 const oflow_job &j = jobs[mb->members[g][b]];
+                if (j.out.location != OFLOW_HOST) continue;  // written in place
                 const float *ou = mb->kind[g] == OFLOW_SOLVER_TVL1 ? mb->tv[mb->slot[g]]->out_u((int)b)
                                                                    : mb->hs[mb->slot[g]]->out_u((int)b);
                 const float *ov = mb->kind[g] == OFLOW_SOLVER_TVL1 ? mb->tv[mb->slot[g]]->out_v((int)b)
                                                                    : mb->hs[mb->slot[g]]->out_v((int)b);
                 unstage_plane(ou, j.I0.width, j.I0.height, j.out.u, j.out.pitch, j.out.location, s);
                 unstage_plane(ov, j.I0.width, j.I0.height, j.out.v, j.out.pitch, j.out.location, s);
-                if (j.out.location == OFLOW_HOST) device_only = false;
+                device_only = false;
             }
         };
         bool host_io = false;
@@ -631,7 +657,13 @@ oflow_status oflow_batch(oflow_ctx *ctx, int n, const oflow_job *jobs) {
         } else {
             // device buffers: copies on the context stream, then all groups as
             // the branches of one graph
-            for (size_t g = 0; g < G; g++) stage(g, st);
+            for (size_t g = 0; g < G; g++) {
+                stage(g, st);
+                if (mb->kind[g] == OFLOW_SOLVER_TVL1)
+                    mb->tv[mb->slot[g]]->upload_frames(st);
+                else
+                    mb->hs[mb->slot[g]]->upload_io(st);
+            }
             if (!mb->graph.ready()) {
                 mb->graph.capture(st, [&](cudaStream_t s) {
                     cudaEvent_t fork = mb->events.back();
@@ -964,6 +996,7 @@ oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_
         }
         OF_CHECK(wp->level_w(3) == net->net->out_w() && wp->level_h(3) == net->net->out_h(),
                  "tvl1 warm: scale 3 does not match the network output");
+        // the judge reads both solves' flows from the plans' own buffers
         for (int b = 0; b < n; b++) stage_pair_raw(*wp, b, I0[b], I1[b], st);
         net->net->forward(wp->raw_input(0, 0), g.dtype, wp->plane_stride(), st);
         net->net->flow_to(wp->uz(), wp->plane_stride(), nullptr, st);

@@ -23,6 +23,9 @@ class HsPlan {
     // plan's output buffer (out_u / out_v).
     void bind_out(int b, float *u, float *v, int pitch);
     void bind_own_out(int b);
+    // the frame and output tables to the device (run() does it; a caller that
+    // records the schedule into its own graph does it before each launch)
+    void upload_io(cudaStream_t st) { io_.upload(st); }
     void run(cudaStream_t st);
     void record(cudaStream_t st);
     // Times every Jacobi configuration (tile shape, sweeps per launch) at every

@@ -12,13 +12,6 @@
 
 namespace oflow {
 
-// Output planes of one pair: u and v, row pitch in elements.
-struct OutRef {
-    float *u;
-    float *v;
-    long long pitch;
-};
-
 class PairIo {
   public:
     // dev_frames: 2*B entries (pair b, frame k at 2b+k); dev_outs: B entries

@@ -734,6 +734,10 @@ struct TbArgs {
     // bounded wait gives up
     int use_tma;
     int *err;
+    // queue form only: size a pair's block of iterations to end where the
+    // error's geometric decay predicts its stop (the launch form's fixed
+    // schedule needs full blocks)
+    int predict;
     CUtensorMap tmP;  // p: (2 nx, ny, pair, buffer) 8-byte elements
     CUtensorMap tmU;  // u: (nx, ny, pair, buffer) 8-byte elements
     CUtensorMap tmW;  // (I1wx, I1wy, rho_c, grad): (2 nx, ny, pair) 8-byte elements
@@ -943,10 +947,17 @@ __device__ __forceinline__ TbStart tb_start(const TbArgs &a, const TvCtrl *ctrl)
     t.snaps = false;
     if (t.redo == 0) {
         const float q = fminf(__ldcg(&ctrl->decay), 1.0f);
+        const float le = __ldcg(&ctrl->last_err);
         float qk = 1.0f;
 #pragma unroll
         for (int j = 1; j < K; j++) qk *= q;
-        t.snaps = __ldcg(&ctrl->last_err) * qk < kSnapMargin * a.eps2;
+        t.snaps = le * qk < kSnapMargin * a.eps2;
+        if (a.predict && q > 0.0f && q < 1.0f && le > a.eps2 && le < INFINITY) {
+            // iterations until le * q^n <= eps2; the same inputs give every
+            // tile of the pair the same count
+            const float n = ceilf(logf(a.eps2 / le) / logf(q));
+            if (n >= 1.0f && n < (float)t.kk) t.kk = (int)n;
+        }
     }
     return t;
 }
@@ -1489,15 +1500,18 @@ __global__ void __launch_bounds__(kEnNT) k_energy_true(const float *__restrict__
 }
 
 // ---------------------------------------------------------------- output
-__global__ void k_split(const float2 *U0, const float2 *U1, size_t stride, int N, float *ou,
-                        float *ov, const TvCtrl *ctrl) {
-    const int b = blockIdx.y;
-    const float2 *U = state_buf(U0, U1, ctrl[b].cur) + (size_t)b * stride;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-        const float2 u = U[i];
-        ou[(size_t)b * stride + i] = u.x;
-        ov[(size_t)b * stride + i] = u.y;
-    }
+// The accepted flow of pair b (blockIdx.z) into its output planes: the
+// plan's own buffer or the caller's device planes (any row pitch).
+__global__ void k_split(const float2 *U0, const float2 *U1, size_t stride, int w, int h,
+                        const OutRef *__restrict__ outs, const TvCtrl *ctrl) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const int b = blockIdx.z;
+    const float2 u = (state_buf(U0, U1, ctrl[b].cur) + (size_t)b * stride)[(size_t)y * w + x];
+    const OutRef o = outs[b];
+    o.u[(size_t)y * o.pitch + x] = u.x;
+    o.v[(size_t)y * o.pitch + x] = u.y;
 }
 
 // ================================================================ launchers
@@ -1631,8 +1645,10 @@ static void tb_launch_q(dim3 g, cudaStream_t st, const TbArgs &ta, TbQueue *q, i
 }
 
 // A whole tiled warp stage as one persistent launch (k_tvl1_q).
-static void tb_launch_queue(int cfg, dim3 g, cudaStream_t st, const TbArgs &ta, TbQueue *q,
-                            int *left) {
+static void tb_launch_queue(int cfg, dim3 g, cudaStream_t st, const TbArgs &ta_in, TbQueue *q,
+                            int *left, bool predict) {
+    TbArgs ta = ta_in;
+    ta.predict = predict ? 1 : 0;
     switch (cfg) {
         case 0: tb_launch_q<64, 32, 512>(g, st, ta, q, left); break;
         case 1: tb_launch_q<64, 16, 256>(g, st, ta, q, left); break;
@@ -1760,11 +1776,17 @@ TvPlan::TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, boo
     o_frames_ = ar_.reserve(sizeof(FrameRef) * 2 * B);
     o_queue_ = ar_.reserve(sizeof(TbQueue) * B);
     o_left_ = ar_.reserve(sizeof(int));
+    o_otab_ = ar_.reserve(sizeof(OutRef) * B);
     ar_.commit();
     frames_.resize(2 * (size_t)B);
-    for (int b = 0; b < B; b++)
+    outs_.resize((size_t)B);
+    for (int b = 0; b < B; b++) {
         for (int k = 0; k < 2; k++) bind_raw(b, k);
+        bind_own_out(b);
+    }
     OF_CUDA(cudaMemcpy(ar_.at<FrameRef>(o_frames_), frames_.data(), sizeof(FrameRef) * frames_.size(),
+                       cudaMemcpyHostToDevice));
+    OF_CUDA(cudaMemcpy(ar_.at<OutRef>(o_otab_), outs_.data(), sizeof(OutRef) * outs_.size(),
                        cudaMemcpyHostToDevice));
     OF_CUDA(cudaMemset(ar_.at<char>(o_ctrl_), 0, B * sizeof(TvCtrl)));
     OF_CUDA(cudaMemset(ar_.at<char>(o_queue_), 0, B * sizeof(TbQueue)));
@@ -1772,6 +1794,9 @@ TvPlan::TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, boo
     // iterations (k_tvl1_tb) instead of the persistent work queue (k_tvl1_q)
     if (const char *e = getenv("OFLOW_TB_QUEUE")) queue_off_env_ = atoi(e) == 0;
     queue_ = !queue_off_env_;
+    // OFLOW_TB_PREDICT=1: the queue form sizes each block of iterations to end
+    // at the predicted stop
+    if (const char *e = getenv("OFLOW_TB_PREDICT")) predict_ = atoi(e) != 0;
     // scales above a warm start's first scale never record a count
     OF_CUDA(cudaMemset(ar_.at<char>(o_iters_), 0, (size_t)B * iter_stride_ * 4));
     tb_set_smem_attrs();
@@ -1781,9 +1806,16 @@ void TvPlan::bind_frame(int b, int k, const void *p, int pitch) {
     frames_[2 * (size_t)b + k] = FrameRef{p, pitch};
 }
 void TvPlan::bind_raw(int b, int k) { frames_[2 * (size_t)b + k] = FrameRef{raw_input(b, k), w_}; }
+void TvPlan::bind_out(int b, float *u, float *v, int pitch) { outs_[b] = OutRef{u, v, pitch ? pitch : w_}; }
+void TvPlan::bind_own_out(int b) {
+    float *o = ar_.at<float>(o_out_);
+    outs_[b] = OutRef{o + (size_t)b * N0_, o + (size_t)(B_ + b) * N0_, w_};
+}
 void TvPlan::upload_frames(cudaStream_t st) {
-    // pageable source: the runtime copies it out before returning
+    // pageable sources: the runtime copies them out before returning
     OF_CUDA(cudaMemcpyAsync(ar_.at<FrameRef>(o_frames_), frames_.data(), sizeof(FrameRef) * frames_.size(),
+                            cudaMemcpyHostToDevice, st));
+    OF_CUDA(cudaMemcpyAsync(ar_.at<OutRef>(o_otab_), outs_.data(), sizeof(OutRef) * outs_.size(),
                             cudaMemcpyHostToDevice, st));
 }
 void TvPlan::run_eager(cudaStream_t st) {
@@ -1913,7 +1945,7 @@ void TvPlan::record(cudaStream_t st) {
                     if (cfg == kLevelCfg || cfg == kClusterCfg)
                         tb_launch_cfg(cfg, tg, st, ta);
                     else
-                        tb_launch_queue(cfg, tg, st, ta, queue, left);
+                        tb_launch_queue(cfg, tg, st, ta, queue, left, predict_);
                     launches_ += 1;
                 } else {
                     // blocked schedule: ceil(max/K) launches plus one for a
@@ -1944,8 +1976,8 @@ void TvPlan::record(cudaStream_t st) {
     k_energy<<<dim3(energy_blocks_, B), kEnNT, 0, st>>>(WR, U0, U1, N0, w_, h_, prm_.lambda,
                                                         ctrl, part, max_blocks_, energy,
                                                         energy_slots_, trace_ ? -1 : 0, -1);
-    k_split<<<dim3(imin(div_up((int)N0, 256 * 4), 1024), B), 256, 0, st>>>(
-        U0, U1, N0, (int)N0, ar_.at<float>(o_out_), ar_.at<float>(o_out_) + (size_t)B * N0, ctrl);
+    k_split<<<dim3(div_up(w_, 32), div_up(h_, 8), B), dim3(32, 8), 0, st>>>(
+        U0, U1, N0, w_, h_, ar_.at<OutRef>(o_otab_), ctrl);
     launches_ += 2;
     OF_CUDA(cudaGetLastError());
 }

@@ -59,6 +59,13 @@ struct FrameRef {
     long long pitch;
 };
 
+// Where a plan writes one pair's flow: u and v planes, row pitch in elements.
+struct OutRef {
+    float *u;
+    float *v;
+    long long pitch;
+};
+
 class TvPlan {
   public:
     // start_scale >= 0: warm start -- the solve begins at that scale from the
@@ -102,6 +109,11 @@ class TvPlan {
     // run_eager() and profile().
     void bind_frame(int b, int k, const void *p, int pitch);
     void bind_raw(int b, int k);
+    // Flow of pair b: the caller's device planes (written in place by the
+    // schedule's last kernel; pitch in elements, 0 = width) or this plan's
+    // output buffer (out_u / out_v).  Plans start with their own buffers.
+    void bind_out(int b, float *u, float *v, int pitch);
+    void bind_own_out(int b);
     const float *out_u(int b) const;
     const float *out_v(int b) const;
     const int *iters_dev() const;
@@ -170,9 +182,15 @@ class TvPlan {
     std::vector<FrameRef> frames_;  // [B][2], host copy of the device table
     HostFlag err_;
     size_t o_frames_ = 0;
-    size_t o_queue_ = 0, o_left_ = 0;
+    size_t o_queue_ = 0, o_left_ = 0, o_otab_ = 0;
+    std::vector<OutRef> outs_;  // [B], host copy of the device output table
     bool queue_ = true;  // tiled stages as one persistent launch each
     bool queue_off_env_ = false;
+    bool predict_ = false;  // queue form: blocks of iterations end at the predicted stop
+
+  public:
+    // the frame and output tables to the device (run() does it; a caller that
+    // records the schedule into its own graph does it before each launch)
     void upload_frames(cudaStream_t st);
 };
 

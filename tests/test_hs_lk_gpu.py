@@ -160,12 +160,13 @@ def test_pyrlk_batch_matches_single_pairs(of, orc, ctx):
         assert _same(u, ou) and _same(v, ov)
 
 
-@pytest.mark.parametrize("solver", ["hs", "pyrlk"])
+@pytest.mark.parametrize("solver", ["hs", "pyrlk", "tvl1", "mixed"])
 def test_device_frames_and_flows_in_place(of, ctx, solver):
     """Batches of device frames (uint8 with a row pitch, and float) and device
     flows with a row pitch: read and written in place through the plans'
-    frame and output tables, bit-identical to the same pairs from host
-    memory; padding of the pitched output rows is left untouched."""
+    frame and output tables (HS, pyramidal LK, TV-L1, and a mixed batch of
+    HS and TV-L1 jobs), bit-identical to the same pairs from host memory;
+    padding of the pitched output rows is left untouched."""
     import torch
     from oflow import synth
     w, h = 97, 61
@@ -181,14 +182,25 @@ def test_device_frames_and_flows_in_place(of, ctx, solver):
         pitched.append((pa[:, :w], pb[:, :w]))
     outs = [(torch.full((h, w + 5), 7.0, device=dev)[:, :w],
              torch.full((h, w + 5), 7.0, device=dev)[:, :w]) for _ in gen]
+    run = None
     if solver == "hs":
         prm = of.HSParams(2.0, 2, 2, 30)
-        ref = of.hs_batch(host, prm, ctx)
-        res = of.hs_batch(pitched, prm, ctx, out=outs)
-    else:
+        run = lambda pairs, out=None: of.hs_batch(pairs, prm, ctx, out=out)
+    elif solver == "pyrlk":
         prm = of.LKParams(3, 2, 5, 2, 2)
-        ref = of.pyrlk_batch(host, prm, ctx)
-        res = of.pyrlk_batch(pitched, prm, ctx, out=outs)
+        run = lambda pairs, out=None: of.pyrlk_batch(pairs, prm, ctx, out=out)
+    elif solver == "tvl1":
+        prm = of.TVL1Params(nscales=3, max_iterations=10)
+        run = lambda pairs, out=None: of.tvl1_batch(pairs, prm, ctx, out=out)
+    else:
+        tp, hp = of.TVL1Params(nscales=3, max_iterations=10), of.HSParams(2.0, 1, 1, 20)
+
+        def run(pairs, out=None):
+            jobs = [("tvl1" if i % 2 == 0 else "hs", a, b, tp if i % 2 == 0 else hp)
+                    for i, (a, b) in enumerate(pairs)]
+            return of.batch(jobs, ctx, out=out)
+    ref = run(host)
+    res = run(pitched, outs)
     torch.cuda.synchronize()
     for (ru, rv), (u, v) in zip(ref, res):
         assert np.array_equal(u.cpu().numpy(), ru) and np.array_equal(v.cpu().numpy(), rv)
@@ -198,7 +210,7 @@ def test_device_frames_and_flows_in_place(of, ctx, solver):
     # float frames on the device, contiguous flows
     fl = [(torch.from_numpy(a.astype(np.float32)).to(dev),
            torch.from_numpy(b.astype(np.float32)).to(dev)) for a, b in host]
-    res2 = of.hs_batch(fl, prm, ctx) if solver == "hs" else of.pyrlk_batch(fl, prm, ctx)
+    res2 = run(fl)
     for (ru, rv), (u, v) in zip(ref, res2):
         assert np.array_equal(u.cpu().numpy(), ru) and np.array_equal(v.cpu().numpy(), rv)
 

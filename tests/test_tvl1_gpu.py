@@ -241,12 +241,14 @@ def test_repeated_full_size_solves_match_the_oracle(of, orc, monkeypatch, cfg):
         assert np.array_equal(u, ou) and np.array_equal(v, ov)
 
 
-@pytest.mark.parametrize("env", [{"OFLOW_TB_QUEUE": "0"}, {"OFLOW_TB_QUEUE": "1"}])
+@pytest.mark.parametrize("env", [{"OFLOW_TB_QUEUE": "0"}, {"OFLOW_TB_QUEUE": "1"},
+                                 {"OFLOW_TB_QUEUE": "1", "OFLOW_TB_PREDICT": "1"}])
 @pytest.mark.parametrize("w,h,ns", [(1024, 436, 5), (131, 77, 4), (333, 201, 5)])
 def test_alternative_kernel_forms_match_the_oracle(of, orc, monkeypatch, env, w, h, ns):
-    """The tiled stages as one launch per block of iterations (k_tvl1_tb)
-    and as one persistent work-queue launch per stage (k_tvl1_q): the same
-    bits as the oracle.  Odd widths take the plain region loads."""
+    """The tiled stages as one launch per block of iterations (k_tvl1_tb),
+    as one persistent work-queue launch per stage (k_tvl1_q), and with the
+    queue's blocks of iterations sized to the predicted stop: the same bits
+    as the oracle.  Odd widths take the plain region loads."""
     for k, v in env.items():
         monkeypatch.setenv(k, v)
     _, a, b = _pair(w + h, w, h, radius=min(w, h) / 5.0)
