@@ -178,16 +178,22 @@ void make_side_streams(oflow_ctx *ctx) {
 
 // The plan of chunk slot c for this size and batch (chunks run at once, so
 // each slot has plans of its own).
-TvPlan &side_plan(oflow_ctx *ctx, int c, int w, int h, int B, int dtype, const oflow_tvl1_params &p) {
+TvPlan &side_plan(oflow_ctx *ctx, int c, int chunks, int w, int h, int B, int dtype,
+                  const oflow_tvl1_params &p) {
     auto &v = ctx->tv_side[c];
     for (auto &pl : v)
         if (pl->width() == w && pl->height() == h && pl->batch() == B && pl->dtype() == dtype &&
-            same(pl->params(), p))
+            same(pl->params(), p)) {
+            pl->set_share(chunks);
             return *pl;
+        }
     v.emplace_back(new TvPlan(w, h, B, dtype, p, false, &ctx->tune));
-    // chunks share the GPU: launches per block of iterations interleave with
-    // the other chunks' kernels, where persistent blocks would hold the SMs
-    v.back()->use_queue(false);
+    // chunks share the GPU: each chunk's persistent launches take a share of
+    // the resident slots (OFLOW_SIDE_QUEUE=0: one launch per block of
+    // iterations instead, interleaving with the other chunks' kernels)
+    const char *e = getenv("OFLOW_SIDE_QUEUE");
+    v.back()->use_queue(!(e && atoi(e) == 0));
+    v.back()->set_share(chunks);
     if (v.size() > kMaxPlans) ctx->last_tv.clear();  // an evicted plan may be listed
     keep_recent(v);
     return *v.back();
@@ -324,7 +330,7 @@ void run_tvl1(oflow_ctx *ctx, int n, const oflow_image *I0, const oflow_image *I
             for (int c = 0; c < chunks; c++) {
                 const int b0 = c * ng / chunks, b1 = (c + 1) * ng / chunks;
                 const cudaStream_t sc = ctx->side[c];
-                TvPlan &pl = side_plan(ctx, c, g.w, g.h, b1 - b0, g.dtype, *p);
+                TvPlan &pl = side_plan(ctx, c, chunks, g.w, g.h, b1 - b0, g.dtype, *p);
                 ctx->last_tv.push_back(&pl);
                 pl.check_device_error();  // a failure of an earlier, unsynchronised call
                 OF_CUDA(cudaStreamWaitEvent(sc, ctx->fork, 0));

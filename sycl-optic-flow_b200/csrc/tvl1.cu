@@ -956,7 +956,13 @@ __device__ __forceinline__ TbStart tb_start(const TbArgs &a, const TvCtrl *ctrl)
             // iterations until le * q^n <= eps2; the same inputs give every
             // tile of the pair the same count
             const float n = ceilf(logf(a.eps2 / le) / logf(q));
-            if (n >= 1.0f && n < (float)t.kk) t.kk = (int)n;
+            if (n >= 1.0f && n < (float)t.kk) {
+                t.kk = (int)n;
+                // predict 2: trust the prediction, no snapshots (an earlier
+                // stop re-runs its iterations); measured 1,234 against 1,225
+                // pairs/s with snapshots, 1,176 with full blocks
+                if (a.predict == 2) t.snaps = false;
+            }
         }
     }
     return t;
@@ -1637,23 +1643,27 @@ static int tb_queue_occupancy() {
 }
 
 template <int TW, int TH, int NT>
-static void tb_launch_q(dim3 g, cudaStream_t st, const TbArgs &ta, TbQueue *q, int *left) {
+static void tb_launch_q(dim3 g, cudaStream_t st, const TbArgs &ta, TbQueue *q, int *left,
+                        int share) {
     const int ntiles = (int)(g.x * g.y);
-    const int blocks = imin(ntiles * (int)g.z, tb_queue_occupancy<TW, TH, NT>() * kNumSMs);
+    const int slots = imax(1, tb_queue_occupancy<TW, TH, NT>() * kNumSMs / imax(share, 1));
+    const int blocks = imin(ntiles * (int)g.z, slots);
     k_tvl1_q<TW, TH, kTbK, NT><<<blocks, NT, tb_smem_bytes(TW, TH), st>>>(ta, q, left, (int)g.x,
                                                                          ntiles, (int)g.z);
 }
 
 // A whole tiled warp stage as one persistent launch (k_tvl1_q).
+// share > 1: the plan runs beside share - 1 others of its kind (the chunks of
+// a host batch) and takes that fraction of the resident slots.
 static void tb_launch_queue(int cfg, dim3 g, cudaStream_t st, const TbArgs &ta_in, TbQueue *q,
-                            int *left, bool predict) {
+                            int *left, int predict, int share) {
     TbArgs ta = ta_in;
-    ta.predict = predict ? 1 : 0;
+    ta.predict = predict;
     switch (cfg) {
-        case 0: tb_launch_q<64, 32, 512>(g, st, ta, q, left); break;
-        case 1: tb_launch_q<64, 16, 256>(g, st, ta, q, left); break;
-        case 2: tb_launch_q<32, 16, 256>(g, st, ta, q, left); break;
-        default: tb_launch_q<16, 8, 128>(g, st, ta, q, left); break;
+        case 0: tb_launch_q<64, 32, 512>(g, st, ta, q, left, share); break;
+        case 1: tb_launch_q<64, 16, 256>(g, st, ta, q, left, share); break;
+        case 2: tb_launch_q<32, 16, 256>(g, st, ta, q, left, share); break;
+        default: tb_launch_q<16, 8, 128>(g, st, ta, q, left, share); break;
     }
 }
 
@@ -1794,9 +1804,11 @@ TvPlan::TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, boo
     // iterations (k_tvl1_tb) instead of the persistent work queue (k_tvl1_q)
     if (const char *e = getenv("OFLOW_TB_QUEUE")) queue_off_env_ = atoi(e) == 0;
     queue_ = !queue_off_env_;
-    // OFLOW_TB_PREDICT=1: the queue form sizes each block of iterations to end
-    // at the predicted stop
-    if (const char *e = getenv("OFLOW_TB_PREDICT")) predict_ = atoi(e) != 0;
+    // The queue form sizes each block of iterations to end at the stop its
+    // error decay predicts and drops the snapshots of a shortened block (2,
+    // the default; 1: keeps them; 0: full blocks)
+    predict_ = 2;
+    if (const char *e = getenv("OFLOW_TB_PREDICT")) predict_ = atoi(e);
     // scales above a warm start's first scale never record a count
     OF_CUDA(cudaMemset(ar_.at<char>(o_iters_), 0, (size_t)B * iter_stride_ * 4));
     tb_set_smem_attrs();
@@ -1945,7 +1957,7 @@ void TvPlan::record(cudaStream_t st) {
                     if (cfg == kLevelCfg || cfg == kClusterCfg)
                         tb_launch_cfg(cfg, tg, st, ta);
                     else
-                        tb_launch_queue(cfg, tg, st, ta, queue, left, predict_);
+                        tb_launch_queue(cfg, tg, st, ta, queue, left, predict_, share_);
                     launches_ += 1;
                 } else {
                     // blocked schedule: ceil(max/K) launches plus one for a

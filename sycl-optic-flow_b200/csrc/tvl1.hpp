@@ -100,6 +100,13 @@ class TvPlan {
         if (on != queue_) graph_.reset();
         queue_ = on && !queue_off_env_;
     }
+    // The plan runs beside parts - 1 others of its kind on the GPU (the
+    // chunks of a host batch): its persistent launches take that fraction of
+    // the resident slots.
+    void set_share(int parts) {
+        if (parts != share_) graph_.reset();
+        share_ = parts < 1 ? 1 : parts;
+    }
     // Device destination of input frame k (0: I0, 1: I1) of pair b: a dense
     // w*h plane of the plan's dtype.
     void *raw_input(int b, int k) const;
@@ -186,7 +193,8 @@ class TvPlan {
     std::vector<OutRef> outs_;  // [B], host copy of the device output table
     bool queue_ = true;  // tiled stages as one persistent launch each
     bool queue_off_env_ = false;
-    bool predict_ = false;  // queue form: blocks of iterations end at the predicted stop
+    int predict_ = 2;  // queue form: blocks of iterations end at the predicted stop
+    int share_ = 1;    // fraction (1/share_) of the resident slots a queue launch takes
 
   public:
     // the frame and output tables to the device (run() does it; a caller that
