@@ -174,12 +174,12 @@ def test_host_batch_in_chunks_matches_device_batch(of, ctx):
         assert all(s["energy"] > 0 for s in st_h)
 
 
-@pytest.mark.parametrize("side_queue", ["1", "0"])
+@pytest.mark.parametrize("side_queue", ["0", "1", "4"])
 def test_host_chunks_of_tiled_levels_match_device_batch(of, monkeypatch, side_queue):
     """Host frames and flows of tiled levels (256x128): the chunks on side
-    streams run the work queue on a share of the SMs (or, with
-    OFLOW_SIDE_QUEUE=0, one launch per block of iterations); the flows equal
-    the device batch solved as one plan."""
+    streams run one launch per block of iterations (the default), or the
+    work queue on all or a quarter of the resident slots (OFLOW_SIDE_QUEUE);
+    the flows equal the device batch solved as one plan."""
     import torch
     monkeypatch.setenv("OFLOW_SIDE_QUEUE", side_queue)
     c = of.Context(0)
