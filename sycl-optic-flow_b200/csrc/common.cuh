@@ -45,8 +45,17 @@ __device__ __forceinline__ int clamp_flag(int x, int n, bool &out) {
 // Keys cubic (a = -1/2) through v0..v3 at offset x from v1, with single
 // precision differences and double precision for the rest, as in
 // src/tvl1/sequential/bicubic_interpolation/bicubic_interpolation.cpp:38-46.
-__device__ __forceinline__ float cubic_cell(float v0, float v1, float v2, float v3, float x) {
-    const double xd = x;
+// The cell splits into the part that depends on the four samples only
+// (cubic_coef: the cubic and quadratic coefficients in double, the single
+// precision difference v2 - v0, and v1) and the evaluation at x
+// (cubic_eval); cubic_cell is the two in sequence, with the operations and
+// roundings of the reference's one expression.
+struct CubicCoef {
+    double c3, c2;
+    float d20, v1;
+};
+
+__device__ __forceinline__ CubicCoef cubic_coef(float v0, float v1, float v2, float v3) {
     const float d20 = v2 - v0;
     const float d12 = v1 - v2;
     double c3 = 3.0 * (double)d12;
@@ -56,10 +65,22 @@ __device__ __forceinline__ float cubic_cell(float v0, float v1, float v2, float 
     c2 = c2 - 5.0 * (double)v1;
     c2 = c2 + 4.0 * (double)v2;
     c2 = c2 - (double)v3;
+    return CubicCoef{c3, c2, d20, v1};
+}
+
+// xd = (double)x, hx = 0.5 * xd (exact), shared by the cells of one sample.
+__device__ __forceinline__ float cubic_eval(double c3, double c2, float d20, float v1, double xd,
+                                            double hx) {
     c2 = c2 + xd * c3;
     const double t = (double)d20 + xd * c2;
-    const double r = (double)v1 + (0.5 * xd) * t;
+    const double r = (double)v1 + hx * t;
     return (float)r;
+}
+
+__device__ __forceinline__ float cubic_cell(float v0, float v1, float v2, float v3, float x) {
+    const double xd = x;
+    const CubicCoef k = cubic_coef(v0, v1, v2, v3);
+    return cubic_eval(k.c3, k.c2, k.d20, k.v1, xd, 0.5 * xd);
 }
 
 // Stencil of the reference's bicubic sample (bicubic_interpolation.cpp:74-128):

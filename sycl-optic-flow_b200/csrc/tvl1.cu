@@ -8,7 +8,8 @@
 //   raw[b][2]      staged input frames (u8 or f32)
 //   T[b][2]        float scratch planes (ingest output, blur output)
 //   pyr_s[b][2]    pyramid level s of I0 / I1, dense nx_s*ny_s
-//   I1g[b]         float4 (I1, I1x, I1y, 0) of the current level
+//   cc*[b], dv*[b] column coefficients of the warp's bicubic samples of
+//                  (I1, I1x, I1y) at the current level (WarpCoef, 72 B/px)
 //   WR[b]          float4 (I1wx, I1wy, rho_c, |grad I1w|^2) of the current warp
 //   U[k][b]        float2 (u1, u2), k = 0..7; Uz[b] upsampled flow
 //   P[k][b]        float4 (p11, p12, p21, p22), k = 0..7
@@ -425,21 +426,45 @@ __global__ void k_zoom_flow(const float2 *U0, const float2 *U1, size_t stride, i
 }
 
 // ---------------------------------------------------------------- gradient
-// Centered gradient of I1 (mask.cpp:139-196) packed with I1 itself so a warp
-// sample reads all three channels with one 16-byte load per tap.
-__global__ void k_grad_pack(const float *__restrict__ pyr, size_t pyr_stride, int nx, int ny,
-                            float4 *I1g, size_t stride) {
+// Centered gradient of I1 (mask.cpp:139-196) at (x, y), packed with I1
+// itself: (I1, I1x, I1y).
+__device__ __forceinline__ float3 grad_at(const float *__restrict__ I, int x, int y, int nx, int ny) {
+    const size_t row = (size_t)y * nx;
+    const float ddx = __ldg(I + row + imin(x + 1, nx - 1)) - __ldg(I + row + imax(x - 1, 0));
+    const float ddy = __ldg(I + (size_t)imin(y + 1, ny - 1) * nx + x) -
+                      __ldg(I + (size_t)imax(y - 1, 0) * nx + x);
+    return make_float3(__ldg(I + row + x), (float)(0.5 * (double)ddx), (float)(0.5 * (double)ddy));
+}
+
+// Column coefficients of the warp's bicubic samples, once per scale.  A
+// sample that is not zeroed at the border has rows y-1..y+2 and columns
+// x-1..x+2 of its base texel (x, y) (bicubic_stencil: a negative coordinate
+// always reaches outside, so both steps are +1), and its first pass evaluates
+// the column cubic of rows y-1..y+2 at ty for each of the four columns.  The
+// part of that cubic that does not depend on ty (cubic_coef) is computed here
+// for every texel (x, y) and each of I1, I1x, I1y; the warp then evaluates it
+// (cubic_eval) with the same operations in the same order.  Rows outside
+// [1, ny-3] are never read by a sample; they hold the coefficients of the
+// clamped rows.
+__global__ void k_cubic_pack(const float *__restrict__ pyr, size_t pyr_stride, int nx, int ny,
+                             WarpCoef wc, size_t stride) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int b = blockIdx.z;
     if (x >= nx || y >= ny) return;
     const float *I = pyr + (size_t)(2 * b + 1) * pyr_stride;
-    const size_t row = (size_t)y * nx;
-    const float ddx = __ldg(I + row + imin(x + 1, nx - 1)) - __ldg(I + row + imax(x - 1, 0));
-    const float ddy = __ldg(I + (size_t)imin(y + 1, ny - 1) * nx + x) -
-                      __ldg(I + (size_t)imax(y - 1, 0) * nx + x);
-    I1g[(size_t)b * stride + row + x] =
-        make_float4(__ldg(I + row + x), (float)(0.5 * (double)ddx), (float)(0.5 * (double)ddy), 0.0f);
+    float3 g[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) g[r] = grad_at(I, x, imin(imax(y - 1 + r, 0), ny - 1), nx, ny);
+    const CubicCoef k0 = cubic_coef(g[0].x, g[1].x, g[2].x, g[3].x);
+    const CubicCoef k1 = cubic_coef(g[0].y, g[1].y, g[2].y, g[3].y);
+    const CubicCoef k2 = cubic_coef(g[0].z, g[1].z, g[2].z, g[3].z);
+    const size_t q = (size_t)b * stride + (size_t)y * nx + x;
+    wc.cc0[q] = make_double2(k0.c3, k0.c2);
+    wc.cc1[q] = make_double2(k1.c3, k1.c2);
+    wc.cc2[q] = make_double2(k2.c3, k2.c2);
+    wc.dv01[q] = make_float4(k0.d20, k0.v1, k1.d20, k1.v1);
+    wc.dv2[q] = make_float2(k2.d20, k2.v1);
 }
 
 // ---------------------------------------------------------------- warping
@@ -450,14 +475,15 @@ __global__ void k_grad_pack(const float *__restrict__ pyr, size_t pyr_stride, in
 // With first_warp, p is zeroed (tvl1.cpp:190-193).
 enum { kWarpFromU = 0, kWarpFromUz = 1, kWarpZero = 2 };
 
-// 6 blocks of 256 per SM (40 registers, a few spilled): the 16-tap gathers
-// need the warps to hide their latency.  The 25 warps of the 1024x436 workload
-// took 3.74 ms at 3 blocks (66 registers), 3.14 at 5, 3.05 at 6, 3.75 at 8.
-// A form that staged each block's samples in shared memory as doubles (one
-// conversion per sample and block instead of per pixel) measured slower,
-// 4.35 against 3.80 ms: 64 registers and 46 KB of shared memory left 4 blocks
-// per SM, and the region load before the block barrier stalled.
-__global__ void __launch_bounds__(256, 6) k_warp(const float *__restrict__ pyr, size_t pyr_stride, const float4 *I1g,
+// The first pass of each sample reads the column coefficients of its four
+// columns (k_cubic_pack) and evaluates them at ty; only the second pass runs
+// the whole cell.  6 blocks of 256 per SM: the gathers need the warps to hide
+// their latency.  Splitting the channels over three threads per pixel (all
+// eight gathers of a channel in flight, the samples combined in shared
+// memory) measured slower: 4.10 against 2.48 ms for the 25 warps of the
+// 1024x436 workload at 32 pairs.
+constexpr int kWarpTW = 32, kWarpTH = 8;
+__global__ void __launch_bounds__(kWarpTW * kWarpTH, 6) k_warp(const float *__restrict__ pyr, size_t pyr_stride, WarpCoef wc,
                        float4 *WR, float2 *U0, float2 *U1, const float2 *Uz, float4 *P0,
                        float4 *P1, size_t stride, int nx, int ny, int mode, int first_warp,
                        TvCtrl *ctrl, TbQueue *q, int *left) {
@@ -493,18 +519,19 @@ __global__ void __launch_bounds__(256, 6) k_warp(const float *__restrict__ pyr, 
     float Iw = 0.0f, Iwx = 0.0f, Iwy = 0.0f;
     BicubicStencil s;
     if (bicubic_stencil(uu, vv, nx, ny, true, s)) {
-        const float4 *G = I1g + off;
+        // base texel (col[1], row[1]); columns col[1]-1 .. col[1]+2
+        const size_t q0 = off + (size_t)nx * s.row[1] + s.col[0];
+        const double ty = s.ty, hy = 0.5 * ty;
         float a[4], bx[4], by[4];
 #pragma unroll
         for (int c = 0; c < 4; c++) {
-            const float4 *col = G + s.col[c];
-            const float4 t0 = __ldg(col + (size_t)nx * s.row[0]);
-            const float4 t1 = __ldg(col + (size_t)nx * s.row[1]);
-            const float4 t2 = __ldg(col + (size_t)nx * s.row[2]);
-            const float4 t3 = __ldg(col + (size_t)nx * s.row[3]);
-            a[c] = cubic_cell(t0.x, t1.x, t2.x, t3.x, s.ty);
-            bx[c] = cubic_cell(t0.y, t1.y, t2.y, t3.y, s.ty);
-            by[c] = cubic_cell(t0.z, t1.z, t2.z, t3.z, s.ty);
+            const size_t q = q0 + c;
+            const double2 k0 = __ldg(wc.cc0 + q), k1 = __ldg(wc.cc1 + q), k2 = __ldg(wc.cc2 + q);
+            const float4 d01 = __ldg(wc.dv01 + q);
+            const float2 d2 = __ldg(wc.dv2 + q);
+            a[c] = cubic_eval(k0.x, k0.y, d01.x, d01.y, ty, hy);
+            bx[c] = cubic_eval(k1.x, k1.y, d01.z, d01.w, ty, hy);
+            by[c] = cubic_eval(k2.x, k2.y, d2.x, d2.y, ty, hy);
         }
         Iw = cubic_cell(a[0], a[1], a[2], a[3], s.tx);
         Iwx = cubic_cell(bx[0], bx[1], bx[2], bx[3], s.tx);
@@ -1768,7 +1795,7 @@ TvPlan::TvPlan(int w, int h, int B, int dtype, const oflow_tvl1_params &prm, boo
     o_raw_ = ar_.reserve(2 * B * N0 * esz);
     o_T_ = ar_.reserve(2 * B * N0 * 4);
     o_pyr_ = ar_.reserve(pyr_total * 4);
-    o_I1g_ = ar_.reserve(B * N0 * 16);
+    o_cc_ = ar_.reserve(B * N0 * 72);  // WarpCoef: 3 x double2, float4, float2 per texel
     o_WR_ = ar_.reserve(B * N0 * 16);
     o_U0_ = ar_.reserve(kStateBufs * B * N0 * 8);  // buffer k at U0 + k*B*N0
     o_Uz_ = ar_.reserve(B * N0 * 8);
@@ -1854,7 +1881,15 @@ void TvPlan::record(cudaStream_t st) {
     const size_t N0 = N0_;
     float *T = ar_.at<float>(o_T_);
     float *pyr = ar_.at<float>(o_pyr_);
-    float4 *I1g = ar_.at<float4>(o_I1g_);
+    WarpCoef wc;
+    {
+        const size_t n = (size_t)B * N0;
+        wc.cc0 = ar_.at<double2>(o_cc_);
+        wc.cc1 = wc.cc0 + n;
+        wc.cc2 = wc.cc1 + n;
+        wc.dv01 = reinterpret_cast<float4 *>(wc.cc2 + n);
+        wc.dv2 = reinterpret_cast<float2 *>(wc.dv01 + n);
+    }
     float4 *WR = ar_.at<float4>(o_WR_);
     float2 *U0 = ubuf(0), *U1 = ubuf(1), *Uz = ar_.at<float2>(o_Uz_);
     float4 *P0 = pbuf(0), *P1 = pbuf(1);
@@ -1930,17 +1965,18 @@ void TvPlan::record(cudaStream_t st) {
                                             (float)ny / cy, inv, ctrl);
             launches_ += 1;
         }
-        k_grad_pack<<<gr, blk, 0, st>>>(pyr + pyr_off_[s], lp, nx, ny, I1g, N0);
+        k_cubic_pack<<<gr, blk, 0, st>>>(pyr + pyr_off_[s], lp, nx, ny, wc, N0);
         launches_ += 1;
         IterArgs ia{WR, U0, U1, P0, P1, N0, nx, ny, l_t, prm_.theta, taut, eps2, ctrl, part,
                     max_blocks_, iters, iter_stride_, 0};
         dim3 ig(div_up(nx, kIterTW), div_up(ny, kIterTH), B);
         const int cfg = tb_cfg_[s];
+        const dim3 wb(kWarpTW, kWarpTH), wg(div_up(nx, kWarpTW), div_up(ny, kWarpTH), B);
         for (int wi = 0; wi < sw_[s]; wi++) {
             const int mode = wi > 0 ? kWarpFromU
                                     : (s == s0_ ? (warm_ ? kWarpFromUz : kWarpZero) : kWarpFromUz);
             mark_begin(-1);
-            k_warp<<<gr, blk, 0, st>>>(pyr + pyr_off_[s], lp, I1g, WR, U0, U1, Uz, P0, P1,
+            k_warp<<<wg, wb, 0, st>>>(pyr + pyr_off_[s], lp, wc, WR, U0, U1, Uz, P0, P1,
                                        N0, nx, ny, mode, wi == 0, ctrl, queue, left);
             mark_end();
             launches_ += 1;

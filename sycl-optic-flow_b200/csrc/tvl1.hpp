@@ -52,6 +52,15 @@ int launch_zoom_out(const float *src, size_t sstride, int nx, int ny, float *T, 
 bool encode_map8(CUtensorMap *m, void *base, int rank, const cuuint64_t *dims,
                  const cuuint64_t *strides, const cuuint32_t *box);
 
+// Column coefficients of the warp's bicubic samples at one level, per texel
+// of every pair: (c3, c2) of I1, I1x and I1y in double, and (v2 - v0, v1) of
+// each in single precision (I1 and I1x in dv01, I1y in dv2).
+struct WarpCoef {
+    double2 *cc0, *cc1, *cc2;
+    float4 *dv01;
+    float2 *dv2;
+};
+
 // Where a plan reads one input frame: a device pointer of the plan's dtype and
 // its row pitch in elements.
 struct FrameRef {
@@ -180,7 +189,7 @@ class TvPlan {
     size_t o_tarr_ = 0, o_tout_ = 0;
     int sw_[OFLOW_MAX_SCALES] = {}, si_[OFLOW_MAX_SCALES] = {};  // warps, iterations per scale
     size_t o_WR_ = 0;
-    size_t o_raw_ = 0, o_T_ = 0, o_pyr_ = 0, o_I1g_ = 0, o_U0_ = 0, o_Uz_ = 0, o_P0_ = 0,
+    size_t o_raw_ = 0, o_T_ = 0, o_pyr_ = 0, o_cc_ = 0, o_U0_ = 0, o_Uz_ = 0, o_P0_ = 0,
            o_out_ = 0, o_ctrl_ = 0, o_part_ = 0, o_recs_ = 0, o_iters_ = 0, o_energy_ = 0;
     float2 *ubuf(int k) const;  // state buffer k of u (all pairs)
     float4 *pbuf(int k) const;  // state buffer k of p
