@@ -79,7 +79,7 @@ constexpr size_t tb_smem_bytes(int tw, int th) { return (size_t)(tw + 2 * kTbK) 
 // for 512 threads, 85 for fewer), matching what their shared memory allows
 // (64x32: 2, 64x16: 3; the smaller tiles are not limited by it).
 constexpr int tb_min_blocks(int nt) { return nt >= 512 ? 2 : nt >= 256 ? 3 : 6; }
-constexpr int kGaussTW = 32, kGaussTH = 16, kGaussNT = 256, kGaussMaxR = 15;
+constexpr int kGaussTW = 64, kGaussTH = 32, kGaussNT = 256, kGaussMaxR = 15;
 constexpr int kIngestNT = 256, kIngestPPT = 8;
 
 // Half-kernel of mask.cpp:225-244 in double on the host.
@@ -182,21 +182,27 @@ template <typename In>
 __global__ void __launch_bounds__(kIngestNT) k_ingest(const FrameRef *__restrict__ frames, int w,
                                                       int h, NormRec *recs, int nblk) {
     const int b = blockIdx.y;
-    const int N = w * h;
     __shared__ NormRec sh[4][kIngestNT / 32];
     NormRec r[4];
     r[0] = {-1.0f, INT_MAX, 0.0f, 0}; r[1] = {INFINITY, INT_MAX, 0.0f, 0};
     r[2] = r[0]; r[3] = r[1];
+    // rows blockIdx.x, +nblk, ...: each thread visits its pixels in increasing
+    // index order, so a tie keeps the earlier pixel by the strict comparison
     for (int k = 0; k < 2; k++) {
         const FrameRef f = frames[2 * b + k];
         const In *src = static_cast<const In *>(f.p);
-        for (int i = blockIdx.x * kIngestNT + threadIdx.x; i < N; i += nblk * kIngestNT) {
-            const int y = i / w, xx = i - y * w;
-            const float x = (float)src[(size_t)y * f.pitch + xx];
-            const NormRec c{fabsf(x), i, x, 0};
-            if (better_max(c, r[2 * k])) r[2 * k] = c;
-            if (better_min(c, r[2 * k + 1])) r[2 * k + 1] = c;
+        NormRec mx = r[2 * k], mn = r[2 * k + 1];
+        for (int y = blockIdx.x; y < h; y += nblk) {
+            const In *row = src + (size_t)y * f.pitch;
+            for (int xx = threadIdx.x; xx < w; xx += kIngestNT) {
+                const float x = (float)__ldg(row + xx);
+                const float ax = fabsf(x);
+                if (ax > mx.a) mx = NormRec{ax, y * w + xx, x, 0};
+                if (ax < mn.a) mn = NormRec{ax, y * w + xx, x, 0};
+            }
         }
+        r[2 * k] = mx;
+        r[2 * k + 1] = mn;
     }
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
@@ -222,20 +228,30 @@ __global__ void __launch_bounds__(kIngestNT) k_ingest(const FrameRef *__restrict
     }
 }
 
-// One block per pair: joint range of both frames (std::max / std::min of the
-// per-frame |x| extrema, tvl1.cpp:316-321).
-__global__ void k_norm_finalize(const NormRec *recs, int nblk, TvCtrl *ctrl) {
+// One block of 4 warps per pair, warp q reducing quantity q of the per-block
+// records: joint range of both frames (std::max / std::min of the per-frame
+// |x| extrema, tvl1.cpp:316-321).  (|x|, index) orders the records totally,
+// so the result does not depend on the reduction's order.
+constexpr int kNormNT = 128;
+__global__ void __launch_bounds__(kNormNT) k_norm_finalize(const NormRec *recs, int nblk, TvCtrl *ctrl) {
     const int b = blockIdx.x;
+    const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
     __shared__ NormRec sh[4];
-    if (threadIdx.x < 4) {
-        const int q = threadIdx.x;
-        NormRec best = recs[((size_t)b * nblk) * 4 + q];
-        for (int i = 1; i < nblk; i++) {
-            const NormRec c = recs[((size_t)b * nblk + i) * 4 + q];
-            if ((q & 1) ? better_min(c, best) : better_max(c, best)) best = c;
-        }
-        sh[q] = best;
+    NormRec best = q & 1 ? NormRec{INFINITY, INT_MAX, 0.0f, 0} : NormRec{-1.0f, INT_MAX, 0.0f, 0};
+    for (int i = lane; i < nblk; i += 32) {
+        const NormRec c = recs[((size_t)b * nblk + i) * 4 + q];
+        if ((q & 1) ? better_min(c, best) : better_max(c, best)) best = c;
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        NormRec c;
+        c.a = __shfl_down_sync(0xffffffffu, best.a, o);
+        c.idx = __shfl_down_sync(0xffffffffu, best.idx, o);
+        c.val = __shfl_down_sync(0xffffffffu, best.val, o);
+        c.pad = 0;
+        if ((q & 1) ? better_min(c, best) : better_max(c, best)) best = c;
+    }
+    if (lane == 0) sh[q] = best;
     __syncthreads();
     if (threadIdx.x == 0) {
         const float a0 = sh[0].val, a1 = sh[2].val, b0 = sh[1].val, b1 = sh[3].val;
@@ -264,18 +280,45 @@ __device__ __forceinline__ int gauss_mirror(int x, int n) {
     return x;
 }
 
+// Row then column pass of the separable Gaussian over one tile, both with the
+// reference's pairing (input[i-j] + input[i+j] in single precision) and double
+// taps and sums (mask.cpp:246-286).  RT > 0: the radius at compile time
+// (loops unrolled, taps from the parameter bank); RT = 0: taps.size - 1.
+template <int RT>
+__device__ __forceinline__ double gauss_sum(const float *c, int step, const GaussTaps &taps, int R) {
+    double sum = taps.B[0] * (double)c[0];
+    if (RT > 0) {
+#pragma unroll
+        for (int j = 1; j <= RT; j++) {
+            const float pair = c[-j * step] + c[j * step];
+            sum += taps.B[j] * (double)pair;
+        }
+    } else {
+        for (int j = 1; j <= R; j++) {
+            const float pair = c[-j * step] + c[j * step];
+            sum += taps.B[j] * (double)pair;
+        }
+    }
+    return sum;
+}
+
 // SRC 0: float planes at src; 1 / 2: uint8 / float frames through the frame
-// table (plane z = frame z of the table), converted to float on load.
-template <int SRC>
+// table (plane z = frame z of the table), converted to float on load.  A
+// uint8 frame is normalised through a 256-entry table of the same expression.
+// Tile kGaussTW x kGaussTH outputs, 256 threads as 32 x 8.
+template <int SRC, int RT>
 __global__ void __launch_bounds__(kGaussNT) k_gauss(const float *__restrict__ src, float *dst,
                                                     int nx, int ny, size_t plane_stride,
                                                     GaussTaps taps, const TvCtrl *ctrl,
                                                     int normalize, const FrameRef *frames) {
-    constexpr int LW = kGaussTW + 2 * kGaussMaxR;
-    __shared__ float sIn[(kGaussTH + 2 * kGaussMaxR) * LW];
-    __shared__ float sRow[(kGaussTH + 2 * kGaussMaxR) * kGaussTW];
-    const int R = taps.size - 1;
+    constexpr int MR = RT > 0 ? RT : kGaussMaxR;
+    constexpr int LW = kGaussTW + 2 * MR, LH = kGaussTH + 2 * MR;
+    __shared__ float sIn[LH * LW];
+    __shared__ float sRow[LH * kGaussTW];
+    __shared__ float sLut[SRC == 1 ? 256 : 1];
+    const int R = RT > 0 ? RT : taps.size - 1;
     const int z = blockIdx.z;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const float *in = src + (size_t)z * plane_stride;
     float *out = dst + (size_t)z * plane_stride;
     const int x0 = blockIdx.x * kGaussTW, y0 = blockIdx.y * kGaussTH;
@@ -287,47 +330,47 @@ __global__ void __launch_bounds__(kGaussNT) k_gauss(const float *__restrict__ sr
         mn = c.norm_min;
         den = c.norm_den;
     }
+    FrameRef f{};
+    if (SRC != 0) f = frames[z];
+    if (SRC == 1) {
+        const float v = (float)threadIdx.x;
+        sLut[threadIdx.x] = apply ? (float)(255.0 * (double)(v - mn) / (double)den) : v;
+        __syncthreads();
+    }
     const int lw = kGaussTW + 2 * R, lh = kGaussTH + 2 * R;
-    for (int i = threadIdx.x; i < lw * lh; i += kGaussNT) {
-        const int ly = i / lw, lx = i % lw;
-        const int my = gauss_mirror(y0 - R + ly, ny), mx = gauss_mirror(x0 - R + lx, nx);
-        float v = 0.0f;
-        if (mx >= 0 && mx < nx && my >= 0 && my < ny) {
-            if (SRC == 0) {
-                v = __ldg(in + (size_t)my * nx + mx);
-            } else {
-                const FrameRef f = frames[z];
-                const size_t q = (size_t)my * f.pitch + mx;
-                v = SRC == 1 ? (float)__ldg(static_cast<const uint8_t *>(f.p) + q)
-                             : __ldg(static_cast<const float *>(f.p) + q);
+    for (int ly = ty; ly < lh; ly += kGaussNT / 32) {
+        const int my = gauss_mirror(y0 - R + ly, ny);
+        const bool row_ok = my >= 0 && my < ny;
+        for (int lx = tx; lx < lw; lx += 32) {
+            const int mx = gauss_mirror(x0 - R + lx, nx);
+            float v = 0.0f;
+            if (row_ok && mx >= 0 && mx < nx) {
+                if (SRC == 0) {
+                    v = __ldg(in + (size_t)my * nx + mx);
+                } else if (SRC == 1) {
+                    v = sLut[__ldg(static_cast<const uint8_t *>(f.p) + (size_t)my * f.pitch + mx)];
+                } else {
+                    v = __ldg(static_cast<const float *>(f.p) + (size_t)my * f.pitch + mx);
+                    if (apply) v = (float)(255.0 * (double)(v - mn) / (double)den);
+                }
             }
-            if (apply) v = (float)(255.0 * (double)(v - mn) / (double)den);
+            sIn[ly * LW + lx] = v;
         }
-        sIn[ly * LW + lx] = v;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < kGaussTW * lh; i += kGaussNT) {
-        const int ly = i / kGaussTW, cx = i % kGaussTW;
-        const float *row = sIn + ly * LW + cx + R;
-        double sum = taps.B[0] * (double)row[0];
-        for (int j = 1; j <= R; j++) {
-            const float pair = row[-j] + row[j];
-            sum += taps.B[j] * (double)pair;
-        }
-        sRow[ly * kGaussTW + cx] = (float)sum;
-    }
+    for (int ly = ty; ly < lh; ly += kGaussNT / 32)
+        for (int cx = tx; cx < kGaussTW; cx += 32)
+            sRow[ly * kGaussTW + cx] = (float)gauss_sum<RT>(sIn + ly * LW + cx + R, 1, taps, R);
     __syncthreads();
-    for (int i = threadIdx.x; i < kGaussTW * kGaussTH; i += kGaussNT) {
-        const int cy = i / kGaussTW, cx = i % kGaussTW;
-        const int x = x0 + cx, y = y0 + cy;
-        if (x >= nx || y >= ny) continue;
-        const float *col = sRow + (cy + R) * kGaussTW + cx;
-        double sum = taps.B[0] * (double)col[0];
-        for (int j = 1; j <= R; j++) {
-            const float pair = col[-j * kGaussTW] + col[j * kGaussTW];
-            sum += taps.B[j] * (double)pair;
+    for (int cy = ty; cy < kGaussTH; cy += kGaussNT / 32) {
+        const int y = y0 + cy;
+        if (y >= ny) break;
+        for (int cx = tx; cx < kGaussTW; cx += 32) {
+            const int x = x0 + cx;
+            if (x >= nx) break;
+            out[(size_t)y * nx + x] =
+                (float)gauss_sum<RT>(sRow + (cy + R) * kGaussTW + cx, kGaussTW, taps, R);
         }
-        out[(size_t)y * nx + x] = (float)sum;
     }
 }
 
@@ -338,50 +381,45 @@ __global__ void __launch_bounds__(kGaussNT) k_gauss(const float *__restrict__ sr
 // plane at the even rows and columns: the row pass runs on even columns only
 // and the column pass on even rows only, with the same taps, mirror, pairing
 // and double sums as k_gauss, so every output is bit-identical to blur then
-// resample.  Tile: kDecTW x kDecTH outputs; gridDim.z = planes.
-constexpr int kDecTW = 32, kDecTH = 16, kDecNT = 256, kDecMaxR = 8;
+// resample.  Tile: kDecTW x kDecTH outputs, 256 threads as 32 x 8; gridDim.z
+// = planes.
+constexpr int kDecTW = 32, kDecTH = 32, kDecNT = 256, kDecMaxR = 8;
+template <int RT>
 __global__ void __launch_bounds__(kDecNT) k_gauss_dec2(const float *__restrict__ src, size_t src_stride,
                                                        int nx, int ny, float *dst, size_t dst_stride,
                                                        int nxx, int nyy, GaussTaps taps) {
-    constexpr int LW = 2 * kDecTW - 1 + 2 * kDecMaxR, LH = 2 * kDecTH - 1 + 2 * kDecMaxR;
+    constexpr int MR = RT > 0 ? RT : kDecMaxR;
+    constexpr int LW = 2 * kDecTW - 1 + 2 * MR, LH = 2 * kDecTH - 1 + 2 * MR;
     __shared__ float sIn[LH * LW];
     __shared__ float sRow[LH * kDecTW];
-    const int R = taps.size - 1;
+    const int R = RT > 0 ? RT : taps.size - 1;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const float *in = src + (size_t)blockIdx.z * src_stride;
     float *out = dst + (size_t)blockIdx.z * dst_stride;
     const int x0 = blockIdx.x * kDecTW, y0 = blockIdx.y * kDecTH;
     const int ix0 = 2 * x0 - R, iy0 = 2 * y0 - R;  // input origin of the region
     const int lw = 2 * kDecTW - 1 + 2 * R, lh = 2 * kDecTH - 1 + 2 * R;
-    for (int i = threadIdx.x; i < lw * lh; i += kDecNT) {
-        const int ly = i / lw, lx = i % lw;
-        const int my = gauss_mirror(iy0 + ly, ny), mx = gauss_mirror(ix0 + lx, nx);
-        float v = 0.0f;
-        if (mx >= 0 && mx < nx && my >= 0 && my < ny) v = __ldg(in + (size_t)my * nx + mx);
-        sIn[ly * LW + lx] = v;
+    for (int ly = ty; ly < lh; ly += kDecNT / 32) {
+        const int my = gauss_mirror(iy0 + ly, ny);
+        const bool row_ok = my >= 0 && my < ny;
+        for (int lx = tx; lx < lw; lx += 32) {
+            const int mx = gauss_mirror(ix0 + lx, nx);
+            float v = 0.0f;
+            if (row_ok && mx >= 0 && mx < nx) v = __ldg(in + (size_t)my * nx + mx);
+            sIn[ly * LW + lx] = v;
+        }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < kDecTW * lh; i += kDecNT) {
-        const int ly = i / kDecTW, cx = i % kDecTW;
-        const float *row = sIn + ly * LW + 2 * cx + R;
-        double sum = taps.B[0] * (double)row[0];
-        for (int j = 1; j <= R; j++) {
-            const float pair = row[-j] + row[j];
-            sum += taps.B[j] * (double)pair;
-        }
-        sRow[ly * kDecTW + cx] = (float)sum;
-    }
+    for (int ly = ty; ly < lh; ly += kDecNT / 32)
+        sRow[ly * kDecTW + tx] = (float)gauss_sum<RT>(sIn + ly * LW + 2 * tx + R, 1, taps, R);
     __syncthreads();
-    for (int i = threadIdx.x; i < kDecTW * kDecTH; i += kDecNT) {
-        const int cy = i / kDecTW, cx = i % kDecTW;
-        const int x = x0 + cx, y = y0 + cy;
-        if (x >= nxx || y >= nyy) continue;
-        const float *col = sRow + (2 * cy + R) * kDecTW + cx;
-        double sum = taps.B[0] * (double)col[0];
-        for (int j = 1; j <= R; j++) {
-            const float pair = col[-j * kDecTW] + col[j * kDecTW];
-            sum += taps.B[j] * (double)pair;
-        }
-        out[(size_t)y * nxx + x] = (float)sum;
+    const int x = x0 + tx;
+    if (x >= nxx) return;
+    for (int cy = ty; cy < kDecTH; cy += kDecNT / 32) {
+        const int y = y0 + cy;
+        if (y >= nyy) break;
+        out[(size_t)y * nxx + x] =
+            (float)gauss_sum<RT>(sRow + (2 * cy + R) * kDecTW + tx, kDecTW, taps, R);
     }
 }
 
@@ -1553,7 +1591,12 @@ GaussTaps make_zoom_taps(float zfactor) { return make_taps(zoom_sigma(zfactor));
 void launch_gauss(const float *src, float *dst, int nx, int ny, size_t stride,
                   const GaussTaps &t, int planes, cudaStream_t st) {
     dim3 g(div_up(nx, kGaussTW), div_up(ny, kGaussTH), planes);
-    k_gauss<0><<<g, kGaussNT, 0, st>>>(src, dst, nx, ny, stride, t, nullptr, 0, nullptr);
+    if (t.size == 5)
+        k_gauss<0, 4><<<g, kGaussNT, 0, st>>>(src, dst, nx, ny, stride, t, nullptr, 0, nullptr);
+    else if (t.size == 6)
+        k_gauss<0, 5><<<g, kGaussNT, 0, st>>>(src, dst, nx, ny, stride, t, nullptr, 0, nullptr);
+    else
+        k_gauss<0, 0><<<g, kGaussNT, 0, st>>>(src, dst, nx, ny, stride, t, nullptr, 0, nullptr);
 }
 
 void launch_resample(const float *src, size_t sstride, int nx, int ny, float *dst,
@@ -1568,7 +1611,10 @@ int launch_zoom_out(const float *src, size_t sstride, int nx, int ny, float *T, 
                     int planes, cudaStream_t st) {
     if (zfactor == 0.5f && t.size - 1 <= kDecMaxR) {
         dim3 g(div_up(nxx, kDecTW), div_up(nyy, kDecTH), planes);
-        k_gauss_dec2<<<g, kDecNT, 0, st>>>(src, sstride, nx, ny, dst, dstride, nxx, nyy, t);
+        if (t.size == 6)  // sigma 0.6 sqrt(3) of zfactor 1/2: radius 5
+            k_gauss_dec2<5><<<g, kDecNT, 0, st>>>(src, sstride, nx, ny, dst, dstride, nxx, nyy, t);
+        else
+            k_gauss_dec2<0><<<g, kDecNT, 0, st>>>(src, sstride, nx, ny, dst, dstride, nxx, nyy, t);
         return 1;
     }
     launch_gauss(src, T, nx, ny, sstride, t, planes, st);
@@ -1929,19 +1975,23 @@ void TvPlan::record(cudaStream_t st) {
             k_ingest<uint8_t><<<g, kIngestNT, 0, st>>>(frames, w_, h_, recs, ingest_blocks_);
         else
             k_ingest<float><<<g, kIngestNT, 0, st>>>(frames, w_, h_, recs, ingest_blocks_);
-        k_norm_finalize<<<B, 32, 0, st>>>(recs, ingest_blocks_, ctrl);
+        k_norm_finalize<<<B, kNormNT, 0, st>>>(recs, ingest_blocks_, ctrl);
         launches_ += 2;
     }
     // conversion, normalisation and pre-smoothing of level 0 in one pass
     // (tvl1.cpp:137-144)
     {
         dim3 g(div_up(w_, kGaussTW), div_up(h_, kGaussTH), 2 * B);
-        if (dtype_ == OFLOW_U8)
-            k_gauss<1><<<g, kGaussNT, 0, st>>>(nullptr, pyr + pyr_off_[0], w_, h_, N0, taps0_, ctrl, 1,
-                                               frames);
+        float *p0 = pyr + pyr_off_[0];
+        const bool r4 = taps0_.size == 5;  // sigma 0.8: radius 4
+        if (dtype_ == OFLOW_U8 && r4)
+            k_gauss<1, 4><<<g, kGaussNT, 0, st>>>(nullptr, p0, w_, h_, N0, taps0_, ctrl, 1, frames);
+        else if (dtype_ == OFLOW_U8)
+            k_gauss<1, 0><<<g, kGaussNT, 0, st>>>(nullptr, p0, w_, h_, N0, taps0_, ctrl, 1, frames);
+        else if (r4)
+            k_gauss<2, 4><<<g, kGaussNT, 0, st>>>(nullptr, p0, w_, h_, N0, taps0_, ctrl, 1, frames);
         else
-            k_gauss<2><<<g, kGaussNT, 0, st>>>(nullptr, pyr + pyr_off_[0], w_, h_, N0, taps0_, ctrl, 1,
-                                               frames);
+            k_gauss<2, 0><<<g, kGaussNT, 0, st>>>(nullptr, p0, w_, h_, N0, taps0_, ctrl, 1, frames);
         launches_ += 1;
     }
     // pyramid (tvl1.cpp:147-154)
