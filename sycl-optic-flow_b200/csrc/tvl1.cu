@@ -64,7 +64,7 @@ inline bool cfg_tile(int c, int &tw, int &th) {
     }
     return false;
 }
-constexpr int kClC = 8, kClNT = 512;
+constexpr int kClC = 8;
 constexpr size_t kClMaxSmem = 200 * 1024;
 __host__ __device__ inline int cl_band_rows(int ny) { return (ny + kClC - 1) / kClC; }
 // u (8 B), p (16 B) and the warp data (16 B) of a band in shared memory
@@ -280,6 +280,30 @@ __device__ __forceinline__ int gauss_mirror(int x, int n) {
     return x;
 }
 
+// Fills the LW x LH region sIn (row stride LW) with fetch(ly, lx), NT
+// threads as 32 x NT/32: every load of a thread is issued before the first
+// store, so they are in flight together.
+template <int NT, int LW, int LH, typename F>
+__device__ __forceinline__ void load_region(float *sIn, F &&fetch) {
+    constexpr int NY = NT / 32, RY = (LH + NY - 1) / NY, RX = (LW + 31) / 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x / 32;
+    float v[RY][RX];
+#pragma unroll
+    for (int a = 0; a < RY; a++)
+#pragma unroll
+        for (int b = 0; b < RX; b++) {
+            const int ly = ty + a * NY, lx = tx + 32 * b;
+            v[a][b] = (ly < LH && lx < LW) ? fetch(ly, lx) : 0.0f;
+        }
+#pragma unroll
+    for (int a = 0; a < RY; a++)
+#pragma unroll
+        for (int b = 0; b < RX; b++) {
+            const int ly = ty + a * NY, lx = tx + 32 * b;
+            if (ly < LH && lx < LW) sIn[ly * LW + lx] = v[a][b];
+        }
+}
+
 // Row then column pass of the separable Gaussian over one tile, both with the
 // reference's pairing (input[i-j] + input[i+j] in single precision) and double
 // taps and sums (mask.cpp:246-286).  RT > 0: the radius at compile time
@@ -338,25 +362,20 @@ __global__ void __launch_bounds__(kGaussNT) k_gauss(const float *__restrict__ sr
         __syncthreads();
     }
     const int lw = kGaussTW + 2 * R, lh = kGaussTH + 2 * R;
-    for (int ly = ty; ly < lh; ly += kGaussNT / 32) {
-        const int my = gauss_mirror(y0 - R + ly, ny);
-        const bool row_ok = my >= 0 && my < ny;
-        for (int lx = tx; lx < lw; lx += 32) {
-            const int mx = gauss_mirror(x0 - R + lx, nx);
-            float v = 0.0f;
-            if (row_ok && mx >= 0 && mx < nx) {
-                if (SRC == 0) {
-                    v = __ldg(in + (size_t)my * nx + mx);
-                } else if (SRC == 1) {
-                    v = sLut[__ldg(static_cast<const uint8_t *>(f.p) + (size_t)my * f.pitch + mx)];
-                } else {
-                    v = __ldg(static_cast<const float *>(f.p) + (size_t)my * f.pitch + mx);
-                    if (apply) v = (float)(255.0 * (double)(v - mn) / (double)den);
-                }
-            }
-            sIn[ly * LW + lx] = v;
-        }
-    }
+    auto fetch = [&](int ly, int lx) -> float {
+        const int my = gauss_mirror(y0 - R + ly, ny), mx = gauss_mirror(x0 - R + lx, nx);
+        if (my < 0 || my >= ny || mx < 0 || mx >= nx) return 0.0f;
+        if (SRC == 0) return __ldg(in + (size_t)my * nx + mx);
+        if (SRC == 1) return sLut[__ldg(static_cast<const uint8_t *>(f.p) + (size_t)my * f.pitch + mx)];
+        float v = __ldg(static_cast<const float *>(f.p) + (size_t)my * f.pitch + mx);
+        if (apply) v = (float)(255.0 * (double)(v - mn) / (double)den);
+        return v;
+    };
+    if (RT > 0)
+        load_region<kGaussNT, LW, LH>(sIn, fetch);
+    else
+        for (int ly = ty; ly < lh; ly += kGaussNT / 32)
+            for (int lx = tx; lx < lw; lx += 32) sIn[ly * LW + lx] = fetch(ly, lx);
     __syncthreads();
     for (int ly = ty; ly < lh; ly += kGaussNT / 32)
         for (int cx = tx; cx < kGaussTW; cx += 32)
@@ -399,16 +418,16 @@ __global__ void __launch_bounds__(kDecNT) k_gauss_dec2(const float *__restrict__
     const int x0 = blockIdx.x * kDecTW, y0 = blockIdx.y * kDecTH;
     const int ix0 = 2 * x0 - R, iy0 = 2 * y0 - R;  // input origin of the region
     const int lw = 2 * kDecTW - 1 + 2 * R, lh = 2 * kDecTH - 1 + 2 * R;
-    for (int ly = ty; ly < lh; ly += kDecNT / 32) {
-        const int my = gauss_mirror(iy0 + ly, ny);
-        const bool row_ok = my >= 0 && my < ny;
-        for (int lx = tx; lx < lw; lx += 32) {
-            const int mx = gauss_mirror(ix0 + lx, nx);
-            float v = 0.0f;
-            if (row_ok && mx >= 0 && mx < nx) v = __ldg(in + (size_t)my * nx + mx);
-            sIn[ly * LW + lx] = v;
-        }
-    }
+    auto fetch = [&](int ly, int lx) -> float {
+        const int my = gauss_mirror(iy0 + ly, ny), mx = gauss_mirror(ix0 + lx, nx);
+        if (my < 0 || my >= ny || mx < 0 || mx >= nx) return 0.0f;
+        return __ldg(in + (size_t)my * nx + mx);
+    };
+    if (RT > 0)
+        load_region<kDecNT, LW, LH>(sIn, fetch);
+    else
+        for (int ly = ty; ly < lh; ly += kDecNT / 32)
+            for (int lx = tx; lx < lw; lx += 32) sIn[ly * LW + lx] = fetch(ly, lx);
     __syncthreads();
     for (int ly = ty; ly < lh; ly += kDecNT / 32)
         sRow[ly * kDecTW + tx] = (float)gauss_sum<RT>(sIn + ly * LW + 2 * tx + R, 1, taps, R);
@@ -438,18 +457,12 @@ __global__ void k_resample(const float *__restrict__ src, size_t src_stride, int
 
 // Flow upsampling to the next finer scale (tvl1.cpp:167-172): bicubic of both
 // components at (j*nx/nxx, i*ny/nyy) then times 1/zfactor.  Reads U[cur].
-__global__ void k_zoom_flow(const float2 *U0, const float2 *U1, size_t stride, int nx, int ny,
-                            float2 *Uz, int nxx, int nyy, float fx, float fy, float inv,
-                            const TvCtrl *ctrl) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = blockIdx.y * blockDim.y + threadIdx.y;
-    const int b = blockIdx.z;
-    if (j >= nxx || i >= nyy) return;
-    const float2 *U = state_buf(U0, U1, ctrl[b].cur) + (size_t)b * stride;
-    const float i2 = (float)i / fy, j2 = (float)j / fx;
-    BicubicStencil s;
-    bicubic_stencil(j2, i2, nx, ny, false, s);
-    float a[4], c[4];
+// Each thread writes the outputs j0 = 2*tid and j0 + 1 of one row: they share
+// ty, and at a zoom factor of 2 also the stencil, so the four columns' first
+// passes are evaluated once for both (a pair whose stencils differ takes them
+// separately).
+__device__ __forceinline__ void zoom_columns(const float2 *U, int nx, const BicubicStencil &s,
+                                             float *a, float *c) {
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         const float2 *col = U + s.col[k];
@@ -458,9 +471,33 @@ __global__ void k_zoom_flow(const float2 *U0, const float2 *U1, size_t stride, i
         a[k] = cubic_cell(t0.x, t1.x, t2.x, t3.x, s.ty);
         c[k] = cubic_cell(t0.y, t1.y, t2.y, t3.y, s.ty);
     }
-    const float u = cubic_cell(a[0], a[1], a[2], a[3], s.tx);
-    const float v = cubic_cell(c[0], c[1], c[2], c[3], s.tx);
-    Uz[(size_t)b * stride + (size_t)i * nxx + j] = make_float2(inv * u, inv * v);
+}
+
+__global__ void k_zoom_flow(const float2 *U0, const float2 *U1, size_t stride, int nx, int ny,
+                            float2 *Uz, int nxx, int nyy, float fx, float fy, float inv,
+                            const TvCtrl *ctrl) {
+    const int j0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+    const int b = blockIdx.z;
+    if (j0 >= nxx || i >= nyy) return;
+    const float2 *U = state_buf(U0, U1, ctrl[b].cur) + (size_t)b * stride;
+    float2 *out = Uz + (size_t)b * stride + (size_t)i * nxx;
+    const float i2 = (float)i / fy;
+    BicubicStencil s0;
+    bicubic_stencil((float)j0 / fx, i2, nx, ny, false, s0);
+    float a[4], c[4];
+    zoom_columns(U, nx, s0, a, c);
+    out[j0] = make_float2(inv * cubic_cell(a[0], a[1], a[2], a[3], s0.tx),
+                          inv * cubic_cell(c[0], c[1], c[2], c[3], s0.tx));
+    const int j1 = j0 + 1;
+    if (j1 >= nxx) return;
+    BicubicStencil s1;
+    bicubic_stencil((float)j1 / fx, i2, nx, ny, false, s1);
+    if (s1.col[0] != s0.col[0] || s1.col[1] != s0.col[1] || s1.col[2] != s0.col[2] ||
+        s1.col[3] != s0.col[3])
+        zoom_columns(U, nx, s1, a, c);
+    out[j1] = make_float2(inv * cubic_cell(a[0], a[1], a[2], a[3], s1.tx),
+                          inv * cubic_cell(c[0], c[1], c[2], c[3], s1.tx));
 }
 
 // ---------------------------------------------------------------- gradient
@@ -888,7 +925,7 @@ __device__ __forceinline__ void tb_iteration(int j, float4 *sP, const float4 *sW
 // SM leave it under 512 bytes a block.)
 template <int K, int NT>
 __device__ __forceinline__ bool tb_decide(const TbArgs &a, TvCtrl *ctrl, int b, int tile,
-                                          int ntiles, const double (&err)[K], int kk, int fin,
+                                          int ntiles, double wsum, int kk, int fin,
                                           int snap, int redo, int n0, TbQueue *q, int *left,
                                           double *scratch) {
     // The K sums share one block barrier: per warp a fixed shuffle tree, then
@@ -900,13 +937,7 @@ __device__ __forceinline__ bool tb_decide(const TbArgs &a, TvCtrl *ctrl, int b, 
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     double *part = a.partials + (size_t)b * a.max_tiles * K;
     __syncthreads();  // every thread has stored its share of the tile (scratch overlays it)
-#pragma unroll
-    for (int j = 0; j < K; j++) {
-        double v = err[j];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-        if (lane == 0) sred[j][wid] = v;
-    }
+    if (lane < K) sred[lane][wid] = wsum;  // the warp sums of tb_tile (lane j: iteration j)
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int j = 0; j < kk; j++) {
@@ -1035,13 +1066,16 @@ __device__ __forceinline__ TbStart tb_start(const TbArgs &a, const TvCtrl *ctrl)
 
 // One tile of one pair for kk <= K iterations: the region in (TMA boxes on
 // `bar` with the given phase parity, or plain loads past L1), the iterations,
-// the snapshot stores and the final store of the owned tile.  err[j] gets the
-// owned pixels' squared change of iteration j.  Returns false if the TMA wait
-// gave up (the error flag is set; the caller leaves).
+// the snapshot stores and the final store of the owned tile.  The owned
+// pixels' squared change of iteration j is summed over each warp right after
+// the iteration (the fixed shuffle tree tb_decide applies) and lane j keeps
+// the warp's sum in wsum, so no per-iteration accumulator stays live across
+// the iterations.  Returns false if the TMA wait gave up (the error flag is
+// set; the caller leaves).
 template <int TW, int TH, int K, int NT>
 __device__ __forceinline__ bool tb_tile(const TbArgs &a, int b, int tx, int ty, const TbStart &t,
                                         uint32_t bar, uint32_t parity, float4 *tb_smem,
-                                        double (&err)[K]) {
+                                        double &wsum) {
     constexpr int RW = TW + 2 * K, RH = TH + 2 * K, RN = RW * RH;
     float4 *sP = tb_smem;                                  // RN
     float4 *sWR = sP + RN;                                 // RN
@@ -1109,16 +1143,21 @@ __device__ __forceinline__ bool tb_tile(const TbArgs &a, int b, int tx, int ty, 
             Pd[q] = sP[r];
         }
     };
+    wsum = 0.0;
 #pragma unroll
     for (int j = 0; j < K; j++) {
-        err[j] = 0.0;
         if (j < kk) {  // uniform over the block
+            double e = 0.0;
             if (interior)
                 tb_iteration<TW, TH, K, NT, true>(j + 1, sP, sWR, sU, ox, oy, nx, ny, a.l_t,
-                                                  a.theta, a.taut, err[j]);
+                                                  a.theta, a.taut, e);
             else
                 tb_iteration<TW, TH, K, NT, false>(j + 1, sP, sWR, sU, ox, oy, nx, ny, a.l_t,
-                                                   a.theta, a.taut, err[j]);
+                                                   a.theta, a.taut, e);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
+            e = __shfl_sync(0xffffffffu, e, 0);
+            if ((threadIdx.x & 31) == j) wsum = e;
             if (t.snaps && j + 1 < kk) {  // snapshot: the state a stop after iteration j+1 accepts
                 store_owned(state_buf(a.U0, a.U1, snap + j) + off, state_buf(a.P0, a.P1, snap + j) + off);
                 // the next iteration updates u and p in place: every thread must
@@ -1162,11 +1201,11 @@ __global__ void __launch_bounds__(NT, tb_min_blocks(NT)) k_tvl1_tb(const __grid_
         fence_mbar_init();
     }
     __syncthreads();  // the barrier is initialised before anyone waits on it
-    double err[K];
-    if (!tb_tile<TW, TH, K, NT>(a, b, blockIdx.x, blockIdx.y, t, bar, 0, tb_smem, err)) return;
+    double wsum;
+    if (!tb_tile<TW, TH, K, NT>(a, b, blockIdx.x, blockIdx.y, t, bar, 0, tb_smem, wsum)) return;
     const int fin = t.cur == 0 ? 1 : 0;
     const int snap = (t.cur >= 2 && t.cur < 2 + (K - 1)) ? 2 + (K - 1) : 2;
-    tb_decide<K, NT>(a, ctrl, b, blockIdx.y * gridDim.x + blockIdx.x, gridDim.x * gridDim.y, err,
+    tb_decide<K, NT>(a, ctrl, b, blockIdx.y * gridDim.x + blockIdx.x, gridDim.x * gridDim.y, wsum,
                      t.kk, fin, t.snaps ? snap : -1, t.redo, t.n0, nullptr, nullptr,
                      reinterpret_cast<double *>(tb_smem));
 }
@@ -1188,19 +1227,22 @@ __global__ void __launch_bounds__(NT, tb_min_blocks(NT)) k_tvl1_q(const __grid_c
     extern __shared__ __align__(128) float4 tb_smem[];
     __shared__ __align__(8) unsigned long long s_bar;
     __shared__ int s_b, s_tile;
+    // thread 0 only (in shared memory, not in every thread's registers): the
+    // pair last worked on (first pair to look at), and a tile of that pair's
+    // current block of iterations claimed ahead
+    __shared__ int s_hint, s_ahead;
     __shared__ TbStart s_t;
     const uint32_t bar = smem_u32(&s_bar);
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
         fence_mbar_init();
+        s_hint = blockIdx.x % B;
+        s_ahead = -1;
     }
     uint32_t parity = 0;
-    // thread 0 only: the pair last worked on (first pair to look at), and a
-    // tile of that pair's current block of iterations claimed ahead
-    int hint = blockIdx.x % B;
-    int ahead = -1;
     for (;;) {
         if (threadIdx.x == 0) {
+            int hint = s_hint, ahead = s_ahead;
             int got_b = -1, got_t = 0;
             if (ahead >= 0) {
                 // claimed while this block held a tile of the same block of
@@ -1254,15 +1296,17 @@ __global__ void __launch_bounds__(NT, tb_min_blocks(NT)) k_tvl1_q(const __grid_c
             }
             s_b = got_b;
             s_tile = got_t;
+            s_hint = hint;
+            s_ahead = ahead;
         }
         __syncthreads();
         const int b = s_b;
         if (b < 0) return;
         const TbStart t = s_t;
         const int tile = s_tile;
-        double err[K];
+        double wsum;
         if (!tb_tile<TW, TH, K, NT>(a, b, tile % tiles_x, tile / tiles_x, t, bar, parity, tb_smem,
-                                    err))
+                                    wsum))
             return;
         parity ^= 1u;
         // The tile's stores reach other SMs before the pair's decision opens
@@ -1271,7 +1315,7 @@ __global__ void __launch_bounds__(NT, tb_min_blocks(NT)) k_tvl1_q(const __grid_c
         // grid-wide barrier).
         const int fin = t.cur == 0 ? 1 : 0;
         const int snap = (t.cur >= 2 && t.cur < 2 + (K - 1)) ? 2 + (K - 1) : 2;
-        tb_decide<K, NT>(a, a.ctrl + b, b, tile, ntiles, err, t.kk, fin, t.snaps ? snap : -1,
+        tb_decide<K, NT>(a, a.ctrl + b, b, tile, ntiles, wsum, t.kk, fin, t.snaps ? snap : -1,
                          t.redo, t.n0, q, left, reinterpret_cast<double *>(tb_smem));
         __syncthreads();  // shared state of this item is dead before the next claim
     }
@@ -1378,12 +1422,24 @@ __global__ void __launch_bounds__(kLvNT) k_tvl1_level(TbArgs a) {
 // order from the others' shared memory, so all take the same stopping decision
 // (tvl1.cpp:216) and run the same number of cluster barriers.  The per-pixel
 // arithmetic is th_u_update and dual_update, as in the tiled kernels.
-__global__ void __cluster_dims__(kClC, 1, 1) __launch_bounds__(kClNT) k_tvl1_cluster(TbArgs a) {
+// (ly, x) of pixel i + NT from that of pixel i in rows of nx pixels.
+template <int NT>
+__device__ __forceinline__ void cl_step(int &ly, int &x, int nx) {
+    ly += NT / nx;
+    x += NT % nx;
+    if (x >= nx) {
+        x -= nx;
+        ly += 1;
+    }
+}
+
+template <int NT>
+__global__ void __cluster_dims__(kClC, 1, 1) __launch_bounds__(NT) k_tvl1_cluster(TbArgs a) {
     namespace cg = cooperative_groups;
     cg::cluster_group cluster = cg::this_cluster();
     const int c = (int)cluster.block_rank();
     extern __shared__ float4 cl_smem[];
-    __shared__ double sred[kClNT / 32];
+    __shared__ double sred[NT / 32];
     __shared__ double s_part;
     const int nx = a.nx, ny = a.ny, tid = threadIdx.x;
     const int r0 = c * ny / kClC, r1 = (c + 1) * ny / kClC, nb = r1 - r0;
@@ -1400,7 +1456,7 @@ __global__ void __cluster_dims__(kClC, 1, 1) __launch_bounds__(kClNT) k_tvl1_clu
     const float4 *__restrict__ Pin = state_buf(a.P0, a.P1, cur) + off + (size_t)r0 * nx;
     const float4 *__restrict__ Wg = a.WR + off + (size_t)r0 * nx;
     const int N = nb * nx;
-    for (int i = tid; i < N; i += kClNT) {
+    for (int i = tid; i < N; i += NT) {
         sU[i] = Uin[i];
         sP[i] = Pin[i];
         sW[i] = Wg[i];
@@ -1412,10 +1468,11 @@ __global__ void __cluster_dims__(kClC, 1, 1) __launch_bounds__(kClNT) k_tvl1_clu
     cluster.sync();
     int n = *((volatile int *)&ctrl->n);
     bool done = n >= a.max_it;
+    const int ly0 = tid / nx, x0 = tid - ly0 * nx;  // band row and column of pixel tid
     while (!done) {
         double err = 0.0;
-        for (int i = tid; i < N; i += kClNT) {
-            const int ly = i / nx, x = i - ly * nx, y = r0 + ly;
+        for (int i = tid, ly = ly0, x = x0; i < N; i += NT, cl_step<NT>(ly, x, nx)) {
+            const int y = r0 + ly;
             const float2 u = sU[i];
             const float4 pc = sP[i];
             const float4 pl = x > 0 ? sP[i - 1] : pc;  // unused on the left border
@@ -1427,7 +1484,7 @@ __global__ void __cluster_dims__(kClC, 1, 1) __launch_bounds__(kClNT) k_tvl1_clu
             const float term = e1 * e1 + e2 * e2;
             err += (double)term;
         }
-        const double bs = block_sum_double<kClNT>(err, sred);
+        const double bs = block_sum_double<NT>(err, sred);
         if (tid == 0) s_part = bs;
         cluster.sync();  // u new in every band, the bands' sums posted
         double tot = 0.0;
@@ -1437,8 +1494,8 @@ __global__ void __cluster_dims__(kClC, 1, 1) __launch_bounds__(kClNT) k_tvl1_clu
         float e = (float)tot;
         e = e / (float)(nx * ny);
         const bool stop = !(e > a.eps2) || n >= a.max_it;
-        for (int i = tid; i < N; i += kClNT) {
-            const int ly = i / nx, x = i - ly * nx, y = r0 + ly;
+        for (int i = tid, ly = ly0, x = x0; i < N; i += NT, cl_step<NT>(ly, x, nx)) {
+            const int y = r0 + ly;
             const float2 uc = sU[i];
             float f1x = 0.0f, f2x = 0.0f, f1y = 0.0f, f2y = 0.0f;
             if (x < nx - 1) {
@@ -1458,7 +1515,7 @@ __global__ void __cluster_dims__(kClC, 1, 1) __launch_bounds__(kClNT) k_tvl1_clu
     }
     float2 *__restrict__ Uout = state_buf(a.U0, a.U1, fin) + off + (size_t)r0 * nx;
     float4 *__restrict__ Pout = state_buf(a.P0, a.P1, fin) + off + (size_t)r0 * nx;
-    for (int i = tid; i < N; i += kClNT) {
+    for (int i = tid; i < N; i += NT) {
         Uout[i] = sU[i];
         Pout[i] = sP[i];
     }
@@ -1685,8 +1742,15 @@ static void tb_launch(dim3 g, cudaStream_t st, const TbArgs &ta) {
 
 static void tb_launch_cfg(int cfg, dim3 g, cudaStream_t st, const TbArgs &ta) {
     if (cfg == kClusterCfg) {
-        const size_t smem = (size_t)cl_band_rows(ta.ny) * ta.nx * (2 * sizeof(float4) + sizeof(float2));
-        k_tvl1_cluster<<<dim3(kClC, g.z), kClNT, smem, st>>>(ta);
+        // 256 threads where they cover a band in one pass, else 512 (1024
+        // threads leave one block per SM: 32 clusters of 8 then take two
+        // waves, and the 128x55 level took 1.6 ms instead of 0.95)
+        const int band = cl_band_rows(ta.ny) * ta.nx;
+        const size_t smem = (size_t)band * (2 * sizeof(float4) + sizeof(float2));
+        if (band <= 256)
+            k_tvl1_cluster<256><<<dim3(kClC, g.z), 256, smem, st>>>(ta);
+        else
+            k_tvl1_cluster<512><<<dim3(kClC, g.z), 512, smem, st>>>(ta);
         return;
     }
     if (cfg == kLevelCfg) {
@@ -1751,7 +1815,9 @@ static void tb_set_smem_attrs() {
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tb_smem_bytes(64, 16)));
     OF_CUDA(cudaFuncSetAttribute(k_tvl1_level, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  kLvMaxPx * (int)(sizeof(float4) + sizeof(float2))));
-    OF_CUDA(cudaFuncSetAttribute(k_tvl1_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    OF_CUDA(cudaFuncSetAttribute(k_tvl1_cluster<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kClMaxSmem));
+    OF_CUDA(cudaFuncSetAttribute(k_tvl1_cluster<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kClMaxSmem));
 }
 
@@ -2011,7 +2077,8 @@ void TvPlan::record(cudaStream_t st) {
         dim3 blk(32, 8), gr(div_up(nx, 32), div_up(ny, 8), B);
         if (s < s0_) {
             const int cx = nx_[s + 1], cy = ny_[s + 1];
-            k_zoom_flow<<<gr, blk, 0, st>>>(U0, U1, N0, cx, cy, Uz, nx, ny, (float)nx / cx,
+            const dim3 zg(div_up(nx, 64), div_up(ny, 8), B);
+            k_zoom_flow<<<zg, blk, 0, st>>>(U0, U1, N0, cx, cy, Uz, nx, ny, (float)nx / cx,
                                             (float)ny / cy, inv, ctrl);
             launches_ += 1;
         }
