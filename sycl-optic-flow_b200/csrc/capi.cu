@@ -91,9 +91,14 @@ struct MixedBatch {
 };
 }  // namespace
 
-// A TV-L1 batch with frames or flows in host memory is solved in up to this
-// many chunks, each a plan of its own on a side stream, so that the copies of
-// one chunk overlap the solves of the others.
+// A TV-L1 batch with frames or flows in host memory may be solved in up to
+// this many chunks, each a plan of its own on a side stream, so that the
+// copies of one chunk overlap the solves of the others (OFLOW_HOST_CHUNKS).
+// By default it is one plan with its copies before and after: for 32 pairs of
+// 1024x436 that measured 1,155 pairs/s end to end against 1,143 with four
+// concurrent chunks (one launch per block of iterations) and 778-986 with the
+// chunks' solves one after another, each with the work queue (a small plan
+// pays the latency-bound coarse scales again).
 constexpr int kHostChunks = 4;
 constexpr int kChunkMinPairs = 4;
 
@@ -183,6 +188,13 @@ int side_share(int chunks) {
     const char *e = getenv("OFLOW_SIDE_QUEUE");
     const int n = e ? atoi(e) : 0;
     return n > 0 ? n : chunks;
+}
+
+// Chunks of a host batch (OFLOW_HOST_CHUNKS, 1..kHostChunks; default 1).
+int host_chunks() {
+    const char *e = getenv("OFLOW_HOST_CHUNKS");
+    const int n = e ? atoi(e) : 1;
+    return n < 1 ? 1 : (n > kHostChunks ? kHostChunks : n);
 }
 
 TvPlan &side_plan(oflow_ctx *ctx, int c, int chunks, int w, int h, int B, int dtype,
@@ -331,7 +343,7 @@ void run_tvl1(oflow_ctx *ctx, int n, const oflow_image *I0, const oflow_image *I
             host_io = host_io || I0[i].location == OFLOW_HOST || I1[i].location == OFLOW_HOST ||
                       out[i].location == OFLOW_HOST;
         const int chunks = (host_io && !prof && !energy_trace)
-                               ? std::max(1, std::min(kHostChunks, ng / kChunkMinPairs))
+                               ? std::max(1, std::min(host_chunks(), ng / kChunkMinPairs))
                                : 1;
         if (chunks > 1) {
             // chunk c: pairs [c*ng/chunks, (c+1)*ng/chunks) on side stream c

@@ -140,41 +140,54 @@ __global__ void k_lk_grad(const float *__restrict__ src, size_t sstride, int nx,
     G[(size_t)blockIdx.z * gstride + (size_t)y * nx + x] = make_float2(ax, ay);
 }
 
-// lk_window_solve with the window radius known at compile time (the loops
-// unroll; the same sums in the same order).
-template <int C>
-__device__ __forceinline__ void lk_window_solve_c(const float *gx, const float *gy, const float *gt,
-                                                  int RW, int cidx, float &vx, float &vy) {
-    float sxx = 0.0f, sxy = 0.0f, syy = 0.0f, sxt = 0.0f, syt = 0.0f;
+// Window sums and the 2x2 solve of P vertically adjacent pixels (column cidx,
+// rows of centres crow .. crow+P-1 in shared memory): each window element is
+// loaded and its five products formed once for every pixel whose window holds
+// it; each pixel still adds them in the reference's row-major order
+// (kernels.cu:150-179), so its sums are those of lk_window_solve.
+template <int C, int P>
+__device__ __forceinline__ void lk_window_solve_p(const float *gx, const float *gy, const float *gt,
+                                                  int RW, int top, float (&vx)[P], float (&vy)[P]) {
+    float sxx[P], sxy[P], syy[P], sxt[P], syt[P];
 #pragma unroll
-    for (int ii = -C; ii <= C; ii++) {
-        const int row = cidx + ii * RW;
+    for (int k = 0; k < P; k++) sxx[k] = sxy[k] = syy[k] = sxt[k] = syt[k] = 0.0f;
 #pragma unroll
-        for (int jj = -C; jj <= C; jj++) {
-            const int q = row + jj;
-            const float ix = gx[q], iy = gy[q], it = gt[q];
-            sxx += ix * ix;
-            sxy += ix * iy;
-            syy += iy * iy;
-            sxt += ix * it;
-            syt += iy * it;
+    for (int r = 0; r < 2 * C + P; r++) {
+        const int row = top + r * RW;
+#pragma unroll
+        for (int jj = 0; jj <= 2 * C; jj++) {
+            const float ix = gx[row + jj], iy = gy[row + jj], it = gt[row + jj];
+            const float pxx = ix * ix, pxy = ix * iy, pyy = iy * iy, pxt = ix * it, pyt = iy * it;
+#pragma unroll
+            for (int k = 0; k < P; k++)
+                if (r - k >= 0 && r - k <= 2 * C) {
+                    sxx[k] += pxx;
+                    sxy[k] += pxy;
+                    syy[k] += pyy;
+                    sxt[k] += pxt;
+                    syt[k] += pyt;
+                }
         }
     }
-    const float det = (sxx * syy - sxy * sxy);
-    vx = 0.0f;
-    vy = 0.0f;
-    if (det != 0.0f) {
-        vx = 1.0f / det * (syy * (-sxt) + (-sxy) * (-syt));
-        vy = 1.0f / det * ((-sxy) * (-sxt) + sxx * (-syt));
+#pragma unroll
+    for (int k = 0; k < P; k++) {
+        const float det = (sxx[k] * syy[k] - sxy[k] * sxy[k]);
+        vx[k] = 0.0f;
+        vy[k] = 0.0f;
+        if (det != 0.0f) {
+            vx[k] = 1.0f / det * (syy[k] * (-sxt[k]) + (-sxy[k]) * (-syt[k]));
+            vy[k] = 1.0f / det * ((-sxy[k]) * (-sxt[k]) + sxx[k] * (-syt[k]));
+        }
     }
 }
 
 // One refinement of pyramidal LK: warp I1 by the current flow (bilinear,
 // clamp-to-edge), It = 0 + (-1)*I0 + 1*I1w, window solve, Uout = Uin + d.
-// Tile 32 x 16 with the window radius C as halo.  (Window sums read from
+// Tile 32 x kPTH with the window radius C as halo; a thread solves kPP
+// vertically adjacent pixels (lk_window_solve_p).  (Window sums read from
 // precomputed product planes measured slower: 18.2k against 21.4k pairs/s
 // batched; five loads per window element instead of three bound the LSU pipe.)
-constexpr int kPTW = 32, kPTH = 16, kPNT = kPTW * kPTH;
+constexpr int kPTW = 32, kPP = 2, kPTH = 32, kPNT = kPTW * kPTH / kPP;
 template <int C>
 __global__ void __launch_bounds__(kPNT) k_pyrlk_iter(const float *__restrict__ pyr, size_t lp,
                                                      const float2 *__restrict__ G, size_t gstride,
@@ -191,7 +204,11 @@ __global__ void __launch_bounds__(kPNT) k_pyrlk_iter(const float *__restrict__ p
     const int x0 = blockIdx.x * kPTW - C, y0 = blockIdx.y * kPTH - C;
     for (int i = threadIdx.x; i < RW * RH; i += kPNT) {
         const int x = x0 + i % RW, y = y0 + i / RW;
-        if (x < 0 || x >= nx || y < 0 || y >= ny) continue;
+        if (x < 0 || x >= nx || y < 0 || y >= ny) {
+            // read only by the sums of border pixels, whose results are not used
+            gx[i] = gy[i] = gt[i] = 0.0f;
+            continue;
+        }
         const size_t p = (size_t)y * nx + x;
         const float2 u = Ub[p];
         const float w = bilinear_clamped(I1, nx, ny, (float)x + u.x, (float)y + u.y);
@@ -204,15 +221,21 @@ __global__ void __launch_bounds__(kPNT) k_pyrlk_iter(const float *__restrict__ p
         gt[i] = it;
     }
     __syncthreads();
-    const int tx = threadIdx.x % kPTW, ty = threadIdx.x / kPTW;
-    const int x = blockIdx.x * kPTW + tx, y = blockIdx.y * kPTH + ty;
-    if (x >= nx || y >= ny) return;
-    float dx = 0.0f, dy = 0.0f;
-    if (x >= C && y >= C && x < nx - C && y < ny - C)
-        lk_window_solve_c<C>(gx, gy, gt, RW, (ty + C) * RW + tx + C, dx, dy);
-    const size_t p = (size_t)b * ustride + (size_t)y * nx + x;
-    const float2 u = Ub[(size_t)y * nx + x];
-    Uout[p] = make_float2(u.x + dx, u.y + dy);
+    const int tx = threadIdx.x % kPTW, ty = (threadIdx.x / kPTW) * kPP;
+    const int x = blockIdx.x * kPTW + tx, yb = blockIdx.y * kPTH + ty;
+    if (x >= nx || yb >= ny) return;
+    float dx[kPP], dy[kPP];
+    // top-left of the first pixel's window: row ty, column tx of the region
+    lk_window_solve_p<C, kPP>(gx, gy, gt, RW, ty * RW + tx, dx, dy);
+#pragma unroll
+    for (int k = 0; k < kPP; k++) {
+        const int y = yb + k;
+        if (y >= ny) break;
+        const bool in = x >= C && y >= C && x < nx - C && y < ny - C;
+        const size_t q = (size_t)y * nx + x;
+        const float2 u = Ub[q];
+        Uout[(size_t)b * ustride + q] = make_float2(u.x + (in ? dx[k] : 0.0f), u.y + (in ? dy[k] : 0.0f));
+    }
 }
 
 static void launch_pyrlk_iter(int c, dim3 g, cudaStream_t st, const float *pyr, size_t lp,

@@ -155,12 +155,15 @@ def test_device_frames_read_in_place_then_host_frames(of, orc, ctx):
     check(Bp, of.tvl1_batch(Bp, prm, ctx))
 
 
-def test_host_batch_in_chunks_matches_device_batch(of, ctx):
-    """A batch with host frames and host flows runs as up to four chunks on
-    side streams (copies of one chunk overlap the solves of the others); the
-    flows and statistics equal those of the same batch solved as one plan from
-    device frames, including a batch that does not split evenly."""
+@pytest.mark.parametrize("chunks", ["1", "4"])
+def test_host_batch_in_chunks_matches_device_batch(of, ctx, monkeypatch, chunks):
+    """A batch with host frames and host flows runs as one plan with its copies
+    around it (the default) or as up to four chunks on side streams
+    (OFLOW_HOST_CHUNKS; copies of one chunk overlap the solves of the others);
+    the flows and statistics equal those of the same batch solved as one plan
+    from device frames, including a batch that does not split evenly."""
     import torch
+    monkeypatch.setenv("OFLOW_HOST_CHUNKS", chunks)
     prm = of.TVL1Params(nscales=3, max_iterations=14)
     for n in (8, 13):
         pairs = [_pair(900 + i, 84, 60)[1:] for i in range(n)]
@@ -176,11 +179,13 @@ def test_host_batch_in_chunks_matches_device_batch(of, ctx):
 
 @pytest.mark.parametrize("side_queue", ["0", "1", "4"])
 def test_host_chunks_of_tiled_levels_match_device_batch(of, monkeypatch, side_queue):
-    """Host frames and flows of tiled levels (256x128): the chunks on side
-    streams run one launch per block of iterations (the default), or the
+    """Host frames and flows of tiled levels (256x128) in four chunks
+    (OFLOW_HOST_CHUNKS=4): the chunks on side streams run one launch per
+    block of iterations (the default), or the
     work queue on all or a quarter of the resident slots (OFLOW_SIDE_QUEUE);
     the flows equal the device batch solved as one plan."""
     import torch
+    monkeypatch.setenv("OFLOW_HOST_CHUNKS", "4")
     monkeypatch.setenv("OFLOW_SIDE_QUEUE", side_queue)
     c = of.Context(0)
     prm = of.TVL1Params(nscales=3, max_iterations=20)
