@@ -326,6 +326,7 @@ void run_tvl1(oflow_ctx *ctx, int n, const oflow_image *I0, const oflow_image *I
         }
     };
     auto collect = [&](TvPlan &pl, const Group &g, int b0, int b1, cudaStream_t s) {
+        if (stats) pl.compute_energy(s);
         for (int b = b0; b < b1; b++) {
             const oflow_flow &o = out[g.idx[b]];
             if (o.location == OFLOW_HOST) {
@@ -1040,8 +1041,10 @@ oflow_status oflow_tvl1_warm(oflow_ctx *ctx, oflow_net *net, int n, const oflow_
         std::vector<int> acc(n, 1);
         wp->true_energy(ew.data(), st);  // synchronises
         wp->check_device_error();
-        if (stats)
+        if (stats) {
+            wp->compute_energy(st);
             for (int b = 0; b < n; b++) wp->read_stats(b, &stats[b], st);
+        }
         TvPlan *pp = nullptr;
         if (plain) {
             pp = &tv_plan(ctx, g.w, g.h, n, g.dtype, *plain, false);
@@ -1192,6 +1195,7 @@ oflow_status oflow_stream_push(oflow_stream *s, const oflow_image *frames, const
         else
             s->hs->run(st);
         OF_CUDA(cudaEventRecord(s->done[k % 3], st));
+        if (stats && s->tv) s->tv->compute_energy(st);
         for (int i = 0; i < d.lanes; i++) {
             const float *ou = s->tv ? s->tv->out_u(i) : s->hs->out_u(i);
             const float *ov = s->tv ? s->tv->out_v(i) : s->hs->out_v(i);

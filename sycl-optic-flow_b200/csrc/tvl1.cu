@@ -2137,13 +2137,17 @@ void TvPlan::record(cudaStream_t st) {
             }
         }
     }
-    // final energy at the finest scale, last warp
-    k_energy<<<dim3(energy_blocks_, B), kEnNT, 0, st>>>(WR, U0, U1, N0, w_, h_, prm_.lambda,
-                                                        ctrl, part, max_blocks_, energy,
-                                                        energy_slots_, trace_ ? -1 : 0, -1);
+    // final energy at the finest scale, last warp: in the schedule of a traced
+    // plan; otherwise on demand (compute_energy), when statistics are read
+    if (trace_) {
+        k_energy<<<dim3(energy_blocks_, B), kEnNT, 0, st>>>(WR, U0, U1, N0, w_, h_, prm_.lambda,
+                                                            ctrl, part, max_blocks_, energy,
+                                                            energy_slots_, -1, -1);
+        launches_ += 1;
+    }
     k_split<<<dim3(div_up(w_, 32), div_up(h_, 8), B), dim3(32, 8), 0, st>>>(
         U0, U1, N0, w_, h_, ar_.at<OutRef>(o_otab_), ctrl);
-    launches_ += 2;
+    launches_ += 1;
     OF_CUDA(cudaGetLastError());
 }
 
@@ -2342,6 +2346,14 @@ void TvPlan::run(cudaStream_t st) {
     // tested without making any GPU wait run out.
     if (const char *e = getenv("OFLOW_INJECT_TIMEOUT"))
         if (atoi(e) == 1) err_.raise();
+}
+
+void TvPlan::compute_energy(cudaStream_t st) {
+    if (trace_) return;  // the traced schedule computes it
+    k_energy<<<dim3(energy_blocks_, B_), kEnNT, 0, st>>>(
+        ar_.at<float4>(o_WR_), ubuf(0), ubuf(1), N0_, w_, h_, prm_.lambda, ar_.at<TvCtrl>(o_ctrl_),
+        ar_.at<double>(o_part_), max_blocks_, ar_.at<double>(o_energy_), energy_slots_, 0, -1);
+    OF_CUDA(cudaGetLastError());
 }
 
 void TvPlan::read_stats(int b, oflow_tvl1_stats *out, cudaStream_t st) const {

@@ -140,6 +140,10 @@ class TvPlan {
     void record(cudaStream_t st);
     // upload the frame table, then record(): an eager run
     void run_eager(cudaStream_t st);
+    // The final energy (k_energy) of the last run's result, per pair, for
+    // read_stats; enqueue once after run() when statistics are wanted (traced
+    // plans compute it in their schedule).
+    void compute_energy(cudaStream_t st);
     void read_stats(int b, oflow_tvl1_stats *out, cudaStream_t st) const;
     // Eager run with events around each warp / inner-iteration launch.
     void profile(cudaStream_t st, oflow_tvl1_profile *out);

@@ -206,8 +206,8 @@ def test_launch_count_of_the_schedule(of, monkeypatch, queue):
     than 9216 pixels, ceil(50/4)+1 tiled inner-iteration launches (one for a
     re-run after a stop inside a launch that wrote no snapshots).  A smaller
     level runs its whole stage in one launch either way.  Plus the ingest,
-    pyramid (one fused blur-and-decimate launch per level), gradient, zoom
-    and output launches."""
+    pyramid (one fused blur-and-decimate launch per level), gradient and
+    column-coefficient, zoom and output launches."""
     if not queue:
         monkeypatch.setenv("OFLOW_TB_QUEUE", "0")
     ctx = of.Context(0)
@@ -222,8 +222,9 @@ def test_launch_count_of_the_schedule(of, monkeypatch, queue):
     per_stage = [1 + (1 if (w * h <= 9216 or queue) else 14) for w, h in sizes]
     expect = 5 * sum(per_stage)
     n = ctx.last_launches()
-    # ingest 2, level-0 blur 1, pyramid ns-1, gradients ns, zooms ns-1, energy and output 2
-    assert n == expect + 3 * ns + 3
+    # ingest 2, level-0 blur 1, pyramid ns-1, column coefficients ns, zooms ns-1, output 1
+    # (the final energy runs on demand, when statistics are read)
+    assert n == expect + 3 * ns + 2
     ctx.close()
 
 
