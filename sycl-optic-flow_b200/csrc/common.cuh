@@ -42,6 +42,26 @@ __device__ __forceinline__ int clamp_flag(int x, int n, bool &out) {
     return x;
 }
 
+// Visits the inclusive rectangle [x0,x1] x [y0,y1] of a region of width RW
+// with NT threads, one pixel per step (one division per call).
+template <int NT, typename F>
+__device__ __forceinline__ void for_rect(int x0, int x1, int y0, int y1, F &&f) {
+    const int w = x1 - x0 + 1, n = w * (y1 - y0 + 1);
+    if (n <= 0) return;
+    const int t = threadIdx.x;
+    int rx = x0 + t % w, ry = y0 + t / w;
+    const int sx = NT % w, sy = NT / w;
+    for (int k = t; k < n; k += NT) {
+        f(rx, ry);
+        rx += sx;
+        ry += sy;
+        if (rx > x1) {
+            rx -= w;
+            ry += 1;
+        }
+    }
+}
+
 // Keys cubic (a = -1/2) through v0..v3 at offset x from v1, with single
 // precision differences and double precision for the rest, as in
 // src/tvl1/sequential/bicubic_interpolation/bicubic_interpolation.cpp:38-46.

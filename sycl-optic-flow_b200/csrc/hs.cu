@@ -86,6 +86,37 @@ __global__ void __launch_bounds__(kDTW *kDTH) k_hs_warp_deriv(
     D[(size_t)b * dstride + (size_t)y * w + x] = make_float4(Ix, Iy, Iz, den);
 }
 
+// One Jacobi sweep (solverKernel.cuh:41-153) over cone j of the region:
+// neighbour mean of the increments (clamped at the image border), then
+// frac = (Ix*su + Iy*sv + Iz) / (Ix^2 + Iy^2 + alpha) and the update, in the
+// reference's order.  The division is Markstein's correction from the
+// precomputed reciprocal; operands outside its proven range take the IEEE
+// division.
+template <int RW, int RH, int NT, bool INTERIOR>
+__device__ __forceinline__ void hs_sweep(int j, const float2 *src, float2 *dst, const float4 *sD,
+                                         const float *sR, int x0, int y0, int w, int h) {
+    for_rect<NT>(j, RW - 1 - j, j, RH - 1 - j, [&](int rx, int ry) {
+        const int i = ry * RW + rx;
+        int l = i - 1, r = i + 1, up = i + RW, dn = i - RW;
+        if (!INTERIOR) {
+            const int x = x0 + rx, y = y0 + ry;
+            if (x < 0 || x >= w || y < 0 || y >= h) return;
+            if (x == 0) l = i;
+            if (x == w - 1) r = i;
+            if (y == h - 1) up = i;
+            if (y == 0) dn = i;
+        }
+        const float2 al = src[l], ar = src[r], au = src[up], ad = src[dn];
+        const float su = (al.x + ar.x + au.x + ad.x) * 0.25f;
+        const float sv = (al.y + ar.y + au.y + ad.y) * 0.25f;
+        const float4 d = sD[i];
+        const float p = d.x * su + d.y * sv + d.z;
+        float frac = markstein(p, d.w, sR[i]);
+        if (!(rcp_in_range(d.w) && markstein_safe(p))) frac = p / d.w;
+        dst[i] = make_float2(su - d.x * frac, sv - d.y * frac);
+    });
+}
+
 // Region loads of k_hs_jacobi by TMA: D as (2w, h, pair) and the incoming
 // increments as (w, h, pair), 8-byte elements, zero fill outside the level
 // (pixels outside are never read by a sweep).  use = 0: plain loads.
@@ -110,6 +141,7 @@ __global__ void __launch_bounds__(NT) k_hs_jacobi(const float4 *__restrict__ D, 
     float4 *sD = smem;                                   // RN
     float2 *sA = reinterpret_cast<float2 *>(sD + RN);    // RN
     float2 *sB = sA + RN;                                // RN
+    float *sR = reinterpret_cast<float *>(sB + RN);      // RN
     const int b = blockIdx.z;
     const float4 *Db = D + (size_t)b * dstride;
     const float2 *In = dUin + (size_t)b * stride;
@@ -151,25 +183,23 @@ __global__ void __launch_bounds__(NT) k_hs_jacobi(const float4 *__restrict__ D, 
         }
     }
     __syncthreads();
+    // RN(1 / (Ix^2 + Iy^2 + alpha)) per region pixel, constant over the sweeps:
+    // the quotient below is then Markstein's exact form (exact_math.cuh)
+    for (int i = threadIdx.x; i < RN; i += NT) sR[i] = rcp_near_rn(sD[i].w);
+    __syncthreads();
+    // Sweep j (1-based) updates [j, RW-1-j] x [j, RH-1-j]: exactly the cells
+    // whose values can still reach the owned tile, so no read leaves the
+    // region.  A region inside the image with a one-pixel margin takes the
+    // path without image-border tests.
+    const bool interior = x0 >= 0 && y0 >= 0 && x0 + RW <= w && y0 + RH <= h;
     float2 *src = sA, *dst = sB;
-    for (int s = 0; s < sweeps; s++) {
-        for (int i = threadIdx.x; i < RN; i += NT) {
-            const int rx = i % RW, ry = i / RW;
-            const int x = x0 + rx, y = y0 + ry;
-            if (x < 0 || x >= w || y < 0 || y >= h) continue;
-            // clamped image neighbours; at the tile-region edge (not the image
-            // edge) the value is stale but never reaches the owned tile
-            const int l = (x > 0 && rx > 0) ? i - 1 : i;
-            const int r = (x < w - 1 && rx < RW - 1) ? i + 1 : i;
-            const int up = (y < h - 1 && ry < RH - 1) ? i + RW : i;
-            const int dn = (y > 0 && ry > 0) ? i - RW : i;
-            const float2 al = src[l], ar = src[r], au = src[up], ad = src[dn];
-            const float su = (al.x + ar.x + au.x + ad.x) * 0.25f;
-            const float sv = (al.y + ar.y + au.y + ad.y) * 0.25f;
-            const float4 d = sD[i];
-            const float frac = (d.x * su + d.y * sv + d.z) / d.w;
-            dst[i] = make_float2(su - d.x * frac, sv - d.y * frac);
-        }
+#pragma unroll
+    for (int j = 1; j <= KH; j++) {
+        if (j > sweeps) break;
+        if (interior)
+            hs_sweep<RW, RH, NT, true>(j, src, dst, sD, sR, x0, y0, w, h);
+        else
+            hs_sweep<RW, RH, NT, false>(j, src, dst, sD, sR, x0, y0, w, h);
         __syncthreads();
         float2 *t = src;
         src = dst;
@@ -288,20 +318,21 @@ void launch_split2(const float2 *U, size_t stride, int N, float *out, int B, cud
 constexpr int kJTW = 32, kJTH = 16, kJK = 4, kJNT = 256;
 
 // Jacobi configurations: tile tw x th, up to k sweeps per launch (halo k),
-// nt threads; 32 B of shared memory per region pixel (D 16, two u buffers).
+// nt threads; 36 B of shared memory per region pixel (D 16, two u buffers,
+// the reciprocal of the denominator).
 struct HsJCfg {
     int tw, th, k, nt;
 };
 constexpr HsJCfg kHsCfgs[] = {{32, 16, 4, 256}, {32, 16, 8, 256}, {64, 32, 8, 512},
                               {64, 16, 4, 256}, {32, 32, 16, 512}};
 constexpr int kHsNumCfgs = 5;
-constexpr size_t hs_smem(const HsJCfg &c) { return (size_t)(c.tw + 2 * c.k) * (c.th + 2 * c.k) * 32; }
+constexpr size_t hs_smem(const HsJCfg &c) { return (size_t)(c.tw + 2 * c.k) * (c.th + 2 * c.k) * 36; }
 
 template <int TW, int TH, int KH, int NT>
 static void hs_jacobi_launch(dim3 g, cudaStream_t st, const float4 *D, size_t dstride,
                              const float2 *in, float2 *out, float2 *U, size_t stride, int w,
                              int h, int sweeps, int first, int last, const HsTma &tma) {
-    const size_t smem = (size_t)(TW + 2 * KH) * (TH + 2 * KH) * 32;
+    const size_t smem = (size_t)(TW + 2 * KH) * (TH + 2 * KH) * 36;
     k_hs_jacobi<TW, TH, KH, NT><<<g, NT, smem, st>>>(D, dstride, in, out, U, stride, w, h, sweeps,
                                                      first, last, tma);
 }
@@ -617,7 +648,7 @@ void hs_enqueue_into(void *scratch, const float *I0, const float *I1, int w, int
     }
     int ub = 0;
     OF_CUDA(cudaMemsetAsync(Ubuf[ub], 0, N * 8, st));  // the flow starts at zero
-    const size_t smem = (size_t)(kJTW + 2 * kJK) * (kJTH + 2 * kJK) * 32;
+    const size_t smem = (size_t)(kJTW + 2 * kJK) * (kJTH + 2 * kJK) * 36;
     for (int l = 0; l < L; l++) {
         const int lw = Wl[l], lh = Hl[l];
         const size_t lp = (size_t)lw * lh;

@@ -845,26 +845,6 @@ struct TbArgs {
     CUtensorMap tmW;  // (I1wx, I1wy, rho_c, grad): (2 nx, ny, pair) 8-byte elements
 };
 
-// Visits the inclusive rectangle [x0,x1] x [y0,y1] of a region of width RW
-// with NT threads, one pixel per step (one division per call).
-template <int NT, typename F>
-__device__ __forceinline__ void for_rect(int x0, int x1, int y0, int y1, F &&f) {
-    const int w = x1 - x0 + 1, n = w * (y1 - y0 + 1);
-    if (n <= 0) return;
-    const int t = threadIdx.x;
-    int rx = x0 + t % w, ry = y0 + t / w;
-    const int sx = NT % w, sy = NT / w;
-    for (int k = t; k < n; k += NT) {
-        f(rx, ry);
-        rx += sx;
-        ry += sy;
-        if (rx > x1) {
-            rx -= w;
-            ry += 1;
-        }
-    }
-}
-
 // One blocked iteration j (1-based) over the region.  Phase B (TH + u update)
 // covers [j, RW-j]^2 and phase C (dual update) [j, RW-1-j]^2: exactly the
 // pixels whose values reach the owned tile after K iterations, so no read
