@@ -389,7 +389,8 @@ def solver_measure(oflow, synth, np, torch, ctx, stream, dev, peak):
     per_pair = 320 * 240 * (200 * 28 + 24)
     epe = float(np.mean([synth.epe(o[0].cpu().numpy(), o[1].cpu().numpy(), g.u, g.v, g.valid, 8)
                          for o, g in zip(hs_out[:8], gen[:8])]))
-    out["hs_320x240"] = {"pairs_per_s": 64 / t, "achieved_gbs": 64 * per_pair / t / 1e9,
+    out["hs_320x240"] = {"pairs_per_s": 64 / t, "mpixels_per_s": 64 * 320 * 240 / t / 1e6,
+                         "achieved_gbs": 64 * per_pair / t / 1e9,
                          "frac": 64 * per_pair / t / 1e9 / peak, "epe_vs_ground_truth": round(epe, 4),
                          "jacobi_config_per_level": hs_cfg,
                          "pairs_per_s_untuned": 64 / t_fixed,
@@ -401,7 +402,8 @@ def solver_measure(oflow, synth, np, torch, ctx, stream, dev, peak):
     t = timed(lambda: oflow.pyrlk(a, b, lp, ctx, out=lo), 50)
     per_pair = 3 * (640 * 480 + 320 * 240 + 160 * 120) * 24
     epe = synth.epe(lo[0].cpu().numpy(), lo[1].cpu().numpy(), g.u, g.v, g.valid, 8)
-    out["pyrlk_640x480"] = {"pairs_per_s": 1 / t, "achieved_gbs": per_pair / t / 1e9,
+    out["pyrlk_640x480"] = {"pairs_per_s": 1 / t, "mpixels_per_s": 640 * 480 / t / 1e6,
+                            "achieved_gbs": per_pair / t / 1e9,
                             "frac": per_pair / t / 1e9 / peak, "epe_vs_ground_truth": round(float(epe), 4),
                             "config": "3 levels x 3 refinements, 5x5 window, one pair per call"}
     # the same configuration, 64 pairs per call (oflow_pyrlk_batch)
@@ -412,7 +414,8 @@ def solver_measure(oflow, synth, np, torch, ctx, stream, dev, peak):
     t = timed(lambda: oflow.pyrlk_batch(lk_in, lp, ctx, out=lk_out), 10)
     epe = float(np.mean([synth.epe(o[0].cpu().numpy(), o[1].cpu().numpy(), q.u, q.v, q.valid, 8)
                          for o, q in zip(lk_out[:8], gl[:8])]))
-    out["pyrlk_640x480_batch"] = {"pairs_per_s": nb / t, "achieved_gbs": nb * per_pair / t / 1e9,
+    out["pyrlk_640x480_batch"] = {"pairs_per_s": nb / t, "mpixels_per_s": nb * 640 * 480 / t / 1e6,
+                                  "achieved_gbs": nb * per_pair / t / 1e9,
                                   "frac": nb * per_pair / t / 1e9 / peak,
                                   "epe_vs_ground_truth": round(epe, 4),
                                   "config": "3 levels x 3 refinements, 5x5 window, 64 pairs per call"}
@@ -594,6 +597,8 @@ def our_arm(args, rank, world, local_rank):
         "e2e": {"value": world * P * e2e_steps / t_e2e, "unit": "pairs/s",
                 "h2d_bytes_per_step": P * 2 * W * H, "d2h_bytes_per_step": P * 2 * W * H * 4},
         "gpu_launches": args.steps * launches_per_step,
+        # frame-pair pixels solved per second (whole job), the Mpixel/s form of value
+        "mpixels_per_s": value * W * H / 1e6,
         "roofline": {"bound": "hbm", "kernel": "k_tvl1_q (inner iterations, finest scale)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
@@ -774,6 +779,7 @@ def batch_measure(ctx, dev, stream, steps, warmup, n_pairs, seed, max_over_ranks
     px = sum(w * h for (_, w, h, _) in specs)
     ach = alg * steps / t / 1e9
     return {"value": n * steps / t, "unit": "pairs/s", "ms_per_step": 1e3 * t / steps,
+            "mpixels_per_s": px * steps / t / 1e6,
             "steps": steps,
             "config": {"workload": "mixed batch (HS alpha 15, 1 level, 1 warp, 200 sweeps; "
                                    "TV-L1 5 scales x 5 warps x <=50)",
