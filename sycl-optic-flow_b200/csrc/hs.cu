@@ -272,20 +272,36 @@ void launch_upscale2(const float2 *src, size_t sstride, int w, int h, float2 *ds
     k_upscale2<<<g, blk, 0, st>>>(src, sstride, w, h, dst, dstride, nw, nh, sx, sy);
 }
 
+// Each thread converts four consecutive pixels of a row; rows whose source and destination allow it move them as one vector.
+constexpr int kTabPx = 4;
 template <typename T>
 __global__ void k_ingest_tab(const FrameRef *__restrict__ frames, int w, int h, float *dst,
                              size_t N) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int x = (blockIdx.x * blockDim.x + threadIdx.x) * kTabPx;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= w || y >= h) return;
     const FrameRef f = frames[blockIdx.z];
-    dst[(size_t)blockIdx.z * N + (size_t)y * w + x] =
-        (float)__ldg(static_cast<const T *>(f.p) + (size_t)y * f.pitch + x);
+    const T *src = static_cast<const T *>(f.p) + (size_t)y * f.pitch + x;
+    float *d = dst + (size_t)blockIdx.z * N + (size_t)y * w + x;
+    const bool vec = x + kTabPx <= w && reinterpret_cast<uintptr_t>(d) % 16 == 0 &&
+                     reinterpret_cast<uintptr_t>(src) % (kTabPx * sizeof(T)) == 0;
+    if (vec) {
+        float4 v;
+        if (sizeof(T) == 4) {
+            v = __ldg(reinterpret_cast<const float4 *>(src));
+        } else {
+            const uchar4 c = __ldg(reinterpret_cast<const uchar4 *>(src));
+            v = make_float4((float)c.x, (float)c.y, (float)c.z, (float)c.w);
+        }
+        *reinterpret_cast<float4 *>(d) = v;
+        return;
+    }
+    for (int k = 0; k < kTabPx && x + k < w; k++) d[k] = (float)__ldg(src + k);
 }
 
 void launch_ingest_tab(const FrameRef *frames, int dtype, int w, int h, float *dst, size_t N,
                        int planes, cudaStream_t st) {
-    dim3 blk(32, 8), g(div_up(w, 32), div_up(h, 8), planes);
+    dim3 blk(32, 8), g(div_up(w, 32 * kTabPx), div_up(h, 8), planes);
     if (dtype == OFLOW_U8)
         k_ingest_tab<uint8_t><<<g, blk, 0, st>>>(frames, w, h, dst, N);
     else
@@ -294,18 +310,32 @@ void launch_ingest_tab(const FrameRef *frames, int dtype, int w, int h, float *d
 
 __global__ void k_split_tab(const float2 *__restrict__ U, size_t stride, int w, int h,
                             const OutRef *__restrict__ outs) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int x = (blockIdx.x * blockDim.x + threadIdx.x) * kTabPx;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= w || y >= h) return;
     const OutRef o = outs[blockIdx.z];
-    const float2 u = U[(size_t)blockIdx.z * stride + (size_t)y * w + x];
-    o.u[(size_t)y * o.pitch + x] = u.x;
-    o.v[(size_t)y * o.pitch + x] = u.y;
+    const float2 *s = U + (size_t)blockIdx.z * stride + (size_t)y * w + x;
+    float *du = o.u + (size_t)y * o.pitch + x, *dv = o.v + (size_t)y * o.pitch + x;
+    const bool vec = x + kTabPx <= w &&
+                     ((reinterpret_cast<uintptr_t>(s) | reinterpret_cast<uintptr_t>(du) |
+                       reinterpret_cast<uintptr_t>(dv)) % 16 == 0);
+    if (vec) {
+        const float4 a = reinterpret_cast<const float4 *>(s)[0];
+        const float4 b = reinterpret_cast<const float4 *>(s)[1];
+        *reinterpret_cast<float4 *>(du) = make_float4(a.x, a.z, b.x, b.z);
+        *reinterpret_cast<float4 *>(dv) = make_float4(a.y, a.w, b.y, b.w);
+        return;
+    }
+    for (int k = 0; k < kTabPx && x + k < w; k++) {
+        const float2 u = s[k];
+        du[k] = u.x;
+        dv[k] = u.y;
+    }
 }
 
 void launch_split_tab(const float2 *U, size_t stride, int w, int h, const OutRef *outs, int B,
                       cudaStream_t st) {
-    dim3 blk(32, 8), g(div_up(w, 32), div_up(h, 8), B);
+    dim3 blk(32, 8), g(div_up(w, 32 * kTabPx), div_up(h, 8), B);
     k_split_tab<<<g, blk, 0, st>>>(U, stride, w, h, outs);
 }
 

@@ -77,7 +77,7 @@ __device__ __forceinline__ void lk_window_solve(const float *gx, const float *gy
 // temporal FIR over the ring, window sums and solve.  Pixels closer than the
 // window radius to the border get 0.
 __global__ void __launch_bounds__(kLNT) k_lk_step(const uint8_t *__restrict__ ring, int T,
-                                                  int iframe, int nx, int ny, LkTaps taps,
+                                                  int iframe, int nx, int ny, const __grid_constant__ LkTaps taps,
                                                   int c, float *Vx, float *Vy) {
     constexpr int RWm = kLTW + 2 * kLMaxC, RHm = kLTH + 2 * kLMaxC;
     constexpr int FWm = RWm + 2 * kLMaxF, FHm = RHm + 2 * kLMaxF;
@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(kLNT) k_lk_step(const uint8_t *__restrict__ ri
 
 // Spatial FIR (zero padding by dropped taps) of a float plane -> float2 (Ix, Iy).
 __global__ void k_lk_grad(const float *__restrict__ src, size_t sstride, int nx, int ny,
-                          LkTaps taps, float2 *G, size_t gstride) {
+                          const __grid_constant__ LkTaps taps, float2 *G, size_t gstride) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= nx || y >= ny) return;
