@@ -123,21 +123,45 @@ __global__ void __launch_bounds__(kLNT) k_lk_step(const uint8_t *__restrict__ ri
     Vy[(size_t)y * nx + x] = vy;
 }
 
-// Spatial FIR (zero padding by dropped taps) of a float plane -> float2 (Ix, Iy).
+// Spatial FIR (zero padding by dropped taps) of a float plane -> float2 (Ix, Iy),
+// NS taps at compile time (every tap added, the zero one too, as the
+// reference does); pixels at least NS/2 from every border skip the tests.
+template <int NS>
 __global__ void k_lk_grad(const float *__restrict__ src, size_t sstride, int nx, int ny,
                           const __grid_constant__ LkTaps taps, float2 *G, size_t gstride) {
+    constexpr int FC = (NS - 1) / 2;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= nx || y >= ny) return;
     const float *f = src + (size_t)blockIdx.z * sstride;
-    const int fc = (taps.ns - 1) / 2;
     float ax = 0.0f, ay = 0.0f;
-    for (int k = 0; k < taps.ns; k++) {
-        const int xx = x + k - fc, yy = y + k - fc;
-        if (xx >= 0 && xx < nx) ax += __ldg(f + (size_t)y * nx + xx) * taps.fs[k];
-        if (yy >= 0 && yy < ny) ay += __ldg(f + (size_t)yy * nx + x) * taps.fs[k];
+    if (x >= FC && x < nx - FC && y >= FC && y < ny - FC) {
+        const float *row = f + (size_t)y * nx + x - FC, *col = f + (size_t)(y - FC) * nx + x;
+#pragma unroll
+        for (int k = 0; k < NS; k++) {
+            ax += __ldg(row + k) * taps.fs[k];
+            ay += __ldg(col + (size_t)k * nx) * taps.fs[k];
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < NS; k++) {
+            const int xx = x + k - FC, yy = y + k - FC;
+            if (xx >= 0 && xx < nx) ax += __ldg(f + (size_t)y * nx + xx) * taps.fs[k];
+            if (yy >= 0 && yy < ny) ay += __ldg(f + (size_t)yy * nx + x) * taps.fs[k];
+        }
     }
     G[(size_t)blockIdx.z * gstride + (size_t)y * nx + x] = make_float2(ax, ay);
+}
+
+static void launch_lk_grad(dim3 g, dim3 blk, cudaStream_t st, const float *src, size_t sstride,
+                           int nx, int ny, const LkTaps &taps, float2 *G, size_t gstride) {
+    switch (taps.ns) {
+        case 1: k_lk_grad<1><<<g, blk, 0, st>>>(src, sstride, nx, ny, taps, G, gstride); break;
+        case 3: k_lk_grad<3><<<g, blk, 0, st>>>(src, sstride, nx, ny, taps, G, gstride); break;
+        case 5: k_lk_grad<5><<<g, blk, 0, st>>>(src, sstride, nx, ny, taps, G, gstride); break;
+        case 7: k_lk_grad<7><<<g, blk, 0, st>>>(src, sstride, nx, ny, taps, G, gstride); break;
+        default: k_lk_grad<9><<<g, blk, 0, st>>>(src, sstride, nx, ny, taps, G, gstride); break;
+    }
 }
 
 // Window sums and the 2x2 solve of P vertically adjacent pixels (column cidx,
@@ -367,7 +391,7 @@ void PyrLkPlan::record(cudaStream_t st) {
         const size_t lp = (size_t)lw * lh;
         dim3 blk(32, 8), g(div_up(lw, 32), div_up(lh, 8), B);
         // Ix, Iy of I0: plane 2b of the level, so a stride of two planes
-        k_lk_grad<<<g, blk, 0, st>>>(pyr + pyr_off_[l], 2 * lp, lw, lh, taps, G, N_);
+        launch_lk_grad(g, blk, st, pyr + pyr_off_[l], 2 * lp, lw, lh, taps, G, N_);
         dim3 ig(div_up(lw, kPTW), div_up(lh, kPTH), B);
         for (int r = 0; r < prm_.iters; r++) {
             launch_pyrlk_iter(c, ig, st, pyr + pyr_off_[l], lp, G, N_, U[cur], U[cur ^ 1], N_, lw, lh);
