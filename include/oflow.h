@@ -205,7 +205,8 @@ oflow_status oflow_hs_batch(oflow_ctx *ctx, int n, const oflow_image *I0,
 /* Autotuner for Horn-Schunck: solves the n given pairs (one size) once, then
  * times every Jacobi configuration (tile shape and sweeps per launch: 0 =
  * 32x16 tiles with 4 sweeps, 1 = 32x16 with 8, 2 = 64x32 with 8, 3 = 64x16
- * with 4, 4 = 32x32 with 16) at every pyramid level and keeps the fastest for
+ * with 4, 4 = 32x32 with 16, 5 = 64x32 with 4) at every pyramid level and
+ * keeps the fastest for
  * plans of this level size and batch (table entries with solver "hs", saved and
  * loaded with the TV-L1 ones).  cfg_per_level (OFLOW_MAX_SCALES ints, may be
  * NULL) receives the choice per level (coarsest first), -1 past the last.

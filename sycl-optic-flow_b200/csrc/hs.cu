@@ -354,8 +354,8 @@ struct HsJCfg {
     int tw, th, k, nt;
 };
 constexpr HsJCfg kHsCfgs[] = {{32, 16, 4, 256}, {32, 16, 8, 256}, {64, 32, 8, 512},
-                              {64, 16, 4, 256}, {32, 32, 16, 512}};
-constexpr int kHsNumCfgs = 5;
+                              {64, 16, 4, 256}, {32, 32, 16, 512}, {64, 32, 4, 512}};
+constexpr int kHsNumCfgs = 6;
 constexpr size_t hs_smem(const HsJCfg &c) { return (size_t)(c.tw + 2 * c.k) * (c.th + 2 * c.k) * 36; }
 
 template <int TW, int TH, int KH, int NT>
@@ -375,6 +375,7 @@ static void hs_jacobi_cfg(int c, dim3 g, cudaStream_t st, const float4 *D, size_
         case 2: hs_jacobi_launch<64, 32, 8, 512>(g, st, D, dstride, in, out, U, stride, w, h, sweeps, first, last, t); break;
         case 3: hs_jacobi_launch<64, 16, 4, 256>(g, st, D, dstride, in, out, U, stride, w, h, sweeps, first, last, t); break;
         case 4: hs_jacobi_launch<32, 32, 16, 512>(g, st, D, dstride, in, out, U, stride, w, h, sweeps, first, last, t); break;
+        case 5: hs_jacobi_launch<64, 32, 4, 512>(g, st, D, dstride, in, out, U, stride, w, h, sweeps, first, last, t); break;
         default: hs_jacobi_launch<32, 16, 4, 256>(g, st, D, dstride, in, out, U, stride, w, h, sweeps, first, last, t); break;
     }
 }
@@ -412,6 +413,8 @@ static void hs_set_smem_attrs() {
                                  (int)hs_smem(kHsCfgs[3])));
     OF_CUDA(cudaFuncSetAttribute(k_hs_jacobi<32, 32, 16, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)hs_smem(kHsCfgs[4])));
+    OF_CUDA(cudaFuncSetAttribute(k_hs_jacobi<64, 32, 4, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)hs_smem(kHsCfgs[5])));
 }
 
 // OFLOW_HS_CFG forces one configuration (used to test and time them); else

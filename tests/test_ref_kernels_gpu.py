@@ -139,7 +139,7 @@ def test_hs_solve_equals_reference_kernels(of, refg, ctx, alpha, L, nw, ns, w, h
     assert np.array_equal(u, ru) and np.array_equal(v, rv)
 
 
-@pytest.mark.parametrize("cfg", range(5))
+@pytest.mark.parametrize("cfg", range(6))
 def test_hs_every_jacobi_config_equals_reference_kernels(of, refg, monkeypatch, cfg):
     """Every Jacobi tiling of the library (tile shape, sweeps per launch)
     against the reference kernels: 37 sweeps, ragged tiles, two levels."""
