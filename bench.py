@@ -590,7 +590,8 @@ def our_arm(args, rank, world, local_rank):
         "config": {"workload": f"tvl1 1024x436, 5 scales x 5 warps x <=50 inner iterations, "
                                f"{P} uint8 pairs per GPU per step (plain TV-L1)",
                    "batch_pairs_per_gpu": P, "parallelism": f"independent pairs x{world}",
-                   "l2": f"inputs larger than L2 (per-step state ~{P * 0.052:.1f} GB)",
+                   "l2": f"inputs larger than L2 (finest-level u, p, warp data and coefficients "
+                         f"~{P * W * H * 136 / 1e9:.1f} GB)",
                    "inner_iterations_per_step": iters_total,
                    "tile_config_per_scale": tuned,
                    "epe_vs_ground_truth": round(epe, 5)},
