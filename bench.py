@@ -637,7 +637,8 @@ def once_other(args):
     of the 320x240 HS configuration (alpha 15, 200 sweeps); pyrlk: --batch
     pairs of the 640x480 pyramidal LK configuration; color: flowToColor of
     --batch 1024x436 flows; conv: the warm-start network's forward pass on
-    --batch 1024x436 pairs."""
+    --batch 1024x436 pairs; train: one training step of the network (forward,
+    backward, Adam) on --batch pairs, after two untimed ones."""
     import numpy as np
     import torch
     import oflow
@@ -666,7 +667,12 @@ def once_other(args):
         net.set_params(params)
         pairs = make_pairs(n, 0)
         fr = torch.from_numpy(np.stack([np.stack([a, b]) for a, b, _ in pairs])).to(dev)
-        net.predict(fr)
+        if args.once_solver == "conv":
+            net.predict(fr)
+        else:
+            tg = torch.zeros((n, net.out_h, net.out_w, 2), dtype=torch.float32, device=dev)
+            for _ in range(3):
+                net.train_step(fr, tg, 1e-6)
     torch.cuda.synchronize()
     log("done:", args.once_solver, n)
     return 0
@@ -858,7 +864,7 @@ def main():
     ap.add_argument("--cpu-worker", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--once", action="store_true",
                     help="one solve of --batch device-resident pairs and exit (profiling case)")
-    ap.add_argument("--once-solver", choices=["tvl1", "hs", "pyrlk", "color", "conv"],
+    ap.add_argument("--once-solver", choices=["tvl1", "hs", "pyrlk", "color", "conv", "train"],
                     default="tvl1", help="kernel family of the --once profiling case")
     ap.add_argument("--nscales", type=int, default=PARAMS["nscales"])
     ap.add_argument("--iters", type=int, default=PARAMS["max_iterations"])

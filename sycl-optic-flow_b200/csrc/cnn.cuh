@@ -53,7 +53,9 @@ bool conv_forward_umma(const ConvDims &d, const __nv_bfloat16 *x, const __nv_bfl
 size_t conv_backward_data_umma_scratch(const ConvDims &d);
 // backward-weight on the tcgen05 kernel (transposing gathers, reduction over
 // output pixels split across CTAs, atomics into gw); gw and gb are
-// overwritten.  scratch: the same size as for backward-data.  false (nothing
+// overwritten; for K % 4 == 0 the bias gradient is a fixed-order sum of
+// per-block partial sums made in the pass that masks the gradient.  scratch:
+// the same size as for backward-data.  false (nothing
 // launched) when K > 128, C is not a multiple of 16 or x is not 16-byte aligned.
 bool conv_backward_weight_umma(const ConvDims &d, const float *g, const __nv_bfloat16 *y_act,
                                const __nv_bfloat16 *x, float *gw, float *gb, void *scratch,
@@ -61,9 +63,11 @@ bool conv_backward_weight_umma(const ConvDims &d, const float *g, const __nv_bfl
 // bias gradient alone: gb[k] = sum over output pixels of the masked gradient
 void conv_bias_grad(const ConvDims &d, const float *g, const __nv_bfloat16 *y_act, float *gb,
                     cudaStream_t st);
+// g_masked: scratch already holds the masked bf16 gradient (the backward-weight
+// product on the same scratch and gradient wrote it), so it is not made again.
 bool conv_backward_data_umma(const ConvDims &d, const float *g, const __nv_bfloat16 *y_act,
                              const __nv_bfloat16 *w, float *gin, bool accumulate, void *scratch,
-                             int *err, cudaStream_t st);
+                             int *err, cudaStream_t st, bool g_masked = false);
 // backward-data: g f32 [N,P,Q,K] (masked by y_act > 0 when y_act != null,
 // y_act bf16 [N,P,Q,K]) -> gin f32 [N,H,W,C]; accumulate adds to gin.
 void conv_backward_data(const ConvDims &d, const float *g, const __nv_bfloat16 *y_act,

@@ -313,43 +313,52 @@ bool dispatch_np(int np, const ConvDims &d, const __nv_bfloat16 *x, const __nv_b
 }
 
 // Backward-weight product on the tensor cores:
-//   gw[k][tap][c] += sum_m g[m][k] * x[pixel(m, tap)][c]
-// as a GEMM with M = the layer's output channels k (up to 128 rows), N = NP
-// input channels of one tap, and the reduction over output pixels m, 16 per
-// stage (one 128 x NP x 16 MMA).  The operands are gathered transposed into
-// the same no-swizzle K-major layout as the forward kernel: thread t packs
-// row t of A (the masked bf16 gradient of channel k = t at the stage's 16
-// pixels) and row t of B (channel c0 + t of the tap-shifted input at those
-// pixels) into two 16-byte chunks each.  A CTA reduces a range of pixels and
-// adds its 128 x NP tile to gw with atomics (gridDim.y splits the pixels,
-// gridDim.x runs over (tap, channel chunk)).  Same pipeline and bounded
-// waits as the forward kernel.
-template <int NP>
-__global__ void __launch_bounds__(kUmNT) k_conv_wgrad_umma(ConvDims d, const __nv_bfloat16 *__restrict__ gb,
-                                                           const __nv_bfloat16 *__restrict__ x, float *gw,
-                                                           int pix_per_cta, int *err) {
-    static_assert(NP % 16 == 0 && NP >= 16 && NP <= 128, "N = 16..128, step 16");
-    constexpr int A_BYTES = kUmBM * 16 * 2;
-    constexpr int STAGE = (kUmBM + NP) * 16 * 2;
-    constexpr uint32_t TCOLS = tmem_cols<NP>();
-    constexpr uint32_t IDESC = umma_idesc_bf16(kUmBM, NP);
+//   gw[k][tap][c] = sum_m x[pixel(m, tap)][c] * g[m][k]
+// as D = A B with the rows of D the (tap, c) pairs of the layer (9C rows, in
+// 128-row UMMA tiles, row = tap * C + c), its columns the output channels k
+// (K rounded up to 16 = KP) and the reduction over output pixels m, 32 per
+// stage.  Both operands are read in the layout they have in memory and
+// staged MN-major (no swizzle): a core matrix is 8 reduction rows (pixels) of
+// 16 bytes, each 16 bytes being 8 consecutive (tap, c) rows of A -- the
+// channels c..c+7 of one input pixel -- or 8 consecutive output channels of B
+// -- g[m][k..k+7].  So every gather is one 16-byte cp.async of NHWC memory,
+// with no transposition.  In a stage, core matrices along the reduction are
+// 128 bytes apart (LBO) and groups of 8 rows 512 bytes apart (SBO); tile t of
+// A starts t * 8 KB into the stage.  A CTA owns up to kWgMT tiles of rows
+// (gridDim.x runs over groups of tiles), shares each stage's gradient tile
+// between them, reduces a range of pixels (gridDim.y splits the pixels) and
+// adds its rows to gw with atomics.  Pipeline, commits and bounded waits as in
+// the forward kernel.
+constexpr int kWgMT = 4;       // row tiles a CTA at most
+constexpr int kWgPix = 32;     // pixels a stage
+constexpr int kWgTile = kUmBM * kWgPix * 2;  // bytes of one row tile a stage
+
+template <int KP>
+__global__ void __launch_bounds__(kUmNT) k_conv_wgrad_mn(ConvDims d, const __nv_bfloat16 *__restrict__ gb,
+                                                         const __nv_bfloat16 *__restrict__ x, float *gw,
+                                                         int ntg, int pix_per_cta, uint32_t tcols, int *err) {
+    static_assert(KP % 16 == 0 && KP >= 16 && KP <= 128, "N = 16..128, step 16");
+    constexpr uint32_t IDESC = umma_idesc_bf16(kUmBM, KP) | (1u << 15) | (1u << 16);  // A, B MN-major
+    constexpr int B_BYTES = KP * kWgPix * 2;
     extern __shared__ __align__(1024) uint8_t um_smem[];
     __shared__ __align__(8) uint64_t mbar[kUmStages];
     __shared__ uint32_t tmem_base;
-    __shared__ long long s_ga[kUmStages][16], s_xa[kUmStages][16];  // element offsets, -1: zero
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int M = d.N * d.P * d.Q;
-    const int nchunk = d.C / NP;
-    const int tap = blockIdx.x / nchunk, c0 = (blockIdx.x % nchunk) * NP;
+    const int rows = 9 * d.C;
+    const int tiles = div_up(rows, kUmBM);
+    const int t0 = blockIdx.x * ntg;                 // first row tile of this CTA
+    const int nt = imin(ntg, tiles - t0);            // row tiles of this CTA
+    const int stage_bytes = ntg * kWgTile + B_BYTES;
     const int m_lo = blockIdx.y * pix_per_cta;
     const int m_hi = imin(M, m_lo + pix_per_cta);
-    const int nst = m_hi > m_lo ? div_up(m_hi - m_lo, 16) : 0;
+    const int nst = m_hi > m_lo ? div_up(m_hi - m_lo, kWgPix) : 0;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                          smem_u32(&tmem_base)),
-                     "r"(TCOLS)
+                     "r"(tcols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
     }
@@ -363,76 +372,95 @@ __global__ void __launch_bounds__(kUmNT) k_conv_wgrad_umma(ConvDims d, const __n
     const uint32_t tmem = tmem_base;
     const uint32_t sbase = smem_u32(um_smem);
 
-    // offsets of stage s's 16 pixels: gradient row m*K, input pixel of the tap
-    auto offsets = [&](int s) {
-        if (tid < 16) {
-            const int m = m_lo + s * 16 + tid;
-            long long ga = -1, xa = -1;
-            if (m < m_hi) {
-                const int q = m % d.Q, t = m / d.Q, p = t % d.P, n = t / d.P;
-                ga = (long long)m * d.K;
-                const int yy = p * d.stride + tap / 3 - 1, xx = q * d.stride + tap % 3 - 1;
-                if (yy >= 0 && yy < d.H && xx >= 0 && xx < d.W)
-                    xa = (((long long)n * d.H + yy) * d.W + xx) * d.C + c0;
-            }
-            s_ga[s % kUmStages][tid] = ga;
-            s_xa[s % kUmStages][tid] = xa;
+    // This thread gathers pixel j = 8 warp + (lane & 7) of every stage, for the
+    // 8-row groups g = 4 i + (lane >> 3) of A and the channel groups
+    // kg = 4 i + (lane >> 3) of B.  Row group g: tap, first channel, and the
+    // element offset of its 8 channels from the tap's centre pixel.
+    const int j = warp * 8 + (lane & 7), gs = lane >> 3;
+    int toff[kWgMT * 4], tap_rs[kWgMT * 4];
+#pragma unroll
+    for (int i = 0; i < kWgMT * 4; i++) {
+        const int R = (t0 * 16 + 4 * i + gs) * 8;  // first row of the group
+        if (i < nt * 4 && R < rows) {
+            const int tap = R / d.C, c = R % d.C, r = tap / 3, sx = tap % 3;
+            toff[i] = (r * d.W + sx) * d.C + c;
+            tap_rs[i] = r | (sx << 2);
+        } else {
+            toff[i] = 0;
+            tap_rs[i] = -1;
         }
-    };
-    // rows of A (channel k = tid) and B (channel c0 + tid) of stage s,
-    // transposed into 8-element K-major chunks
+    }
+    const uint32_t jo = (uint32_t)((j >> 3) * 128 + (j & 7) * 16);
+
     auto gather = [&](int s) {
-        const int buf = s % kUmStages;
-        const uint32_t a = sbase + buf * STAGE, b = a + A_BYTES;
-        const unsigned short *G = reinterpret_cast<const unsigned short *>(gb);
-        const unsigned short *X = reinterpret_cast<const unsigned short *>(x);
+        const uint32_t a = sbase + (s % kUmStages) * stage_bytes;
+        const uint32_t b = a + ntg * kWgTile;
+        const int m = m_lo + s * kWgPix + j;
+        const bool mv = m < m_hi;
+        int y0 = 0, x0 = 0;
+        long long pbase = 0;
+        if (mv) {
+            const int q = m % d.Q, t = m / d.Q, p = t % d.P, n = t / d.P;
+            y0 = p * d.stride - 1;
+            x0 = q * d.stride - 1;
+            pbase = (((long long)n * d.H + y0) * d.W + x0) * d.C;
+        }
 #pragma unroll
-        for (int kc = 0; kc < 2; kc++) {
-            uint32_t pa[4], pb[4];
-#pragma unroll
-            for (int e = 0; e < 4; e++) {
-                uint32_t va[2], vb[2];
-#pragma unroll
-                for (int h = 0; h < 2; h++) {
-                    const int j = kc * 8 + e * 2 + h;
-                    const long long ga = s_ga[buf][j], xa = s_xa[buf][j];
-                    va[h] = (ga >= 0 && tid < d.K) ? G[ga + tid] : 0u;
-                    vb[h] = (xa >= 0 && tid < NP) ? X[xa + tid] : 0u;
-                }
-                pa[e] = va[0] | (va[1] << 16);
-                pb[e] = vb[0] | (vb[1] << 16);
+        for (int i = 0; i < kWgMT * 4; i++) {
+            if (i < nt * 4) {
+                const int rs = tap_rs[i];
+                const bool ok = mv && rs >= 0 && (unsigned)(y0 + (rs & 3)) < (unsigned)d.H &&
+                                (unsigned)(x0 + (rs >> 2)) < (unsigned)d.W;
+                cp_async16(a + (uint32_t)(4 * i + gs) * 512 + jo, ok ? x + pbase + toff[i] : x, ok);
             }
-            asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};\n" ::"r"(a + kc * (kUmBM * 16) + tid * 16),
-                         "r"(pa[0]), "r"(pa[1]), "r"(pa[2]), "r"(pa[3])
-                         : "memory");
-            if (tid < NP)
-                asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};\n" ::"r"(b + kc * (NP * 16) + tid * 16),
-                             "r"(pb[0]), "r"(pb[1]), "r"(pb[2]), "r"(pb[3])
-                             : "memory");
+        }
+#pragma unroll
+        for (int i = 0; i < (KP / 8 + 3) / 4; i++) {
+            const int kg = 4 * i + gs;
+            if (kg < KP / 8) {
+                const bool ok = mv && kg * 8 < d.K;
+                cp_async16(b + (uint32_t)kg * 512 + jo, ok ? gb + (size_t)m * d.K + kg * 8 : gb, ok);
+            }
         }
     };
 
+    // one cp.async group per stage (empty past the last), so waiting until
+    // kUmAhead groups are pending means stage s has landed
     bool timed_out = false;
 #pragma unroll 1
+    for (int s = 0; s < kUmAhead; s++) {
+        if (s < nst) gather(s);
+        cp_async_commit();
+    }
+#pragma unroll 1
     for (int s = 0; s < nst; s++) {
-        // buffer s % 4 last held stage s - 4: its MMA must be done
-        if (s >= kUmStages && !timed_out) {
-            const int so = s - kUmStages;
-            if (!mbar_wait_bounded(smem_u32(&mbar[so % kUmStages]), (so / kUmStages) & 1))
-                timed_out = true;
+        const int sl = s + kUmAhead;
+        if (sl < nst) {
+            // buffer sl % 4 last held stage sl - 4 = s - 2, committed two stages ago
+            if (sl >= kUmStages && !timed_out) {
+                const int so = sl - kUmStages;
+                if (!mbar_wait_bounded(smem_u32(&mbar[so % kUmStages]), (so / kUmStages) & 1))
+                    timed_out = true;
+            }
+            gather(sl);
         }
-        offsets(s);
-        __syncthreads();
-        gather(s);
+        cp_async_commit();
+        cp_async_wait<kUmAhead>();
         fence_async_smem();
         __syncthreads();
         if (tid == 0) {
             tc_fence_after();
             const int buf = s % kUmStages;
-            const uint32_t a = sbase + buf * STAGE, b = a + A_BYTES;
-            const uint64_t ad = umma_desc(a, kUmBM * 16, 128);
-            const uint64_t bd = umma_desc(b, NP * 16, 128);
-            umma_bf16(tmem, ad, bd, IDESC, s > 0 ? 1u : 0u);
+            const uint32_t a = sbase + buf * stage_bytes, b = a + ntg * kWgTile;
+#pragma unroll 1
+            for (int t = 0; t < nt; t++) {
+#pragma unroll
+                for (int h = 0; h < kWgPix / 16; h++) {
+                    const uint64_t ad = umma_desc(a + t * kWgTile + h * 256, 128, 512);
+                    const uint64_t bd = umma_desc(b + h * 256, 128, 512);
+                    umma_bf16(tmem + (uint32_t)(t * KP), ad, bd, IDESC, (s > 0 || h > 0) ? 1u : 0u);
+                }
+            }
             umma_commit(smem_u32(&mbar[buf]));
         }
     }
@@ -441,39 +469,51 @@ __global__ void __launch_bounds__(kUmNT) k_conv_wgrad_umma(ConvDims d, const __n
         if (!timed_out && !mbar_wait_bounded(smem_u32(&mbar[sL % kUmStages]), (sL / kUmStages) & 1))
             timed_out = true;
     }
+    cp_async_wait<0>();
     timed_out = __syncthreads_or(timed_out);
     if (timed_out && tid == 0) atomicOr(err, 1);
     tc_fence_after();
     if (!timed_out && nst > 0) {
-        const int k = warp * 32 + lane;  // TMEM lane = output channel
 #pragma unroll 1
-        for (int cc = 0; cc < NP; cc += 16) {
-            uint32_t r[16];
-            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cc, r);
-            if (k >= d.K) continue;
-            float *o = gw + ((size_t)k * 9 + tap) * d.C + c0 + cc;
+        for (int t = 0; t < nt; t++) {
+            const int R = (t0 + t) * kUmBM + warp * 32 + lane;  // TMEM lane = row of D
+            const bool rv = R < rows;
+            const int tap = rv ? R / d.C : 0, c = rv ? R % d.C : 0;
+#pragma unroll 1
+            for (int cc = 0; cc < KP; cc += 16) {
+                uint32_t r[16];
+                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(t * KP + cc), r);
+                if (!rv) continue;
 #pragma unroll
-            for (int j = 0; j < 16; j++) atomicAdd(o + j, __uint_as_float(r[j]));
+                for (int e = 0; e < 16; e++)
+                    if (cc + e < d.K) atomicAdd(gw + ((size_t)(cc + e) * 9 + tap) * d.C + c, __uint_as_float(r[e]));
+            }
         }
     }
     tc_fence_before();
     __syncthreads();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(tcols)
                      : "memory");
 }
 
-template <int NP>
+template <int KP>
 void launch_wgrad(const ConvDims &d, const __nv_bfloat16 *gb, const __nv_bfloat16 *x, float *gw,
                   int *err, cudaStream_t st) {
-    constexpr int smem = kUmStages * (kUmBM + NP) * 16 * 2;
-    OF_CUDA(cudaFuncSetAttribute(k_conv_wgrad_umma<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int M = d.N * d.P * d.Q;
-    const int nx = 9 * (d.C / NP);
-    // enough CTAs to fill the GPU a few times over, at least 256 pixels each
-    const int splits = imax(1, imin(div_up(M, 256), div_up(4 * kNumSMs * 8, nx)));
-    const int per = div_up(div_up(M, splits), 16) * 16;
-    k_conv_wgrad_umma<NP><<<dim3(nx, div_up(M, per)), kUmNT, smem, st>>>(d, gb, x, gw, per, err);
+    if (M <= 0) return;
+    const int tiles = div_up(9 * d.C, kUmBM);
+    const int groups = div_up(tiles, kWgMT);
+    const int ntg = div_up(tiles, groups);  // row tiles a CTA, balanced over the groups
+    const int smem = kUmStages * (ntg * kWgTile + KP * kWgPix * 2);
+    uint32_t tcols = 32;
+    while (tcols < (uint32_t)(ntg * KP)) tcols <<= 1;
+    OF_CUDA(cudaFuncSetAttribute(k_conv_wgrad_mn<KP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    // CTAs an SM holds by shared memory and tensor memory; one wave of them
+    const int occ = imax(1, imin((227 * 1024) / (smem + 1024), (int)(512 / tcols)));
+    const int splits = imax(1, imin(div_up(M, kWgPix), div_up(kNumSMs * occ, groups)));
+    const int per = div_up(div_up(M, splits), kWgPix) * kWgPix;
+    k_conv_wgrad_mn<KP><<<dim3(groups, div_up(M, per)), kUmNT, smem, st>>>(d, gb, x, gw, ntg, per, tcols, err);
 }
 
 // bf16 copy of the output gradient, zero where the layer's ReLU was inactive
@@ -486,6 +526,83 @@ __global__ void k_mask_bf16(const float *__restrict__ g, const __nv_bfloat16 *__
         if (yact && !(__bfloat162float(yact[i]) > 0.0f)) v = 0.0f;
         out[i] = __float2bfloat16(v);
     }
+}
+
+// The same masked bf16 copy fused with the bias gradient's first stage, for
+// K % 4 == 0 (K <= 128): block b covers the gradient rows (output pixels)
+// [b * rpb, (b + 1) * rpb); a thread keeps four adjacent channels (one float4
+// of a row) and walks R = 256 / (K / 4) rows apart, so each step of the block
+// reads whole rows.  The per-thread sums then go, in a fixed order, to one
+// partial sum per channel and block: partial[b * K + k].
+constexpr int kBiasBlocks = 4 * kNumSMs;
+constexpr int kBiasFinalNT = 256;
+
+// Scratch of the backward products, in bytes from its start: the masked bf16
+// gradient, the rotated weights (each rounded up to 64 elements, 128-byte
+// aligned), then the bias partial sums (kBiasBlocks x K floats).
+size_t bwd_scratch_part(const ConvDims &d) {
+    const size_t g = (size_t)d.N * d.P * d.Q * d.K, wt = (size_t)d.K * 9 * d.C;
+    return ((g + 63) / 64 * 64 + (wt + 63) / 64 * 64) * sizeof(__nv_bfloat16);
+}
+
+__global__ void __launch_bounds__(256) k_mask_bias(const float *__restrict__ g,
+                                                   const __nv_bfloat16 *__restrict__ yact,
+                                                   __nv_bfloat16 *__restrict__ out, int M, int K,
+                                                   int rpb, float *__restrict__ partial) {
+    __shared__ float4 sh[256];
+    const int Q = K >> 2, R = 256 / Q, t = threadIdx.x;
+    const int q = t % Q, ro = t / Q;
+    float4 s = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (ro < R) {
+        const int r0 = blockIdx.x * rpb, r1 = imin(r0 + rpb, M);
+        for (int r = r0 + ro; r < r1; r += R) {
+            const size_t i = (size_t)r * K + 4 * q;
+            float4 v = __ldg(reinterpret_cast<const float4 *>(g + i));
+            if (yact) {
+                const uint2 a = __ldg(reinterpret_cast<const uint2 *>(yact + i));
+                const __nv_bfloat162 a01 = *reinterpret_cast<const __nv_bfloat162 *>(&a.x);
+                const __nv_bfloat162 a23 = *reinterpret_cast<const __nv_bfloat162 *>(&a.y);
+                if (!(__low2float(a01) > 0.0f)) v.x = 0.0f;
+                if (!(__high2float(a01) > 0.0f)) v.y = 0.0f;
+                if (!(__low2float(a23) > 0.0f)) v.z = 0.0f;
+                if (!(__high2float(a23) > 0.0f)) v.w = 0.0f;
+            }
+            s.x += v.x;
+            s.y += v.y;
+            s.z += v.z;
+            s.w += v.w;
+            const __nv_bfloat162 o01 = __floats2bfloat162_rn(v.x, v.y);
+            const __nv_bfloat162 o23 = __floats2bfloat162_rn(v.z, v.w);
+            uint2 o;
+            o.x = *reinterpret_cast<const uint32_t *>(&o01);
+            o.y = *reinterpret_cast<const uint32_t *>(&o23);
+            *reinterpret_cast<uint2 *>(out + i) = o;
+        }
+    }
+    sh[t] = s;
+    __syncthreads();
+    if (t < K) {
+        const int qq = t >> 2, e = t & 3;
+        float acc = 0.0f;
+        for (int j = 0; j < R; j++) {
+            const float4 w = sh[j * Q + qq];
+            acc += e == 0 ? w.x : e == 1 ? w.y : e == 2 ? w.z : w.w;
+        }
+        partial[(size_t)blockIdx.x * K + t] = acc;
+    }
+}
+
+// gb[k] = the sum of the nb partial sums of channel k, one block a channel:
+// thread t adds blocks t, t + NT, ... in order, then a fixed tree adds the
+// threads' sums.
+__global__ void __launch_bounds__(kBiasFinalNT) k_bias_final(const float *__restrict__ partial,
+                                                             int nb, int K, float *gb) {
+    __shared__ double scratch[kBiasFinalNT / 32];
+    const int k = blockIdx.x;
+    float acc = 0.0f;
+    for (int b = threadIdx.x; b < nb; b += kBiasFinalNT) acc += __ldg(partial + (size_t)b * K + k);
+    const double r = block_sum_double<kBiasFinalNT>((double)acc, scratch);
+    if (threadIdx.x == 0) gb[k] = (float)r;
 }
 
 // wt[c][tap][k] = w[k][8 - tap][c]: the weights of the backward-data product
@@ -519,44 +636,54 @@ bool conv_forward_umma(const ConvDims &d, const __nv_bfloat16 *x, const __nv_bfl
 bool conv_backward_weight_umma(const ConvDims &d, const float *g, const __nv_bfloat16 *y_act,
                                const __nv_bfloat16 *x, float *gw, float *gb, void *scratch,
                                int *err, cudaStream_t st) {
-    if (d.K > 128 || d.C % 16 != 0) return false;
-    int np = 0;  // the widest channel chunk that divides C
-    for (int c : {128, 96, 64, 48, 32, 16})
-        if (d.C % c == 0) {
-            np = c;
-            break;
-        }
-    if (!np || (reinterpret_cast<uintptr_t>(x) & 15u) != 0) return false;
+    if (d.K > 128 || d.K % 8 != 0 || d.C % 16 != 0) return false;
+    if ((reinterpret_cast<uintptr_t>(x) & 15u) != 0 || (reinterpret_cast<uintptr_t>(scratch) & 15u) != 0)
+        return false;
     const size_t ng = (size_t)d.N * d.P * d.Q * d.K;
     __nv_bfloat16 *gbf = static_cast<__nv_bfloat16 *>(scratch);
-    k_mask_bf16<<<imin((int)((ng + 255) / 256), 4096), 256, 0, st>>>(g, y_act, gbf, ng);
-    OF_CUDA(cudaMemsetAsync(gw, 0, sizeof(float) * (size_t)d.K * 9 * d.C, st));
-    switch (np) {
-        case 128: launch_wgrad<128>(d, gbf, x, gw, err, st); break;
-        case 96: launch_wgrad<96>(d, gbf, x, gw, err, st); break;
-        case 64: launch_wgrad<64>(d, gbf, x, gw, err, st); break;
-        case 48: launch_wgrad<48>(d, gbf, x, gw, err, st); break;
-        case 32: launch_wgrad<32>(d, gbf, x, gw, err, st); break;
-        default: launch_wgrad<16>(d, gbf, x, gw, err, st); break;
+    // the masked bf16 copy and the bias gradient in one pass over g where the
+    // channels split into float4 quads
+    const int M = d.N * d.P * d.Q;
+    const bool fused = M > 0 && d.K % 4 == 0 && (reinterpret_cast<uintptr_t>(g) & 15u) == 0 &&
+                       (y_act == nullptr || (reinterpret_cast<uintptr_t>(y_act) & 7u) == 0);
+    if (fused) {
+        const int R = 256 / (d.K / 4);
+        const int rpb = div_up(div_up(M, imin(kBiasBlocks, imax(1, div_up(M, 4 * R)))), R) * R;
+        const int nb = div_up(M, rpb);
+        float *part = reinterpret_cast<float *>(static_cast<char *>(scratch) + bwd_scratch_part(d));
+        k_mask_bias<<<nb, 256, 0, st>>>(g, y_act, gbf, M, d.K, rpb, part);
+        k_bias_final<<<d.K, kBiasFinalNT, 0, st>>>(part, nb, d.K, gb);
+    } else {
+        k_mask_bf16<<<imin((int)((ng + 255) / 256), 4096), 256, 0, st>>>(g, y_act, gbf, ng);
     }
-    conv_bias_grad(d, g, y_act, gb, st);
+    OF_CUDA(cudaMemsetAsync(gw, 0, sizeof(float) * (size_t)d.K * 9 * d.C, st));
+    switch ((d.K + 15) / 16 * 16) {
+        case 16: launch_wgrad<16>(d, gbf, x, gw, err, st); break;
+        case 32: launch_wgrad<32>(d, gbf, x, gw, err, st); break;
+        case 48: launch_wgrad<48>(d, gbf, x, gw, err, st); break;
+        case 64: launch_wgrad<64>(d, gbf, x, gw, err, st); break;
+        case 80: launch_wgrad<80>(d, gbf, x, gw, err, st); break;
+        case 96: launch_wgrad<96>(d, gbf, x, gw, err, st); break;
+        case 112: launch_wgrad<112>(d, gbf, x, gw, err, st); break;
+        default: launch_wgrad<128>(d, gbf, x, gw, err, st); break;
+    }
+    if (!fused) conv_bias_grad(d, g, y_act, gb, st);
     return true;
 }
 
 size_t conv_backward_data_umma_scratch(const ConvDims &d) {
-    const size_t g = (size_t)d.N * d.P * d.Q * d.K, wt = (size_t)d.K * 9 * d.C;
-    return (g + wt + 64) * sizeof(__nv_bfloat16);
+    return bwd_scratch_part(d) + sizeof(float) * kBiasBlocks * (size_t)d.K;
 }
 
 bool conv_backward_data_umma(const ConvDims &d, const float *g, const __nv_bfloat16 *y_act,
                              const __nv_bfloat16 *w, float *gin, bool accumulate, void *scratch,
-                             int *err, cudaStream_t st) {
+                             int *err, cudaStream_t st, bool g_masked) {
     if (d.K % 16 != 0 || d.C % 16 != 0) return false;
     if ((reinterpret_cast<uintptr_t>(gin) & 15u) != 0) return false;
     const size_t ng = (size_t)d.N * d.P * d.Q * d.K;
     __nv_bfloat16 *gb = static_cast<__nv_bfloat16 *>(scratch);
     __nv_bfloat16 *wt = gb + (ng + 63) / 64 * 64;  // 128-byte aligned
-    k_mask_bf16<<<imin((int)((ng + 255) / 256), 4096), 256, 0, st>>>(g, y_act, gb, ng);
+    if (!g_masked) k_mask_bf16<<<imin((int)((ng + 255) / 256), 4096), 256, 0, st>>>(g, y_act, gb, ng);
     k_flip_weights<<<imin(div_up(d.K * 9 * d.C, 256), 1024), 256, 0, st>>>(w, d.K, d.C, wt);
     // the product as a forward convolution over the output gradient: input
     // (N, P, Q, K), output (N, H, W, C); stride 2 layers read a dilated input

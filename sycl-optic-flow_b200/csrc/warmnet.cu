@@ -151,11 +151,15 @@ double WarmNet::train_step(const void *frames, int dtype, size_t pair_stride, co
         const __nv_bfloat16 *yact = yact_t >= 0 ? A(yact_t) : nullptr;
         // both backward products on the tensor-core kernels where the shape
         // allows (OFLOW_CNN_BWD_MMA=1 keeps them on the mma.sync kernel, to compare)
-        if (bwd_mma_ || !conv_backward_weight_umma(d, g, yact, A(x_t), gp + woff_[l], gp + boff_[l],
-                                                   ar_.at<char>(o_bwd_), ar_.at<int>(o_err_), st))
-            conv_backward_weight(d, g, yact, A(x_t), gp + woff_[l], gp + boff_[l], st);
+        const bool wg = !bwd_mma_ && conv_backward_weight_umma(d, g, yact, A(x_t), gp + woff_[l],
+                                                               gp + boff_[l], ar_.at<char>(o_bwd_),
+                                                               ar_.at<int>(o_err_), st);
+        if (!wg) conv_backward_weight(d, g, yact, A(x_t), gp + woff_[l], gp + boff_[l], st);
+        // the tensor-core backward-weight product left the masked bf16
+        // gradient at the start of the shared scratch
         if (gin && (bwd_mma_ || !conv_backward_data_umma(d, g, yact, W + woff_[l], gin, acc,
-                                                          ar_.at<char>(o_bwd_), ar_.at<int>(o_err_), st)))
+                                                          ar_.at<char>(o_bwd_), ar_.at<int>(o_err_), st,
+                                                          wg)))
             conv_backward_data(d, g, yact, W + woff_[l], gin, acc, st);
     };
     back(9, ar_.at<float>(o_gout_), -1, 11, G(11), false);  // c10: -> g(c9)
