@@ -279,30 +279,44 @@ void upcat_backward(const float *g, int H, int W, int Ca, int Cb, int N, float *
 template <typename T>
 __global__ void k_cnn_input(const T *frames, int w, int h, int N, size_t pair_stride,
                             __nv_bfloat16 *x0) {
+    // one output row (pair n, half-resolution row y) per block step; a
+    // pixel's 16 channels (32 bytes) leave as two 16-byte stores
     const int w2 = (w + 1) / 2, h2 = (h + 1) / 2;
-    const size_t total = (size_t)N * w2 * h2;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-         i += (size_t)gridDim.x * blockDim.x) {
-        const int x = (int)(i % w2), y = (int)((i / w2) % h2), n = (int)(i / ((size_t)w2 * h2));
-        const int xa = 2 * x, xb = imin(2 * x + 1, w - 1), ya = 2 * y, yb = imin(2 * y + 1, h - 1);
-        __nv_bfloat16 *o = x0 + i * 16;
-        float m[2];
-        for (int k = 0; k < 2; k++) {
-            const T *f = frames + pair_stride * (2 * n + k);
-            const float s = (float)f[(size_t)ya * w + xa] + (float)f[(size_t)ya * w + xb] +
-                            (float)f[(size_t)yb * w + xa] + (float)f[(size_t)yb * w + xb];
-            m[k] = s * (0.25f / 255.0f);
-            o[k] = __float2bfloat16(m[k] - 0.5f);
+    const int rows = N * h2;
+    for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+        const int n = row / h2, y = row - n * h2;
+        const int ya = 2 * y, yb = imin(2 * y + 1, h - 1);
+        const T *f0 = frames + pair_stride * (2 * (size_t)n);
+        const T *f1 = frames + pair_stride * (2 * (size_t)n + 1);
+        for (int x = threadIdx.x; x < w2; x += blockDim.x) {
+            const int xa = 2 * x, xb = imin(2 * x + 1, w - 1);
+            float m[2];
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                const T *f = k ? f1 : f0;
+                const float s = (float)f[(size_t)ya * w + xa] + (float)f[(size_t)ya * w + xb] +
+                                (float)f[(size_t)yb * w + xa] + (float)f[(size_t)yb * w + xb];
+                m[k] = s * (0.25f / 255.0f);
+            }
+            const __nv_bfloat162 c01 = __floats2bfloat162_rn(m[0] - 0.5f, m[1] - 0.5f);
+            const __nv_bfloat162 c23 = __floats2bfloat162_rn(4.0f * (m[1] - m[0]), 0.0f);
+            uint4 lo;
+            lo.x = *reinterpret_cast<const uint32_t *>(&c01);
+            lo.y = *reinterpret_cast<const uint32_t *>(&c23);
+            lo.z = 0u;
+            lo.w = 0u;
+            uint4 *o = reinterpret_cast<uint4 *>(x0 + ((size_t)row * w2 + x) * 16);
+            o[0] = lo;
+            o[1] = make_uint4(0u, 0u, 0u, 0u);
         }
-        o[2] = __float2bfloat16(4.0f * (m[1] - m[0]));
-        for (int k = 3; k < 16; k++) o[k] = __float2bfloat16(0.0f);
     }
 }
 
 void cnn_input(const void *frames, int dtype, int w, int h, int N, size_t pair_stride,
                __nv_bfloat16 *x0, cudaStream_t st) {
-    const size_t total = (size_t)N * ((w + 1) / 2) * ((h + 1) / 2);
-    const int nb = imin((int)((total + 255) / 256), 8192);
+    const int nb = imin(N * ((h + 1) / 2), 8 * kNumSMs);
+    if (nb <= 0) return;
+    OF_CHECK((reinterpret_cast<uintptr_t>(x0) & 15u) == 0, "cnn_input: x0 not 16-byte aligned");
     if (dtype == OFLOW_U8)
         k_cnn_input<uint8_t><<<nb, 256, 0, st>>>(static_cast<const uint8_t *>(frames), w, h, N,
                                                  pair_stride, x0);
