@@ -364,9 +364,10 @@ oflow_status oflow_flow_to_color(oflow_ctx *ctx, int n, int width, int height,
  * of its bounded waits gave up); mode 3: the same product on the mma.sync
  * kernel; mode 1: gin = conv^T(g) (f32; g masked by y_act > 0 when y_act is
  * non-NULL) on the tcgen05 kernel, as a forward convolution of the masked
- * gradient with rotated weights (C % 16 == 0, K % 16 == 0); mode 4: the same
- * product on the mma.sync kernel; mode 2: gw = dL/dw, gbias = dL/db (f32) on
- * the tcgen05 kernel (C % 16 == 0, K <= 128); mode 5: the same on the
+ * gradient with rotated weights (C % 16 == 0, K % 8 == 0; K is padded to a
+ * multiple of 16 with zero channels); mode 4: the same product on the mma.sync
+ * kernel; mode 2: gw = dL/dw, gbias = dL/db (f32) on the tcgen05 kernel
+ * (C % 16 == 0, K % 8 == 0, K <= 128); mode 5: the same on the
  * mma.sync kernel.  x, w, y_act: bf16; g: f32.  Shapes: x [N,H,W,C],
  * w [K,3,3,C], y [N,P,Q,K]. */
 oflow_status oflow_conv3x3(int mode, int N, int H, int W, int C, int K, int stride, int relu,

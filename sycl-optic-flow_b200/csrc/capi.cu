@@ -1315,7 +1315,7 @@ oflow_status oflow_conv3x3(int mode, int N, int H, int W, int C, int K, int stri
             OF_CHECK(conv_forward_umma(d, static_cast<const __nv_bfloat16 *>(a),
                                        static_cast<const __nv_bfloat16 *>(b), bias, out, out_f32 != 0,
                                        relu != 0, err.as<int>(), st),
-                     "conv3x3: shape outside the tensor-core kernel (C % 16 == 0, K <= 128)");
+                     "conv3x3: shape outside the tensor-core kernel (C % 16 == 0, K % 8 == 0, K <= 128)");
             int e = 0;
             OF_CUDA(cudaMemcpyAsync(&e, err.as<int>(), sizeof(int), cudaMemcpyDeviceToHost, st));
             OF_CUDA(cudaStreamSynchronize(st));
@@ -1334,7 +1334,7 @@ oflow_status oflow_conv3x3(int mode, int N, int H, int W, int C, int K, int stri
                                              static_cast<const __nv_bfloat16 *>(b),
                                              static_cast<float *>(out), false, scratch.as<void>(),
                                              err.as<int>(), st),
-                     "conv3x3: shape outside the tensor-core kernel (C % 16 == 0, K % 16 == 0)");
+                     "conv3x3: shape outside the tensor-core kernel (C % 16 == 0, K % 8 == 0)");
             int e = 0;
             OF_CUDA(cudaMemcpyAsync(&e, err.as<int>(), sizeof(int), cudaMemcpyDeviceToHost, st));
             OF_CUDA(cudaStreamSynchronize(st));
@@ -1353,7 +1353,7 @@ oflow_status oflow_conv3x3(int mode, int N, int H, int W, int C, int K, int stri
                                                static_cast<const __nv_bfloat16 *>(b),
                                                static_cast<float *>(out), gbias, scratch.as<void>(),
                                                err.as<int>(), st),
-                     "conv3x3: shape outside the tensor-core kernel (C % 16 == 0, K <= 128)");
+                     "conv3x3: shape outside the tensor-core kernel (C % 16 == 0, K % 8 == 0, K <= 128)");
             int e = 0;
             OF_CUDA(cudaMemcpyAsync(&e, err.as<int>(), sizeof(int), cudaMemcpyDeviceToHost, st));
             OF_CUDA(cudaStreamSynchronize(st));

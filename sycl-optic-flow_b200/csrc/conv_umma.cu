@@ -541,7 +541,8 @@ constexpr int kBiasFinalNT = 256;
 // gradient, the rotated weights (each rounded up to 64 elements, 128-byte
 // aligned), then the bias partial sums (kBiasBlocks x K floats).
 size_t bwd_scratch_part(const ConvDims &d) {
-    const size_t g = (size_t)d.N * d.P * d.Q * d.K, wt = (size_t)d.K * 9 * d.C;
+    const size_t kp = (size_t)(d.K + 15) / 16 * 16;  // gradient channels padded to 16
+    const size_t g = (size_t)d.N * d.P * d.Q * kp, wt = kp * 9 * d.C;
     return ((g + 63) / 64 * 64 + (wt + 63) / 64 * 64) * sizeof(__nv_bfloat16);
 }
 
@@ -607,13 +608,30 @@ __global__ void __launch_bounds__(kBiasFinalNT) k_bias_final(const float *__rest
 
 // wt[c][tap][k] = w[k][8 - tap][c]: the weights of the backward-data product
 // seen as a forward convolution (rotated taps, input and output channels
-// exchanged)
-__global__ void k_flip_weights(const __nv_bfloat16 *__restrict__ w, int K, int C,
+// exchanged), with Kp >= K input channels (zero for k >= K)
+__global__ void k_flip_weights(const __nv_bfloat16 *__restrict__ w, int K, int Kp, int C,
                                __nv_bfloat16 *wt) {
-    const int n = K * 9 * C;
+    const int n = Kp * 9 * C;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int k = i % K, tap = (i / K) % 9, c = i / (9 * K);
-        wt[i] = w[((size_t)k * 9 + (8 - tap)) * C + c];
+        const int k = i % Kp, tap = (i / Kp) % 9, c = i / (9 * Kp);
+        wt[i] = k < K ? w[((size_t)k * 9 + (8 - tap)) * C + c] : __float2bfloat16(0.0f);
+    }
+}
+
+// masked bf16 gradient with its K channels padded to Kp (zero): out[m][k]
+__global__ void k_mask_pad_bf16(const float *__restrict__ g, const __nv_bfloat16 *__restrict__ yact,
+                                int M, int K, int Kp, __nv_bfloat16 *out) {
+    const size_t n = (size_t)M * Kp;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const size_t m = i / Kp;
+        const int k = (int)(i - m * Kp);
+        float v = 0.0f;
+        if (k < K) {
+            v = g[m * K + k];
+            if (yact && !(__bfloat162float(yact[m * K + k]) > 0.0f)) v = 0.0f;
+        }
+        out[i] = __float2bfloat16(v);
     }
 }
 
@@ -678,19 +696,26 @@ size_t conv_backward_data_umma_scratch(const ConvDims &d) {
 bool conv_backward_data_umma(const ConvDims &d, const float *g, const __nv_bfloat16 *y_act,
                              const __nv_bfloat16 *w, float *gin, bool accumulate, void *scratch,
                              int *err, cudaStream_t st, bool g_masked) {
-    if (d.K % 16 != 0 || d.C % 16 != 0) return false;
+    if (d.K % 8 != 0 || d.C % 16 != 0) return false;
     if ((reinterpret_cast<uintptr_t>(gin) & 15u) != 0) return false;
-    const size_t ng = (size_t)d.N * d.P * d.Q * d.K;
+    // the gradient's channels are the product's input channels: padded to a
+    // multiple of 16 (zero channels, zero weights) where K is not one
+    const int Kp = (d.K + 15) / 16 * 16;
+    const int M = d.N * d.P * d.Q;
+    const size_t ng = (size_t)M * Kp;
     __nv_bfloat16 *gb = static_cast<__nv_bfloat16 *>(scratch);
     __nv_bfloat16 *wt = gb + (ng + 63) / 64 * 64;  // 128-byte aligned
-    if (!g_masked) k_mask_bf16<<<imin((int)((ng + 255) / 256), 4096), 256, 0, st>>>(g, y_act, gb, ng);
-    k_flip_weights<<<imin(div_up(d.K * 9 * d.C, 256), 1024), 256, 0, st>>>(w, d.K, d.C, wt);
+    if (Kp != d.K)
+        k_mask_pad_bf16<<<imin((int)((ng + 255) / 256), 4096), 256, 0, st>>>(g, y_act, M, d.K, Kp, gb);
+    else if (!g_masked)
+        k_mask_bf16<<<imin((int)((ng + 255) / 256), 4096), 256, 0, st>>>(g, y_act, gb, ng);
+    k_flip_weights<<<imin(div_up(Kp * 9 * d.C, 256), 1024), 256, 0, st>>>(w, d.K, Kp, d.C, wt);
     // the product as a forward convolution over the output gradient: input
-    // (N, P, Q, K), output (N, H, W, C); stride 2 layers read a dilated input
-    ConvDims t{d.N, d.P, d.Q, d.K, d.H, d.W, 0, d.stride == 1 ? 1 : -2};
+    // (N, P, Q, Kp), output (N, H, W, C); stride 2 layers read a dilated input
+    ConvDims t{d.N, d.P, d.Q, Kp, d.H, d.W, 0, d.stride == 1 ? 1 : -2};
     for (int c0 = 0; c0 < d.C; c0 += 128) {  // at most 128 output channels a launch
         t.K = imin(128, d.C - c0);
-        if (!conv_forward_umma(t, gb, wt + (size_t)c0 * 9 * d.K, nullptr, gin + c0, true, false, err,
+        if (!conv_forward_umma(t, gb, wt + (size_t)c0 * 9 * Kp, nullptr, gin + c0, true, false, err,
                                st, d.C, accumulate))
             return false;
     }

@@ -54,14 +54,14 @@ def test_conv_products_match_cpu_oracle(of, N, H, W, C, K, stride, relu):
     gx_ref, gw_ref, gb_ref = cnn_ref.backward(x.float().numpy(), w.float().numpy(), gout_b.numpy(),
                                               stride, yb.float().cpu().numpy() if relu else None)
     gx = torch.empty((N, H, W, C), dtype=torch.float32, device="cuda")
-    if K % 16 == 0:  # mode 1: tcgen05, the backward-data product as a forward convolution
+    if K % 8 == 0:  # mode 1: tcgen05, the backward-data product as a forward convolution
         of.conv3x3(1, N, H, W, C, K, stride, relu, True, gout.cuda(), yact, wd, gx)
         assert _rel(gx.cpu().numpy(), gx_ref) < REL
         gx.fill_(float("nan"))
     of.conv3x3(4, N, H, W, C, K, stride, relu, True, gout.cuda(), yact, wd, gx)  # mma.sync
     gw = torch.empty((K, 3, 3, C), dtype=torch.float32, device="cuda")
     gb = torch.empty(K, dtype=torch.float32, device="cuda")
-    # mode 2: tcgen05 (transposing gathers, pixels split across CTAs); mode 5: mma.sync
+    # mode 2: tcgen05 (MN-major operands, pixels split across CTAs); mode 5: mma.sync
     of.conv3x3(2, N, H, W, C, K, stride, relu, True, gout.cuda(), yact, xd, gw, gbias=gb)
     torch.cuda.synchronize()
     assert _rel(gw.cpu().numpy(), gw_ref) < REL
