@@ -48,15 +48,18 @@ bool conv_forward_umma(const ConvDims &d, const __nv_bfloat16 *x, const __nv_bfl
 // backward-data on the tcgen05 kernel: the ReLU-masked gradient rounded to
 // bf16 and the rotated, transposed weights go to `scratch`
 // (conv_backward_data_umma_scratch bytes), then the product runs as forward
-// convolutions of at most 128 output channels each.  false (nothing
-// launched) when K or C is not a multiple of 16 or gin is not 16-byte aligned.
+// convolutions of at most 128 output channels each; a K that is not a
+// multiple of 16 is padded to one (zero channels, zero weights).  false
+// (nothing launched) when K is not a multiple of 8, C not one of 16, or gin is
+// not 16-byte aligned.
 size_t conv_backward_data_umma_scratch(const ConvDims &d);
-// backward-weight on the tcgen05 kernel (transposing gathers, reduction over
-// output pixels split across CTAs, atomics into gw); gw and gb are
-// overwritten; for K % 4 == 0 the bias gradient is a fixed-order sum of
-// per-block partial sums made in the pass that masks the gradient.  scratch:
-// the same size as for backward-data.  false (nothing
-// launched) when K > 128, C is not a multiple of 16 or x is not 16-byte aligned.
+// backward-weight on the tcgen05 kernel (MN-major operands gathered from NHWC
+// memory, reduction over output pixels split across CTAs, atomics into gw);
+// gw and gb are overwritten; for K % 4 == 0 the bias gradient is a fixed-order
+// sum of per-block partial sums made in the pass that masks the gradient.
+// scratch: the same size as for backward-data.  false (nothing launched) when
+// K > 128, K is not a multiple of 8, C not one of 16, or x or scratch is not
+// 16-byte aligned.
 bool conv_backward_weight_umma(const ConvDims &d, const float *g, const __nv_bfloat16 *y_act,
                                const __nv_bfloat16 *x, float *gw, float *gb, void *scratch,
                                int *err, cudaStream_t st);
