@@ -207,17 +207,22 @@ __device__ __forceinline__ void lk_window_solve_p(const float *gx, const float *
 
 // One refinement of pyramidal LK: warp I1 by the current flow (bilinear,
 // clamp-to-edge), It = 0 + (-1)*I0 + 1*I1w, window solve, Uout = Uin + d.
-// Tile 32 x kPTH with the window radius C as halo; a thread solves kPP
-// vertically adjacent pixels (lk_window_solve_p).  (Window sums read from
-// precomputed product planes measured slower: 18.2k against 21.4k pairs/s
-// batched; five loads per window element instead of three bound the LSU pipe.)
-constexpr int kPTW = 32, kPP = 2, kPTH = 32, kPNT = kPTW * kPTH / kPP;
-template <int C>
-__global__ void __launch_bounds__(kPNT) k_pyrlk_iter(const float *__restrict__ pyr, size_t lp,
-                                                     const float2 *__restrict__ G, size_t gstride,
-                                                     const float2 *__restrict__ Uin,
-                                                     float2 *Uout, size_t ustride, int nx,
-                                                     int ny) {
+// Tile 32 x kPTH with the window radius C as halo; a thread solves PP
+// vertically adjacent pixels (lk_window_solve_p): 4 when a launch has tiles
+// enough to fill the GPU (the elements of eight window rows loaded and
+// multiplied once for four pixels: 29.0k against 28.0k pairs/s on 64 pairs of
+// 640x480), else 2 (twice the threads: 9.7k against 9.2k pairs/s for one
+// pair).  (Window sums read from precomputed product planes measured slower:
+// 18.2k against 21.4k pairs/s batched; five loads per window element instead
+// of three bound the LSU pipe.)
+constexpr int kPTW = 32, kPTH = 32;
+template <int C, int PP>
+__global__ void __launch_bounds__(kPTW * kPTH / PP) k_pyrlk_iter(const float *__restrict__ pyr, size_t lp,
+                                                                 const float2 *__restrict__ G, size_t gstride,
+                                                                 const float2 *__restrict__ Uin,
+                                                                 float2 *Uout, size_t ustride, int nx,
+                                                                 int ny) {
+    constexpr int kPNT = kPTW * kPTH / PP;
     constexpr int RW = kPTW + 2 * C, RH = kPTH + 2 * C;
     __shared__ float gx[RW * RH], gy[RW * RH], gt[RW * RH];
     const int b = blockIdx.z;
@@ -245,14 +250,14 @@ __global__ void __launch_bounds__(kPNT) k_pyrlk_iter(const float *__restrict__ p
         gt[i] = it;
     }
     __syncthreads();
-    const int tx = threadIdx.x % kPTW, ty = (threadIdx.x / kPTW) * kPP;
+    const int tx = threadIdx.x % kPTW, ty = (threadIdx.x / kPTW) * PP;
     const int x = blockIdx.x * kPTW + tx, yb = blockIdx.y * kPTH + ty;
     if (x >= nx || yb >= ny) return;
-    float dx[kPP], dy[kPP];
+    float dx[PP], dy[PP];
     // top-left of the first pixel's window: row ty, column tx of the region
-    lk_window_solve_p<C, kPP>(gx, gy, gt, RW, ty * RW + tx, dx, dy);
+    lk_window_solve_p<C, PP>(gx, gy, gt, RW, ty * RW + tx, dx, dy);
 #pragma unroll
-    for (int k = 0; k < kPP; k++) {
+    for (int k = 0; k < PP; k++) {
         const int y = yb + k;
         if (y >= ny) break;
         const bool in = x >= C && y >= C && x < nx - C && y < ny - C;
@@ -265,13 +270,20 @@ __global__ void __launch_bounds__(kPNT) k_pyrlk_iter(const float *__restrict__ p
 static void launch_pyrlk_iter(int c, dim3 g, cudaStream_t st, const float *pyr, size_t lp,
                               const float2 *G, size_t gstride, const float2 *Uin, float2 *Uout,
                               size_t ustride, int nx, int ny) {
+    const bool wide = (size_t)g.x * g.y * g.z > 4 * (size_t)kNumSMs;
+#define OF_PYRLK(C)                                                                                  \
+    if (wide)                                                                                        \
+        k_pyrlk_iter<C, 4><<<g, kPTW * kPTH / 4, 0, st>>>(pyr, lp, G, gstride, Uin, Uout, ustride, nx, ny); \
+    else                                                                                             \
+        k_pyrlk_iter<C, 2><<<g, kPTW * kPTH / 2, 0, st>>>(pyr, lp, G, gstride, Uin, Uout, ustride, nx, ny);
     switch (c) {
-        case 0: k_pyrlk_iter<0><<<g, kPNT, 0, st>>>(pyr, lp, G, gstride, Uin, Uout, ustride, nx, ny); break;
-        case 1: k_pyrlk_iter<1><<<g, kPNT, 0, st>>>(pyr, lp, G, gstride, Uin, Uout, ustride, nx, ny); break;
-        case 2: k_pyrlk_iter<2><<<g, kPNT, 0, st>>>(pyr, lp, G, gstride, Uin, Uout, ustride, nx, ny); break;
-        case 3: k_pyrlk_iter<3><<<g, kPNT, 0, st>>>(pyr, lp, G, gstride, Uin, Uout, ustride, nx, ny); break;
-        default: k_pyrlk_iter<4><<<g, kPNT, 0, st>>>(pyr, lp, G, gstride, Uin, Uout, ustride, nx, ny); break;
+        case 0: OF_PYRLK(0) break;
+        case 1: OF_PYRLK(1) break;
+        case 2: OF_PYRLK(2) break;
+        case 3: OF_PYRLK(3) break;
+        default: OF_PYRLK(4) break;
     }
+#undef OF_PYRLK
 }
 
 // ================================================================ host plans
